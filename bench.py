@@ -1,0 +1,324 @@
+#!/usr/bin/env python
+"""Benchmark: batched Classic McEliece decryption on B200.
+
+Workload (one step): one batch of 65,536 mceliece6960119 ciphertexts (194 B,
+1547-bit syndromes), each an encryption of a uniformly random weight-119 error
+vector under one seeded key (the reference kem/ key regenerated from its fixed
+DRBG seed), decrypted by the fused syndrome -> Berlekamp-Massey -> root search
+kernel.  Every step's output is checked bit-exact against the planted error
+vectors before timing is reported.
+
+  value   decaps/s with ciphertexts resident in HBM (all ranks; weak scaling)
+  e2e     the same through the public host-buffer call cmd_decrypt_batch from
+          pinned host memory (H2D of the ciphertexts, D2H of error vectors and
+          weights inside the timed region)
+  plain   the three-kernel per-stage path on the same batch (the comparison the
+          metric names)
+  roofline: int-ALU -- algorithmic lane-ops (W per decap, see
+          cm_decrypt__b200.roofline) / fused-kernel time vs the device's
+          measured lop3 rate; HBM bytes/decap shown beside it
+  cpu_baseline: the reference's own CPU decoder (oracle/_ref, built from its
+          sources) on all host cores over a bounded sample
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+SET = 6960119
+COUNT = 65536
+L2_BYTES = 126 * 2 ** 20
+KEM_SK = os.path.join(REPO, "tests", "golden", "kem", f"sk_{SET}.bin")
+TRAFFIC_FILE = os.path.join(REPO, "profiles", "fused_6960119_traffic.json")
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--count", type=int, default=COUNT)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    FIELDS = ("clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + ",".join(self.FIELDS),
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self) -> dict | None:
+        rows = [r.split(", ") for r in self.out.strip().splitlines() if r.count(",") >= 7]
+        if not rows:
+            return None
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = max(float(r[1]) for r in rows)
+        reasons = set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            for nm, v in zip(names, r[4:8]):
+                if v.strip() == "Active":
+                    reasons.add(nm)
+        busy = [x for x in sm if x > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())}
+
+
+def cpu_reference(sk: bytes, cts: np.ndarray, seconds_target: float = 15.0) -> dict:
+    """The reference CPU decoder (oracle/_ref, else the oracle restatement) on
+    all host cores over a bounded sample of the workload."""
+    from oracle import oracle as o
+    cores = os.cpu_count() or 1
+    if o.RefLib.available(SET):
+        dec, kind = o.RefLib(SET), "reference"
+    else:
+        dec, kind = o.Oracle(SET), "port"
+    probe = cts[: max(cores, 8)]
+    t0 = time.perf_counter()
+    dec.decrypt(sk, probe, nthreads=cores)
+    rate = probe.shape[0] / (time.perf_counter() - t0)
+    n = int(min(cts.shape[0], max(cores, rate * seconds_target)))
+    t0 = time.perf_counter()
+    dec.decrypt(sk, cts[:n], nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "decaps/s", "cores": cores, "kind": kind,
+            "sample": f"{n} of the {cts.shape[0]} mceliece6960119 ciphertexts, {cores} threads, {dt:.1f} s"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import cm_decrypt__b200 as cmd
+    from oracle import oracle as o
+    sk = open(KEM_SK, "rb").read()
+    pk = cmd.PubKey(SET, sk)
+    cores = os.cpu_count() or 1
+    kind = "reference" if o.RefLib.available(SET) else "port"
+    dec = o.RefLib(SET) if kind == "reference" else o.Oracle(SET)
+    per_step = max(cores, 8) * 4
+    cts, planted, _ = pk.ciphertexts(seed=1, count=per_step)
+    for _ in range(args.warmup):
+        dec.decrypt(sk, cts, nthreads=cores)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        got = dec.decrypt(sk, cts, nthreads=cores)
+    dt = time.perf_counter() - t0
+    assert np.array_equal(got, planted)
+    v = per_step * args.steps / dt
+    line = {
+        "impl": "reference", "metric": "decaps/s", "value": v, "unit": "decaps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/u32 GF(2^13)",
+        "data": "synthetic",
+        "config": {"workload": "mceliece6960119 decrypt, 1 seeded key, uniform weight-119 errors",
+                   "sample_per_step": per_step},
+        "cpu_baseline": {"value": v, "unit": "decaps/s", "cores": cores, "kind": kind,
+                         "sample": f"{per_step} ciphertexts per step, {cores} threads"},
+        "e2e": {"value": v, "unit": "decaps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import cm_decrypt__b200 as cmd
+    from cm_decrypt__b200.roofline import hbm_bytes_per_decap, work_per_decap
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    count = args.count
+
+    eng = cmd.Engine(local)
+    sk = open(KEM_SK, "rb").read()
+    key = cmd.Key(eng, SET, sk)
+    info = key.info
+    pk = cmd.PubKey(SET, sk)
+    cts, planted, valid = pk.ciphertexts(seed=1000 + rank, count=count)
+
+    # Rotating device buffer sets, together larger than 2x L2, so no step
+    # reads inputs or writes outputs the previous step left in L2.
+    per_set = count * (info.ct_bytes + 4 * info.err_words + 2)
+    nbuf = max(2, math.ceil(2 * L2_BYTES / per_set))
+    d_cts = [torch.from_numpy(cts).cuda() for _ in range(nbuf)]
+    d_err = [torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda") for _ in range(nbuf)]
+    d_w = [torch.zeros(count, dtype=torch.int16, device="cuda") for _ in range(nbuf)]
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def step(i: int, path: str) -> None:
+        b = i % nbuf
+        cmd.decrypt_device(eng, key, d_cts[b].data_ptr(), count, d_err[b].data_ptr(), d_w[b].data_ptr(), sp, path)
+
+    def check(b: int) -> None:
+        w = d_err[b].cpu().numpy().astype("<u4").view(np.uint8).reshape(count, -1)[:, : info.err_bytes]
+        if not np.array_equal(w, planted):
+            raise SystemExit("bench: decrypt output differs from the planted error vectors")
+        if not (d_w[b].cpu().numpy().view(np.uint16) == info.t).all():
+            raise SystemExit("bench: weight check failed")
+
+    def timed(path: str, steps: int, warmup: int) -> tuple[float, int, dict | None]:
+        for i in range(warmup):
+            step(i, path)
+        torch.cuda.synchronize()
+        for b in range(min(nbuf, warmup)):
+            check(b)
+        for b in range(nbuf):
+            d_err[b].zero_()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = eng.launch_count()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            e0.record(stream)
+            for i in range(steps):
+                step(i, path)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        launches = eng.launch_count() - l0
+        for b in range(min(nbuf, steps)):
+            check(b)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, launches, clk.summary()
+
+    int_peak = eng.int_peak()
+    ms, launches, clocks = timed("fused", args.steps, args.warmup)
+    ms_plain = None
+    if not args.no_plain:
+        ms_plain, _, _ = timed("plain", max(1, min(args.steps, 3)), 1)
+
+    # End to end through the public host-buffer call, pinned host memory.
+    h_cts = torch.from_numpy(cts).pin_memory().numpy()
+    h_err = torch.empty((count, info.err_bytes), dtype=torch.uint8).pin_memory().numpy()
+    h_w = torch.empty(count, dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    for _ in range(max(1, args.warmup)):
+        cmd.decrypt_into(eng, key, h_cts, h_err, h_w, path="fused")
+    if not np.array_equal(h_err, planted):
+        raise SystemExit("bench: e2e output differs from the planted error vectors")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        cmd.decrypt_into(eng, key, h_cts, h_err, h_w, path="fused")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    value = world * count * args.steps / (ms * 1e-3)
+    per_rank = count * args.steps / (ms * 1e-3)
+    w = work_per_decap(SET)
+    achieved = per_rank * w["total"]
+    hbm = per_rank * hbm_bytes_per_decap(SET)
+    traffic = None
+    if os.path.exists(TRAFFIC_FILE):
+        traffic = json.load(open(TRAFFIC_FILE)).get("dram_bytes_per_launch_scaled")
+    peaks = {}
+    pk_path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(pk_path):
+        peaks = json.load(open(pk_path))
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+
+    line = {
+        "metric": "decaps/s", "value": value, "unit": "decaps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32 bitsliced GF(2^13)", "data": "synthetic",
+        "config": {"workload": "mceliece6960119 fused decrypt, 1 seeded key (reference kem/ key), "
+                               f"{count} ciphertexts/step/GPU, uniform weight-119 errors",
+                   "set": SET, "ciphertexts_per_step": count, "parallelism": f"replicas x{world}",
+                   "l2": f"rotating {nbuf} resident buffer sets ({nbuf * per_set / 2**20:.0f} MiB > 2x L2)"},
+        "gpu_launches": launches,
+        "plain": None if ms_plain is None else {
+            "value": world * count * min(args.steps, 3) / (ms_plain * 1e-3),
+            "ms_per_step": ms_plain / max(1, min(args.steps, 3)),
+            "fused_speedup": (ms_plain / max(1, min(args.steps, 3))) / (ms / args.steps)},
+        "e2e": {"value": world * count * args.steps / e2e_s, "unit": "decaps/s",
+                "h2d_bytes_per_step": count * info.ct_bytes,
+                "d2h_bytes_per_step": count * (info.err_bytes + 2)},
+        "roofline": {"bound": "int_alu", "achieved": achieved / 1e12, "peak": int_peak / 1e12,
+                     "unit": "Tlane-ops/s (lop3)", "frac": achieved / int_peak,
+                     "peak_source": "measured on this GPU: lop3.b32 chains (cmd_bench_int_peak)",
+                     "work_per_decap": w,
+                     "traffic": traffic,
+                     "hbm": {"achieved_gbs": hbm / 1e9, "peak_gbs": hbm_peak, "frac": hbm / 1e9 / hbm_peak,
+                             "bytes_per_decap": hbm_bytes_per_decap(SET)}},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(sk, cts)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    key.free()
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

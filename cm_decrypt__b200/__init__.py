@@ -1,0 +1,347 @@
+"""B200-native batched Classic McEliece decryption engine.
+
+Drop-in for the decrypt path of somesh-vas/CM_Decrypt_: same sk_<set>.bin /
+ct_<set>.bin inputs, same errorstream0_<set>.bin text, bit-exact with the
+reference CPU/ decoder for the five parameter sets.  All decoding runs in the
+CUDA kernels of libcmd_b200.so (sm_100a); this module is a thin ctypes
+front-end over its C ABI (include/cmd_b200.h).  There is no CPU fallback: on a
+machine without a B200 the compute calls raise CmdError.
+
+The names mirror the reference's decoder interface (CPU/include/common/
+root.h, bm.h): ``Key`` replaces initialisation() + support_gen() +
+compute_inverses(); ``synd``, ``bm`` and ``root`` are the per-stage hooks;
+``decrypt`` is the per-ciphertext loop of decrypt.c run as one batch;
+``errorstream`` / ``decrypt_files`` are write_error_positions and the CLI.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libcmd_b200.so")
+CLI_PATH = os.path.join(PKG_DIR, "cmd_decrypt")
+
+SETS = (348864, 460896, 6688128, 6960119, 8192128)
+SET_INDEX = {s: i for i, s in enumerate(SETS)}
+
+# Status codes (include/cmd_b200.h); 0/-1/-4 are the reference's KAT_* codes.
+CMD_OK, CMD_E_FILE, CMD_E_ARG, CMD_E_CUDA = 0, -1, -4, -5
+CMD_E_NOMEM, CMD_E_BUDGET, CMD_E_BUSY, CMD_E_TIMEOUT, CMD_E_NODEVICE = -6, -7, -8, -9, -10
+PATHS = {"auto": 0, "plain": 1, "fused": 2}
+
+
+class CmdError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what} failed with status {code}: {_last_error()}")
+        self.code = code
+
+
+class _SetInfo(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in
+                ("set_id", "m", "n", "t", "ct_bytes", "sk_bytes", "sb", "err_bytes", "err_words")]
+
+
+@dataclass(frozen=True)
+class SetInfo:
+    set_id: int
+    m: int
+    n: int
+    t: int
+    ct_bytes: int
+    sk_bytes: int
+    sb: int
+    err_bytes: int
+    err_words: int
+
+
+_lib: ctypes.CDLL | None = None
+_vp, _sz, _u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64
+_i32 = ctypes.c_int
+
+
+def lib() -> ctypes.CDLL:
+    """Loads libcmd_b200.so (built in-tree by cm_decrypt__b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} missing: run `python -m cm_decrypt__b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    sig = {
+        "cmd_last_error": (ctypes.c_char_p, []),
+        "cmd_set_info_get": (_i32, [_i32, ctypes.POINTER(_SetInfo)]),
+        "cmd_set_from_name": (_i32, [ctypes.c_char_p, ctypes.POINTER(_i32)]),
+        "cmd_engine_create": (_i32, [_i32, _sz, ctypes.POINTER(_vp)]),
+        "cmd_engine_destroy": (None, [_vp]),
+        "cmd_engine_memory": (_i32, [_vp, ctypes.POINTER(_sz), ctypes.POINTER(_sz)]),
+        "cmd_engine_launch_count": (_u64, [_vp]),
+        "cmd_key_expand": (_i32, [_vp, _i32, _vp, _sz, ctypes.POINTER(_vp)]),
+        "cmd_key_free": (None, [_vp]),
+        "cmd_key_set": (_i32, [_vp, ctypes.POINTER(_i32)]),
+        "cmd_key_device_bytes": (_sz, [_vp]),
+        "cmd_key_support": (_i32, [_vp, _vp, _sz]),
+        "cmd_key_goppa": (_i32, [_vp, _vp, _sz]),
+        "cmd_key_synd_table": (_i32, [_vp, _vp, _sz]),
+        "cmd_decrypt_batch": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp]),
+        "cmd_decrypt_device": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp, _vp]),
+        "cmd_decrypt_mixed_device": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+        "cmd_stage_synd": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_stage_bm": (_i32, [_vp, _i32, _vp, _sz, _vp, _vp]),
+        "cmd_stage_root": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),
+        "cmd_stage_root_images": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_errorstream_format": (_i32, [_i32, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz)]),
+        "cmd_errorstream_write": (_i32, [_i32, _vp, _sz, ctypes.c_char_p, _i32]),
+        "cmd_decrypt_files": (_i32, [_vp, _i32, ctypes.c_char_p, ctypes.c_char_p, _sz, ctypes.c_char_p, _i32,
+                                     ctypes.POINTER(ctypes.c_double)]),
+        "cmd_bench_int_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+        "cmd_synth_key": (_i32, [_i32, _vp, _u64, _vp]),
+        "cmd_synth_pubkey": (_i32, [_i32, _vp, ctypes.POINTER(_vp)]),
+        "cmd_synth_pubkey_free": (None, [_vp]),
+        "cmd_synth_ciphertexts": (_i32, [_vp, _u64, _sz, ctypes.c_uint32, _vp, _vp, _vp, _i32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _last_error() -> str:
+    try:
+        return (lib().cmd_last_error() or b"").decode()
+    except Exception:  # pragma: no cover - only when the library is absent
+        return ""
+
+
+def _check(code: int, what: str) -> None:
+    if code != CMD_OK:
+        raise CmdError(code, what)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def set_index(set_id: int) -> int:
+    if set_id in SET_INDEX:
+        return SET_INDEX[set_id]
+    if 0 <= set_id < len(SETS):
+        return set_id
+    raise ValueError(f"unknown parameter set {set_id}")
+
+
+def set_info(set_id: int) -> SetInfo:
+    info = _SetInfo()
+    _check(lib().cmd_set_info_get(set_index(set_id), ctypes.byref(info)), "cmd_set_info_get")
+    return SetInfo(*[getattr(info, f) for f, _ in _SetInfo._fields_])
+
+
+class Engine:
+    """One engine per GPU; owns the stream, scratch and the HBM budget."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = _vp()
+        _check(lib().cmd_engine_create(device, hbm_budget, ctypes.byref(h)), "cmd_engine_create")
+        self.handle = h
+
+    def close(self) -> None:
+        if self.handle:
+            lib().cmd_engine_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def memory(self) -> tuple[int, int]:
+        used, budget = _sz(), _sz()
+        _check(lib().cmd_engine_memory(self.handle, ctypes.byref(used), ctypes.byref(budget)), "memory")
+        return used.value, budget.value
+
+    def launch_count(self) -> int:
+        return int(lib().cmd_engine_launch_count(self.handle))
+
+    def int_peak(self) -> float:
+        """Measured lop3.b32 lane-operations per second (int-ALU roofline)."""
+        v = ctypes.c_double()
+        _check(lib().cmd_bench_int_peak(self.handle, ctypes.byref(v)), "cmd_bench_int_peak")
+        return v.value
+
+
+class Key:
+    """Device-resident expanded secret key (support, 1/g(L)^2, tables)."""
+
+    def __init__(self, engine: Engine, set_id: int, sk: bytes):
+        self.engine = engine
+        self.info = set_info(set_id)
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        h = _vp()
+        _check(lib().cmd_key_expand(engine.handle, set_index(set_id), _ptr(skb), skb.size, ctypes.byref(h)),
+               "cmd_key_expand")
+        self.handle = h
+
+    def free(self) -> None:
+        if self.handle:
+            lib().cmd_key_free(self.handle)
+            self.handle = None
+
+    def device_bytes(self) -> int:
+        return int(lib().cmd_key_device_bytes(self.handle))
+
+    def support(self) -> np.ndarray:
+        out = np.zeros(self.info.n, np.uint16)
+        _check(lib().cmd_key_support(self.handle, _ptr(out), out.size), "cmd_key_support")
+        return out
+
+    def goppa(self) -> np.ndarray:
+        out = np.zeros(self.info.t + 1, np.uint16)
+        _check(lib().cmd_key_goppa(self.handle, _ptr(out), out.size), "cmd_key_goppa")
+        return out
+
+    def synd_table(self) -> np.ndarray:
+        out = np.zeros((self.info.sb, 2 * self.info.t), np.uint16)
+        _check(lib().cmd_key_synd_table(self.handle, _ptr(out), out.size), "cmd_key_synd_table")
+        return out
+
+
+def decrypt(engine: Engine, key: Key, cts, path: str = "auto") -> tuple[np.ndarray, np.ndarray]:
+    """Host batch: cts uint8 [count, ct_bytes] -> (err uint8 [count, n/8], weight uint16 [count])."""
+    info = key.info
+    c = np.ascontiguousarray(np.frombuffer(bytes(cts), np.uint8) if isinstance(cts, (bytes, bytearray))
+                             else cts, np.uint8).reshape(-1, info.ct_bytes)
+    err = np.zeros((c.shape[0], info.err_bytes), np.uint8)
+    w = np.zeros(c.shape[0], np.uint16)
+    _check(lib().cmd_decrypt_batch(engine.handle, key.handle, PATHS[path], _ptr(c), c.shape[0], _ptr(err), _ptr(w)),
+           "cmd_decrypt_batch")
+    return err, w
+
+
+def decrypt_into(engine: Engine, key: Key, cts: np.ndarray, err: np.ndarray, weight: np.ndarray | None = None,
+                 path: str = "auto") -> None:
+    """Host batch into caller buffers (pinned buffers make the copies DMA)."""
+    info = key.info
+    assert cts.dtype == np.uint8 and cts.flags.c_contiguous and cts.size % info.ct_bytes == 0
+    count = cts.size // info.ct_bytes
+    assert err.dtype == np.uint8 and err.flags.c_contiguous and err.size == count * info.err_bytes
+    wp = 0
+    if weight is not None:
+        assert weight.dtype == np.uint16 and weight.size == count
+        wp = _ptr(weight)
+    _check(lib().cmd_decrypt_batch(engine.handle, key.handle, PATHS[path], _ptr(cts), count, _ptr(err), wp or None),
+           "cmd_decrypt_batch")
+
+
+def decrypt_device(engine: Engine, key: Key, d_cts: int, count: int, d_err: int, d_weight: int = 0,
+                   stream: int = 0, path: str = "auto") -> None:
+    """Device pointers (e.g. torch tensor data_ptr()); asynchronous on `stream`."""
+    _check(lib().cmd_decrypt_device(engine.handle, key.handle, PATHS[path], d_cts, count, d_err,
+                                    d_weight or None, stream or None), "cmd_decrypt_device")
+
+
+def decrypt_mixed_device(engine: Engine, keys: list[Key], key_idx: np.ndarray, d_cts: int, ct_off: np.ndarray,
+                         d_err: int, err_off: np.ndarray, d_weight: int = 0, stream: int = 0) -> None:
+    arr = (_vp * len(keys))(*[k.handle for k in keys])
+    ki = np.ascontiguousarray(key_idx, np.uint32)
+    co = np.ascontiguousarray(ct_off, np.uint64)
+    eo = np.ascontiguousarray(err_off, np.uint64)
+    _check(lib().cmd_decrypt_mixed_device(engine.handle, arr, len(keys), _ptr(ki), d_cts, _ptr(co), ki.size, d_err,
+                                          _ptr(eo), d_weight or None, stream or None), "cmd_decrypt_mixed_device")
+
+
+# ---- per-stage hooks (device pointers) -----------------------------------
+def synd(engine: Engine, key: Key, d_cts: int, count: int, d_synd: int, stream: int = 0) -> None:
+    _check(lib().cmd_stage_synd(engine.handle, key.handle, d_cts, count, d_synd, stream or None), "synd")
+
+
+def bm(engine: Engine, set_id: int, d_synd: int, count: int, d_loc: int, stream: int = 0) -> None:
+    _check(lib().cmd_stage_bm(engine.handle, set_index(set_id), d_synd, count, d_loc, stream or None), "bm")
+
+
+def root(engine: Engine, key: Key, d_loc: int, count: int, d_err: int, d_weight: int = 0, stream: int = 0) -> None:
+    _check(lib().cmd_stage_root(engine.handle, key.handle, d_loc, count, d_err, d_weight or None, stream or None),
+           "root")
+
+
+def root_images(engine: Engine, key: Key, d_loc: int, count: int, d_images: int, stream: int = 0) -> None:
+    _check(lib().cmd_stage_root_images(engine.handle, key.handle, d_loc, count, d_images, stream or None),
+           "root_images")
+
+
+# ---- errorstream / file contract -------------------------------------------
+def errorstream(set_id: int, err: np.ndarray) -> bytes:
+    info = set_info(set_id)
+    e = np.ascontiguousarray(err, np.uint8).reshape(-1, info.err_bytes)
+    need = _sz()
+    lib().cmd_errorstream_format(set_index(set_id), _ptr(e), e.shape[0], None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(need.value + 1)
+    _check(lib().cmd_errorstream_format(set_index(set_id), _ptr(e), e.shape[0], buf, need.value + 1,
+                                        ctypes.byref(need)), "cmd_errorstream_format")
+    return buf.raw[:need.value]
+
+
+def write_errorstream(set_id: int, err: np.ndarray, path: str, append: bool = False) -> None:
+    info = set_info(set_id)
+    e = np.ascontiguousarray(err, np.uint8).reshape(-1, info.err_bytes)
+    _check(lib().cmd_errorstream_write(set_index(set_id), _ptr(e), e.shape[0], path.encode(), int(append)),
+           "cmd_errorstream_write")
+
+
+def decrypt_files(engine: Engine, set_id: int, sk_path: str, ct_path: str, katnum: int, out_path: str,
+                  path: str = "auto") -> float:
+    secs = ctypes.c_double()
+    _check(lib().cmd_decrypt_files(engine.handle, set_index(set_id), sk_path.encode(), ct_path.encode(), katnum,
+                                   out_path.encode(), PATHS[path], ctypes.byref(secs)), "cmd_decrypt_files")
+    return secs.value
+
+
+# ---- synthetic workloads -----------------------------------------------------
+def synth_key(set_id: int, base_sk: bytes, seed: int) -> bytes:
+    info = set_info(set_id)
+    base = np.frombuffer(bytes(base_sk), np.uint8).copy()
+    out = np.zeros(info.sk_bytes, np.uint8)
+    _check(lib().cmd_synth_key(set_index(set_id), _ptr(base), seed, _ptr(out)), "cmd_synth_key")
+    return out.tobytes()
+
+
+class PubKey:
+    """Systematic parity-check data for encrypting synthetic ciphertexts."""
+
+    def __init__(self, set_id: int, sk: bytes):
+        self.info = set_info(set_id)
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        h = _vp()
+        _check(lib().cmd_synth_pubkey(set_index(set_id), _ptr(skb), ctypes.byref(h)), "cmd_synth_pubkey")
+        self.handle = h
+
+    def __del__(self):
+        if getattr(self, "handle", None) and _lib is not None:
+            _lib.cmd_synth_pubkey_free(self.handle)
+            self.handle = None
+
+    def ciphertexts(self, seed: int, count: int, malformed_permille: int = 0, nthreads: int = 0):
+        """-> (cts uint8 [count, ct_bytes], planted err uint8 [count, n/8], valid uint8 [count])."""
+        info = self.info
+        cts = np.zeros((count, info.ct_bytes), np.uint8)
+        err = np.zeros((count, info.err_bytes), np.uint8)
+        valid = np.zeros(count, np.uint8)
+        nt = nthreads or min(32, os.cpu_count() or 1)
+        _check(lib().cmd_synth_ciphertexts(self.handle, seed, count, malformed_permille, _ptr(cts), _ptr(err),
+                                           _ptr(valid), nt), "cmd_synth_ciphertexts")
+        return cts, err, valid
+
+
+def cuda_available() -> bool:
+    """True when a CUDA device the engine can drive is present."""
+    try:
+        e = Engine()
+    except (CmdError, FileNotFoundError, OSError):
+        return False
+    e.close()
+    return True

@@ -1,0 +1,79 @@
+// Engine and key objects behind the opaque C handles, plus the helpers the
+// batch, tuning and serving code share.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+struct cmd_engine;
+
+namespace cmd {
+
+// Growable device buffer charged against the engine's HBM budget.
+struct Scratch {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    int reserve(cmd_engine *eng, size_t bytes);
+    void release(cmd_engine *eng);
+};
+
+// Growable pinned host buffer (staging for host-pointer calls).
+struct HostScratch {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    int reserve(size_t bytes);
+    void release();
+};
+
+// Fused-kernel launch configuration chosen per parameter set.
+struct FusedConfig {
+    int wpb = 8;         // warps per CTA (4 or 8)
+    int ctas_per_sm = 1; // resident CTAs per SM the grid is sized for
+    bool tuned = false;
+    double us_per_ct = 0;
+};
+
+int cuda_fail(cudaError_t e, const char *what);
+bool valid_set(int set);
+bool budget_take(cmd_engine *eng, size_t bytes);
+void budget_give(cmd_engine *eng, size_t bytes);
+
+int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
+               uint32_t *d_err, uint16_t *d_weight, cudaStream_t s);
+int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                     uint16_t *d_weight, cudaStream_t s);
+size_t fused_smem(int set, int wpb);
+size_t smem_limit_bytes();
+
+}  // namespace cmd
+
+struct cmd_engine {
+    int device = 0;
+    int num_sms = 0;
+    char gpu_name[256] = {0};
+    size_t budget = 0;
+    std::atomic<size_t> used{0};
+    cudaStream_t stream = nullptr;
+    std::mutex mu;                 // serialises calls that share scratch
+    cmd::Scratch scratch;          // plain-path intermediates
+    cmd::Scratch io;               // device staging for host-buffer calls
+    cmd::Scratch fused;            // fused-kernel work lists
+    cmd::HostScratch host_scratch; // pinned staging
+    uint32_t *tile_counter = nullptr;
+    std::atomic<uint64_t> launches{0};
+    cmd::FusedConfig fcfg[cmd::NSETS];
+    cmd::FusedConfig fcfg_mixed;
+};
+
+struct cmd_key {
+    cmd_engine *eng = nullptr;
+    cmd::KeyDev dev;
+    void *block = nullptr;
+    size_t bytes = 0;
+};

@@ -1,0 +1,418 @@
+// Fused, persistent decrypt kernel: syndrome -> Berlekamp-Massey -> root
+// search -> error-word pack in one launch, for batches of one key or mixed
+// batches of many keys and parameter sets.
+//
+// Work unit ("round"): up to WPB*32 ciphertexts of one key.  A CTA takes
+// rounds from a device counter until none are left; warp w of the CTA owns
+// the 32-ciphertext tile w of the round, so after the shared syndrome-table
+// pipeline every warp runs independently:
+//
+//  1. stage its 32 ciphertexts in shared memory (128-bit loads when the round
+//     is one aligned slab);
+//  2. syndrome (util.c:102-114): lane q accumulates the packed 2t syndromes
+//     of ciphertext q; the key's syndrome table streams through shared memory
+//     in 16-row chunks (cp.async double buffer, shared by all warps) and each
+//     row is masked by the ciphertext bit, never branched on;
+//  3. ballot-transpose the syndromes to bitsliced form (bit q = ciphertext q);
+//  4. Berlekamp-Massey (bm.c:12-68) bitsliced across the 32 ciphertexts: lane
+//     l owns locator coefficients l, l+32, ... in registers, the discrepancy is
+//     a shuffle-XOR reduction, B lives in a shared ring buffer whose rotation
+//     implements the x*B shift, d/b uses a bitsliced inversion chain;
+//  5. root search (root_13.c:216-240) per ciphertext: lanes take 32-point
+//     support words, coefficients become broadcast plane masks, Horner runs
+//     bitsliced; the zero test gives the packed error word directly and the
+//     flagged-position count is reduced per ciphertext.
+#pragma once
+#include "gf.cuh"
+#include "internal.h"
+
+namespace cmd {
+
+constexpr uint32_t FULLMASK = 0xFFFFFFFFu;
+constexpr int TAB_ROWS = 16;  // syndrome-table rows per staged chunk
+
+__host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
+__host__ __device__ constexpr int al16(int x) { return (x + 15) / 16 * 16; }
+
+template <int S> struct Fz {
+    using P = Set<S>;
+    static constexpr int M = P::M, T = P::T, NJ = (T + 1 + 31) / 32;
+    static constexpr int TWP = (T + 3) / 4 * 4;      // padded table row (words)
+    static constexpr int RING = T + 2;               // B ring slots
+    static constexpr int RAW_B = 32 * P::CT;
+    static constexpr int RING_B = RING * M * 4;
+    static constexpr int MASK_B = (T + 1) * 16 * 4;
+    static constexpr int A_B = al16(cmax(RAW_B + 16, cmax(RING_B, MASK_B)));
+    static constexpr int S_B = al16(2 * T * M * 4);  // bitsliced syndromes / locator
+    static constexpr int WARP_B = A_B + S_B;
+    static constexpr int TAB_B = TAB_ROWS * TWP * 4;  // one chunk buffer
+};
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Little-endian 32-bit read at any byte offset of shared memory.
+__device__ __forceinline__ uint32_t ld_u32_any(const uint8_t *p)
+{
+    const uintptr_t a = (uintptr_t)p;
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(a & ~(uintptr_t)3);
+    const uint32_t sh = (uint32_t)(a & 3) * 8;
+    return __funnelshift_r(w[0], w[1], sh);
+}
+
+struct RoundCtx {
+    const FusedArgs *a;
+    FusedTile tile;
+    FusedKeyRef key;
+};
+
+// Index (in the batch) of ciphertext q of warp `warp` in this round.
+__device__ __forceinline__ uint64_t ct_index(const RoundCtx &rc, int warp, int q)
+{
+    const uint64_t slot = rc.tile.first + (uint64_t)warp * 32 + q;
+    return rc.a->order ? rc.a->order[slot] : slot;
+}
+
+template <int S, int WPB>
+__device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
+{
+    using Z = Fz<S>;
+    using P = Set<S>;
+    constexpr int M = Z::M, T = Z::T, TWP = Z::TWP, NW = P::NW;
+    const FusedArgs &a = *rc.a;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int rem = (int)rc.tile.count - warp * 32;
+    const int ntile = rem < 0 ? 0 : (rem > 32 ? 32 : rem);
+
+    uint32_t *tabbuf = reinterpret_cast<uint32_t *>(smem);
+    uint8_t *wbase = smem + 2 * Z::TAB_B + warp * Z::WARP_B;
+    uint8_t *raw = wbase;                                            // phase 1-2
+    uint32_t *ring = reinterpret_cast<uint32_t *>(wbase);            // phase 4
+    uint32_t *masks = reinterpret_cast<uint32_t *>(wbase);           // phase 5
+    uint32_t *sS = reinterpret_cast<uint32_t *>(wbase + Z::A_B);     // phase 3-4
+    uint32_t *sC = sS;                                               // phase 4-5
+    const uint32_t *tab = rc.key.tab;
+
+    // ---- 1. stage ciphertexts --------------------------------------------
+    if (!a.order && ntile == 32) {
+        const uint8_t *src = a.cts + ct_index(rc, warp, 0) * P::CT;
+        if ((((uintptr_t)src) & 15) == 0) {
+            for (int v = lane; v < Z::RAW_B / 16; v += 32)
+                reinterpret_cast<uint4 *>(raw)[v] = __ldg(reinterpret_cast<const uint4 *>(src) + v);
+        } else {
+            for (int v = lane; v < Z::RAW_B; v += 32)
+                raw[v] = src[v];
+        }
+    } else {
+        for (int q = 0; q < ntile; q++) {
+            const uint64_t c = ct_index(rc, warp, q);
+            const uint8_t *src = a.cts + (a.ct_off ? a.ct_off[c] : c * (uint64_t)P::CT);
+            for (int v = lane; v < P::CT; v += 32)
+                raw[q * P::CT + v] = src[v];
+        }
+        for (int v = ntile * P::CT + lane; v < Z::RAW_B; v += 32)
+            raw[v] = 0;
+    }
+    if (lane < 4)
+        reinterpret_cast<uint32_t *>(raw + Z::RAW_B)[lane] = 0;  // tail read by ld_u32_any
+    __syncwarp();
+
+    // ---- 2. syndrome -----------------------------------------------------
+    uint32_t acc[T];
+#pragma unroll
+    for (int w = 0; w < T; w++)
+        acc[w] = 0;
+    constexpr int NCHUNK = P::SB / TAB_ROWS;
+    constexpr int CHUNK_V = TAB_ROWS * TWP / 4;  // 16-byte pieces per chunk
+    {
+        const uint32_t *src = tab;
+        for (int v = tid; v < CHUNK_V; v += WPB * 32)
+            cp_async16(tabbuf + 4 * v, src + 4 * v);
+        cp_async_commit();
+    }
+    const uint8_t *myct = raw + lane * P::CT;
+    uint32_t ctw = 0;
+    for (int c = 0; c < NCHUNK; c++) {
+        if (c + 1 < NCHUNK) {
+            const uint32_t *src = tab + (size_t)(c + 1) * TAB_ROWS * TWP;
+            uint32_t *dst = tabbuf + ((c + 1) & 1) * TAB_ROWS * TWP;
+            for (int v = tid; v < CHUNK_V; v += WPB * 32)
+                cp_async16(dst + 4 * v, src + 4 * v);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const uint32_t *buf = tabbuf + (c & 1) * TAB_ROWS * TWP;
+#pragma unroll 1
+        for (int r = 0; r < TAB_ROWS; r++) {
+            const int b = c * TAB_ROWS + r;
+            if ((b & 31) == 0)
+                ctw = ld_u32_any(myct + (b >> 3));
+            const uint32_t mask = (uint32_t)((int32_t)(ctw << (31 - (b & 31))) >> 31);
+            const uint4 *row = reinterpret_cast<const uint4 *>(buf + r * TWP);
+#pragma unroll
+            for (int v = 0; v < TWP / 4; v++) {
+                const uint4 x = row[v];
+                if (4 * v + 0 < T) acc[4 * v + 0] ^= x.x & mask;
+                if (4 * v + 1 < T) acc[4 * v + 1] ^= x.y & mask;
+                if (4 * v + 2 < T) acc[4 * v + 2] ^= x.z & mask;
+                if (4 * v + 3 < T) acc[4 * v + 3] ^= x.w & mask;
+            }
+        }
+        __syncthreads();
+    }
+    if (ntile == 0)
+        return;  // no work for this warp in this round (the CTA-wide part is done)
+
+    // ---- 3. transpose: sS[j*M + k] bit q = bit k of syndrome j of ct q ----
+#pragma unroll
+    for (int w = 0; w < T; w++) {
+#pragma unroll 1
+        for (int h = 0; h < 2; h++) {
+            const int j = 2 * w + h;
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const uint32_t v = __ballot_sync(FULLMASK, (acc[w] >> (16 * h + k)) & 1u);
+                if (lane == ((j * M + k) & 31))
+                    sS[j * M + k] = v;
+            }
+        }
+    }
+    __syncwarp();
+
+    // ---- 4. Berlekamp-Massey, bitsliced across the 32 ciphertexts --------
+    {
+        constexpr int NJ = Z::NJ, R = Z::RING;
+        uint32_t C[NJ][M];
+#pragma unroll
+        for (int j = 0; j < NJ; j++)
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                C[j][k] = (j == 0 && k == 0 && lane == 0) ? FULLMASK : 0u;
+        for (int v = lane; v < R * M; v += 32)
+            ring[v] = (v == M) ? FULLMASK : 0u;  // B = x
+        uint32_t binv[M];
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            binv[k] = k == 0 ? FULLMASK : 0u;     // 1/b with b = 1
+        int Lq = 0;                               // L of ciphertext `lane`
+        __syncwarp();
+#pragma unroll 1
+        for (int N = 0; N < 2 * T; N++) {
+            const int lim = N < T ? N : T;
+            uint32_t p[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+#pragma unroll
+            for (int j = 0; j < NJ; j++) {
+                const int i = lane + 32 * j;
+                if (i <= lim) {
+                    const uint32_t *sv = sS + (N - i) * M;
+                    uint32_t s[M];
+#pragma unroll
+                    for (int k = 0; k < M; k++)
+                        s[k] = sv[k];
+                    bs_mul_acc<M>(p, C[j], s);
+                }
+            }
+            bs_reduce<M>(p);
+            uint32_t d[M];
+            uint32_t mne = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                uint32_t v = p[k];
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                    v ^= __shfl_xor_sync(FULLMASK, v, off);
+                d[k] = v;
+                mne |= v;
+            }
+            const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
+            const uint32_t mle = __ballot_sync(FULLMASK, my_mle);
+            Lq = my_mle ? N + 1 - Lq : Lq;
+            uint32_t f[M], dinv[M];
+            bs_mul<M>(f, d, binv);        // f = d / b (0 where d = 0)
+            bs_inv<M>(dinv, d);
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                binv[k] = (binv[k] & ~mle) | (dinv[k] & mle);
+            int off = (R - (N % R)) % R;  // slot(i) = (i - N) mod R
+#pragma unroll
+            for (int j = 0; j < NJ; j++) {
+                const int i = lane + 32 * j;
+                if (i <= T) {
+                    int slot = i + off;
+                    slot = slot >= R ? slot - R : slot;
+                    uint32_t *bp = ring + slot * M;
+                    uint32_t bv[M], tv[M];
+#pragma unroll
+                    for (int k = 0; k < M; k++)
+                        bv[k] = bp[k];
+                    bs_mul<M>(tv, f, bv);
+#pragma unroll
+                    for (int k = 0; k < M; k++) {
+                        const uint32_t oc = C[j][k];
+                        C[j][k] = oc ^ tv[k];
+                        bp[k] = (bv[k] & ~mle) | (oc & mle);
+                    }
+                }
+            }
+            // Slot of B_{t+1} at this N becomes B_0 = 0 at N+1.
+            const int freeslot = (R - ((N + 1) % R)) % R;
+            if (lane < M)
+                ring[freeslot * M + lane] = 0;
+            __syncwarp();
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+            const int i = lane + 32 * j;
+            if (i <= T)
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    sC[i * M + k] = C[j][k];
+        }
+        __syncwarp();
+    }
+
+    // ---- 5. root search + pack, one ciphertext at a time ------------------
+    const uint32_t *Lbs = rc.key.Lbs;
+    for (int q = 0; q < ntile; q++) {
+        for (int v = lane; v < (T + 1) * M; v += 32) {
+            const int i = v / M, k = v - (v / M) * M;
+            masks[i * 16 + k] = 0u - ((sC[v] >> q) & 1u);
+        }
+        __syncwarp();
+        const uint64_t c = ct_index(rc, warp, q);
+        uint32_t *erow = a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride);
+        int cnt = 0;
+        for (int w = lane; w < NW; w += 32) {
+            uint32_t av[M], r[M];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                av[k] = __ldg(Lbs + k * NW + w);
+                r[k] = masks[k];  // coefficient C[0] = f[t]
+            }
+#pragma unroll 1
+            for (int i = 1; i <= T; i++) {
+                uint32_t p[2 * M - 1];
+                const uint32_t *mrow = masks + i * 16;
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    p[k] = k < M ? mrow[k] : 0u;
+                bs_mul_acc<M>(p, r, av);
+                bs_reduce<M>(p);
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    r[k] = p[k];
+            }
+            uint32_t any = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                any |= r[k];
+            const int left = P::N - 32 * w;
+            const uint32_t valid = left >= 32 ? FULLMASK : ((1u << left) - 1u);
+            const uint32_t z = ~any & valid;
+            erow[w] = z;
+            cnt += __popc(z);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+            cnt += __shfl_xor_sync(FULLMASK, cnt, off);
+        if (lane == 0 && a.weight)
+            a.weight[c] = (uint16_t)cnt;
+        __syncwarp();
+    }
+}
+
+template <int SETMASK, int WPB>
+__global__ void __launch_bounds__(WPB * 32, 1) k_fused(FusedArgs a)
+{
+    extern __shared__ __align__(16) uint8_t smem[];
+    __shared__ uint32_t s_round;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            s_round = atomicAdd(a.tile_counter, 1u);
+        __syncthreads();
+        const uint32_t r = s_round;
+        if (r >= a.ntiles)
+            return;
+        RoundCtx rc;
+        rc.a = &a;
+        if (a.tiles) {
+            rc.tile = a.tiles[r];
+            rc.key = a.keys[rc.tile.key];
+        } else {
+            const uint64_t first = (uint64_t)r * a.round_cts;
+            const uint64_t left = a.total - first;
+            rc.tile = FusedTile{0u, (uint32_t)(left < a.round_cts ? left : a.round_cts), first};
+            rc.key = a.key0;
+        }
+        const int set = a.single_set >= 0 ? a.single_set : rc.key.set;
+        if ((SETMASK & (1 << S348864)) && set == S348864)
+            fused_round<S348864, WPB>(rc, smem);
+        else if ((SETMASK & (1 << S460896)) && set == S460896)
+            fused_round<S460896, WPB>(rc, smem);
+        else if ((SETMASK & (1 << S6688128)) && set == S6688128)
+            fused_round<S6688128, WPB>(rc, smem);
+        else if ((SETMASK & (1 << S6960119)) && set == S6960119)
+            fused_round<S6960119, WPB>(rc, smem);
+        else if ((SETMASK & (1 << S8192128)) && set == S8192128)
+            fused_round<S8192128, WPB>(rc, smem);
+    }
+}
+
+template <int S> constexpr size_t fz_smem(int wpb) { return 2 * (size_t)Fz<S>::TAB_B + (size_t)wpb * Fz<S>::WARP_B; }
+
+size_t smem_limit_bytes();
+
+// Per-instantiation launch and occupancy helpers (one translation unit per
+// set mask, so the instantiations compile in parallel).
+template <int SETMASK, int WPB> cudaError_t launch_k(const FusedArgs &a, int grid, size_t smem, cudaStream_t s)
+{
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(k_fused<SETMASK, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem_limit_bytes());
+        if (e != cudaSuccess)
+            return e;
+        attr_done = true;
+    }
+    k_fused<SETMASK, WPB><<<grid, WPB * 32, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int SETMASK, int WPB> int occupancy(size_t smem)
+{
+    cudaFuncSetAttribute(k_fused<SETMASK, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem_limit_bytes());
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<SETMASK, WPB>, WPB * 32, smem) != cudaSuccess)
+        return 1;
+    return n;
+}
+
+// Entry points defined in fused_m<mask>.cu.
+#define CMD_FUSED_DECL(MASK)                                                              \
+    cudaError_t fused_launch_##MASK(const FusedArgs &a, int grid, int wpb, size_t smem, cudaStream_t s); \
+    int fused_occ_##MASK(int wpb, size_t smem);
+CMD_FUSED_DECL(1)
+CMD_FUSED_DECL(2)
+CMD_FUSED_DECL(4)
+CMD_FUSED_DECL(8)
+CMD_FUSED_DECL(16)
+CMD_FUSED_DECL(31)
+#undef CMD_FUSED_DECL
+
+}  // namespace cmd

@@ -1,0 +1,90 @@
+// Engine-internal declarations shared by the CUDA launchers and the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "cmd_b200.h"
+#include "params.h"
+
+namespace cmd {
+
+// Device-resident expanded key: one allocation carved into these arrays.
+struct KeyDev {
+    int set = 0;
+    uint16_t *L = nullptr;      // support, n entries (support_gen output)
+    uint16_t *g = nullptr;      // Goppa polynomial, t+1 coefficients, g[t] = 1
+    uint16_t *ginv2 = nullptr;  // 1/g(L_i)^2 for i < n (0 where g(L_i) = 0)
+    uint32_t *tab = nullptr;    // syndrome table, sb rows of twp (t rounded up to
+                                // 4) words; word w < t of row b packs
+                                // L_b^{2w}/g^2 (low) and L_b^{2w+1}/g^2 (high):
+                                // util.c:86-100 values, rows 16-byte aligned
+    uint32_t *Lbs = nullptr;    // bitsliced support, plane-major [m][nw]:
+                                // bit p of Lbs[k*nw+w] = bit k of L[32w+p]
+    uint8_t *sk = nullptr;      // device copy of the secret key bytes
+};
+
+// Records a launch against an engine counter (count of our kernels).
+struct LaunchCounter {
+    std::atomic<uint64_t> *ctr;
+    void bump(uint64_t n = 1) const
+    {
+        if (ctr)
+            ctr->fetch_add(n, std::memory_order_relaxed);
+    }
+};
+
+cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc);
+
+cudaError_t launch_synd_plain(const KeyDev &k, const uint8_t *d_cts, size_t count,
+                              uint32_t *d_synd, cudaStream_t s, LaunchCounter lc);
+cudaError_t launch_bm_plain(int set, const uint16_t *d_synd, size_t count, uint16_t *d_loc,
+                            cudaStream_t s, LaunchCounter lc);
+cudaError_t launch_root_plain(const KeyDev &k, const uint16_t *d_loc, size_t count,
+                              uint32_t *d_err, uint16_t *d_weight, cudaStream_t s,
+                              LaunchCounter lc, int num_sms);
+cudaError_t launch_root_images(const KeyDev &k, const uint16_t *d_loc, size_t count,
+                               uint16_t *d_images, cudaStream_t s, LaunchCounter lc);
+
+// Fused path: one work item = up to 32 ciphertexts of one key.
+struct FusedTile {
+    uint32_t key;     // index into the key table
+    uint32_t count;   // 1..32
+    uint64_t first;   // index of the first ciphertext of the tile in the
+                      // ciphertext index list (mixed) or the batch (single)
+};
+struct FusedKeyRef {
+    int32_t set;
+    int32_t pad;
+    const uint32_t *tab;
+    const uint32_t *Lbs;
+};
+struct FusedArgs {
+    const FusedTile *tiles;        // device list of rounds; null = implicit
+                                   // rounds over one key: round r covers
+                                   // ciphertexts [r*round_cts, +round_cts)
+    uint32_t ntiles;               // number of rounds
+    uint32_t round_cts;            // implicit mode: ciphertexts per round
+    uint64_t total;                // implicit mode: batch size
+    const FusedKeyRef *keys;       // device key table (null in implicit mode)
+    FusedKeyRef key0;              // implicit mode: the one key
+    const uint8_t *cts;            // ciphertext base pointer
+    const uint64_t *ct_off;        // per-ciphertext byte offsets, or null
+    const uint64_t *err_off;       // per-ciphertext error-row word offsets, or null
+    const uint32_t *order;         // ciphertext index per round slot, or null
+    uint32_t *err;
+    uint16_t *weight;
+    uint32_t *tile_counter;        // zeroed before the launch
+    int single_set;                // >= 0: every round has this set
+    uint32_t err_stride;           // words per error row when err_off is null
+};
+cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,
+                         LaunchCounter lc);
+
+void set_last_error(const std::string &msg);
+
+}  // namespace cmd

@@ -1,0 +1,208 @@
+/*
+ * cmd_b200.h -- C ABI of the B200 (sm_100a) batched Classic McEliece
+ * decryption engine.  A drop-in for the decrypt path of somesh-vas/CM_Decrypt_:
+ * it reads the same sk_<set>.bin / ct_<set>.bin fixtures and produces the same
+ * errorstream0_<set>.bin text, bit-exact with the reference CPU/ decoder,
+ * decode failures included.
+ *
+ * The reference has no library API; its boundary is (i) the per-set CLI
+ * `decrypt_<set> [KATNUM]` (CPU/param/param6960119/src/decrypt.c:109-218) with
+ * fixed relative file paths, and (ii) the internal function trio synd/bm/root
+ * over globals set up by initialisation()/compute_inverses()
+ * (CPU/include/common/root.h:8-23, bm.h:14).  Each entry point below names the
+ * reference interface it replaces.  Plain pointers and sizes only; status
+ * codes, never exit().  Device pointers are marked d_*, host pointers h_*.
+ * Streams are passed as void* (a cudaStream_t; NULL = the engine's stream).
+ */
+#ifndef CMD_B200_H
+#define CMD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+/* 0 / -1 / -4 keep the reference's values (CPU/param/param6960119/include/
+ * common.h:10-12: KAT_SUCCESS, KAT_FILE_OPEN_ERROR, KAT_CRYPTO_FAILURE). */
+#define CMD_OK             0
+#define CMD_E_FILE        -1  /* file missing, short, or unwritable          */
+#define CMD_E_ARG         -4  /* bad argument (size, count, set, pointer)     */
+#define CMD_E_CUDA        -5  /* a CUDA call failed; see cmd_last_error()     */
+#define CMD_E_NOMEM       -6  /* host or device allocation failed             */
+#define CMD_E_BUDGET      -7  /* refused: would exceed the engine HBM budget  */
+#define CMD_E_BUSY        -8  /* serving queue full                           */
+#define CMD_E_TIMEOUT     -9  /* a bounded wait gave up                       */
+#define CMD_E_NODEVICE   -10  /* no CUDA device / kernels not loadable        */
+
+/* ---- parameter sets (CPU/param/param<set>/include/common.h) ----------- */
+typedef enum {
+    CMD_348864 = 0,
+    CMD_460896 = 1,
+    CMD_6688128 = 2,
+    CMD_6960119 = 3,
+    CMD_8192128 = 4,
+    CMD_NUM_SETS = 5
+} cmd_set;
+
+typedef struct {
+    int32_t set_id;     /* 348864 ... 8192128                              */
+    int32_t m;          /* GFBITS                                          */
+    int32_t n;          /* SYS_N (support size = error-vector bits)        */
+    int32_t t;          /* SYS_T                                           */
+    int32_t ct_bytes;   /* crypto_kem_CIPHERTEXTBYTES (= SYND_BYTES)       */
+    int32_t sk_bytes;   /* crypto_kem_SECRETKEYBYTES                       */
+    int32_t sb;         /* 8*SYND_BYTES ciphertext bits used by synd()      */
+    int32_t err_bytes;  /* n/8: bytes of one packed error vector           */
+    int32_t err_words;  /* ceil(n/32): 32-bit words of one device error row */
+} cmd_set_info;
+
+/* Replaces the compile-time #defines of common.h with a runtime table. */
+int cmd_set_info_get(cmd_set set, cmd_set_info *out);
+/* "348864", "mceliece6960119", ... -> set.  CMD_E_ARG if unknown. */
+int cmd_set_from_name(const char *name, cmd_set *out);
+
+/* ---- engine ------------------------------------------------------------ */
+typedef struct cmd_engine cmd_engine;
+typedef struct cmd_key cmd_key;
+
+/* One engine per GPU.  hbm_budget_bytes caps the device memory the engine
+ * holds for keys and batch buffers (0 = 80% of free memory at creation). */
+int cmd_engine_create(int device, size_t hbm_budget_bytes, cmd_engine **out);
+void cmd_engine_destroy(cmd_engine *eng);
+/* Bytes currently charged against the budget, and the budget itself. */
+int cmd_engine_memory(const cmd_engine *eng, size_t *used, size_t *budget);
+/* Text of the last error on this thread ("" if none). */
+const char *cmd_last_error(void);
+/* Kernel launches issued by this engine since creation (all streams). */
+uint64_t cmd_engine_launch_count(const cmd_engine *eng);
+
+/* ---- keys: secret-key expansion on the device ------------------------- */
+/* Replaces initialisation() + support_gen() + compute_inverses()
+ * (CPU/param/param6960119/src/util.c:60-100, CPU/src/common/root_13.c:181-211).
+ * Parses sk (exactly sk_bytes), runs the Benes network, evaluates g on the
+ * support and builds the device-resident tables: support L, 1/g(L_i)^2, the
+ * syndrome table and the bitsliced support used by the root search.
+ * CMD_E_BUDGET if the key does not fit the engine budget. */
+int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk,
+                   size_t sk_len, cmd_key **out);
+void cmd_key_free(cmd_key *key);
+int cmd_key_set(const cmd_key *key, cmd_set *out);
+size_t cmd_key_device_bytes(const cmd_key *key);
+/* Parity hooks: copy the device-resident support L[n] (support_gen output),
+ * Goppa g[t+1] and syndrome table [sb][2t] (inverse_elements) to the host. */
+int cmd_key_support(const cmd_key *key, uint16_t *h_L, size_t n);
+int cmd_key_goppa(const cmd_key *key, uint16_t *h_g, size_t t_plus_1);
+int cmd_key_synd_table(const cmd_key *key, uint16_t *h_tab, size_t entries);
+
+/* ---- batched decrypt --------------------------------------------------- */
+/* Path selector: CMD_PATH_PLAIN runs the three per-stage kernels (syndrome,
+ * Berlekamp-Massey, root search + pack); CMD_PATH_FUSED runs the fused
+ * bitsliced kernel; CMD_PATH_AUTO lets the engine's tuner choose. */
+typedef enum { CMD_PATH_AUTO = 0, CMD_PATH_PLAIN = 1, CMD_PATH_FUSED = 2 } cmd_path;
+
+/* Replaces the per-ciphertext loop memcpy -> synd -> bm -> root ->
+ * build_error_vector (CPU/param/param6960119/src/decrypt.c:163-177, 43-53).
+ * h_cts: count * ct_bytes, raw concatenation (the ct_<set>.bin layout).
+ * h_err: count * err_bytes; bit i of vector c is set iff position i is flagged
+ * (the reference's error_vector layout).  h_weight (may be NULL): flagged
+ * positions per ciphertext.  Synchronous; host buffers may be pageable. */
+int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path,
+                      const uint8_t *h_cts, size_t count, uint8_t *h_err,
+                      uint16_t *h_weight);
+
+/* Device-resident form: d_cts as above; d_err is count rows of err_words
+ * 32-bit words (little-endian, so the first err_bytes bytes of a row equal the
+ * host layout; bits >= n are zero).  Asynchronous on `stream`. */
+int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path,
+                       const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                       uint16_t *d_weight, void *stream);
+
+/* Mixed batch in one launch: ciphertext c belongs to keys[h_key_idx[c]]; its
+ * bytes start at d_cts + h_ct_off[c] and its error row at
+ * d_err + h_err_off[c] (in 32-bit words).  Keys may be of different sets.
+ * Always runs the fused kernel.  Asynchronous on `stream`. */
+int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *keys,
+                             size_t nkeys, const uint32_t *h_key_idx,
+                             const uint8_t *d_cts, const uint64_t *h_ct_off,
+                             size_t count, uint32_t *d_err,
+                             const uint64_t *h_err_off, uint16_t *d_weight,
+                             void *stream);
+
+/* ---- per-stage parity hooks (device buffers, asynchronous) ------------- */
+/* synd(): d_synd = count rows of 2t u16 (CPU/param/param6960119/src/
+ * util.c:102-114). */
+int cmd_stage_synd(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
+                   size_t count, uint16_t *d_synd, void *stream);
+/* bm(): d_loc = count rows of t+1 u16, reversed as bm() writes them
+ * (CPU/src/common/bm.c:12-68). */
+int cmd_stage_bm(cmd_engine *eng, cmd_set set, const uint16_t *d_synd,
+                 size_t count, uint16_t *d_loc, void *stream);
+/* root() + build_error_vector: flagged-position rows (err_words words) and
+ * weights from locators (CPU/src/common/root_13.c:233-240, decrypt.c:43-53). */
+int cmd_stage_root(cmd_engine *eng, const cmd_key *key, const uint16_t *d_loc,
+                   size_t count, uint32_t *d_err, uint16_t *d_weight,
+                   void *stream);
+/* root() images themselves: count rows of n u16 (for stage-level diffs). */
+int cmd_stage_root_images(cmd_engine *eng, const cmd_key *key,
+                          const uint16_t *d_loc, size_t count,
+                          uint16_t *d_images, void *stream);
+
+/* ---- errorstream (text) ------------------------------------------------ */
+/* write_error_positions (CPU/param/param6960119/src/decrypt.c:55-66): one
+ * line per vector, " %d" per flagged position ascending, then '\n'.
+ * Returns CMD_OK and the byte count in *out_len; CMD_E_ARG if cap is short
+ * (with *out_len = bytes needed). */
+int cmd_errorstream_format(cmd_set set, const uint8_t *h_err, size_t count,
+                           char *out, size_t cap, size_t *out_len);
+/* Writes (append != 0: appends) the text to path.  CMD_E_FILE on failure. */
+int cmd_errorstream_write(cmd_set set, const uint8_t *h_err, size_t count,
+                          const char *path, int append);
+
+/* ---- file contract ----------------------------------------------------- */
+/* Replaces `decrypt_<set> KATNUM` (decrypt.c:109-218): reads one sk
+ * (sk_bytes) and katnum ciphertexts from the given files, decrypts on the GPU
+ * and writes the errorstream.  CMD_E_FILE (-1) if a file is missing or short,
+ * CMD_E_ARG (-4) for katnum == 0.  *out_seconds (may be NULL) receives the
+ * device decrypt time. */
+int cmd_decrypt_files(cmd_engine *eng, cmd_set set, const char *sk_path,
+                      const char *ct_path, size_t katnum,
+                      const char *errorstream_path, cmd_path path,
+                      double *out_seconds);
+
+/* ---- measurement (no reference counterpart) ---------------------------- */
+/* Integer-ALU roofline denominator: the device's sustained lop3.b32 rate in
+ * lane-operations per second (32 per warp instruction), measured with
+ * independent dependency chains on every SM. */
+int cmd_bench_int_peak(cmd_engine *eng, double *lop3_lane_ops_per_s);
+
+/* ---- synthetic workloads (no reference counterpart: fixture tooling) --- */
+/* Derives a secret key for `set` from a 64-bit seed: the Goppa polynomial of
+ * the base key h_base_sk translated by a seed-chosen field element (which
+ * keeps it irreducible) and fresh seed-drawn Benes control bits, retried
+ * until the first mt support columns form an invertible block.  h_sk_out
+ * receives sk_bytes.  h_base_sk may be NULL for set 0..4 built-in bases. */
+int cmd_synth_key(cmd_set set, const uint8_t *h_base_sk, uint64_t seed,
+                  uint8_t *h_sk_out);
+/* Public data for encryption: the systematic parity-check matrix built from
+ * sk; opaque handle. */
+typedef struct cmd_pubkey cmd_pubkey;
+int cmd_synth_pubkey(cmd_set set, const uint8_t *h_sk, cmd_pubkey **out);
+void cmd_synth_pubkey_free(cmd_pubkey *pk);
+/* count ciphertexts: ciphertext i is valid (an error vector of weight exactly
+ * t, positions uniform over [0,n), seeded by (seed, i)) unless
+ * i is drawn malformed with probability malformed_permille/1000, in which case
+ * it is a uniform random mt-bit string (padding bits zero).  h_err_out (may be
+ * NULL) gets the planted error vectors (all-zero rows for malformed ones),
+ * h_valid_out (may be NULL) 1/0 per ciphertext. */
+int cmd_synth_ciphertexts(const cmd_pubkey *pk, uint64_t seed, size_t count,
+                          uint32_t malformed_permille, uint8_t *h_cts_out,
+                          uint8_t *h_err_out, uint8_t *h_valid_out,
+                          int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CMD_B200_H */

@@ -1,0 +1,222 @@
+"""ctypes front-end to the two CPU checkers in this directory.
+
+TEST INFRASTRUCTURE ONLY.  ``Oracle`` wraps liboracle.so (the C restatement
+of the reference decrypt path, cmd_oracle.c); ``RefLib`` wraps
+_ref/libref_<set>.so (the reference's own CPU/ sources behind ref_harness.c).
+Only tests/, the smoke entry point and bench.py's CPU-baseline leg use them.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SETS = (348864, 460896, 6688128, 6960119, 8192128)
+
+_u16p = ctypes.POINTER(ctypes.c_uint16)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def _ptr(a: np.ndarray, typ):
+    return a.ctypes.data_as(typ)
+
+
+class Params(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int) for name in
+                ("set_id", "m", "n", "t", "ct_bytes", "sk_bytes", "sb", "cond_bytes")]
+
+
+def build(with_reference: bool | None = None) -> None:
+    """Compile liboracle.so and, when the reference tree is mounted, _ref/."""
+    ref_dir = os.environ.get("CMD_REFERENCE_DIR", "/root/reference")
+    targets = ["oracle"]
+    if with_reference or (with_reference is None and os.path.isdir(os.path.join(ref_dir, "CPU"))):
+        targets.append("ref")
+    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}", *targets], check=True)
+
+
+class Oracle:
+    """The C restatement (cmd_oracle.c), runtime-parameterised by set id."""
+
+    def __init__(self, set_id: int):
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build(with_reference=False)
+        self.lib = lib = ctypes.CDLL(path)
+        lib.o_gf_mul.restype = ctypes.c_uint16
+        lib.o_gf_inv.restype = ctypes.c_uint16
+        lib.o_gf_frac.restype = ctypes.c_uint16
+        lib.o_errorstream_format.restype = ctypes.c_long
+        self.p = Params()
+        if lib.o_params_get(int(set_id), ctypes.byref(self.p)) != 0:
+            raise ValueError(f"unknown parameter set {set_id}")
+        self.set_id = set_id
+        self.m, self.n, self.t = self.p.m, self.p.n, self.p.t
+        self.ct_bytes, self.sk_bytes, self.sb = self.p.ct_bytes, self.p.sk_bytes, self.p.sb
+        self._key = None
+
+    # -- field ------------------------------------------------------------
+    def gf_mul(self, a: int, b: int) -> int:
+        return self.lib.o_gf_mul(self.m, a, b)
+
+    def gf_frac(self, den: int, num: int) -> int:
+        return self.lib.o_gf_frac(self.m, den, num)
+
+    def gf_mul_row(self, a: int) -> np.ndarray:
+        out = np.zeros(1 << self.m, np.uint16)
+        self.lib.o_gf_mul_row(self.m, a, _ptr(out, _u16p))
+        return out
+
+    def gf_frac_row(self, num: int) -> np.ndarray:
+        out = np.zeros(1 << self.m, np.uint16)
+        self.lib.o_gf_frac_row(self.m, num, _ptr(out, _u16p))
+        return out
+
+    # -- key --------------------------------------------------------------
+    def support_from_cond(self, cond: bytes) -> np.ndarray:
+        c = np.frombuffer(bytes(cond), np.uint8).copy()
+        out = np.zeros(self.n, np.uint16)
+        if self.lib.o_support_gen(ctypes.byref(self.p), _ptr(c, _u8p), _ptr(out, _u16p)):
+            raise MemoryError
+        return out
+
+    def expand(self, sk: bytes):
+        """Returns (g[t+1], L[n], inv_tab[sb, 2t])."""
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        g = np.zeros(self.t + 1, np.uint16)
+        L = np.zeros(self.n, np.uint16)
+        tab = np.zeros((self.sb, 2 * self.t), np.uint16)
+        if self.lib.o_key_expand(ctypes.byref(self.p), _ptr(skb, _u8p), _ptr(g, _u16p),
+                                 _ptr(L, _u16p), _ptr(tab, _u16p)):
+            raise MemoryError
+        self._key = (g, L, tab)
+        return g, L, tab
+
+    # -- stages -------------------------------------------------------------
+    def synd(self, ct: bytes, tab: np.ndarray | None = None) -> np.ndarray:
+        tab = self._key[2] if tab is None else tab
+        c = np.frombuffer(bytes(ct), np.uint8).copy()
+        s = np.zeros(2 * self.t, np.uint16)
+        self.lib.o_synd(ctypes.byref(self.p), _ptr(np.ascontiguousarray(tab), _u16p),
+                        _ptr(c, _u8p), _ptr(s, _u16p))
+        return s
+
+    def bm(self, s: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(s, np.uint16)
+        loc = np.zeros(self.t + 1, np.uint16)
+        self.lib.o_bm(ctypes.byref(self.p), _ptr(s, _u16p), _ptr(loc, _u16p))
+        return loc
+
+    def root(self, loc: np.ndarray, L: np.ndarray | None = None) -> np.ndarray:
+        L = self._key[1] if L is None else L
+        loc = np.ascontiguousarray(loc, np.uint16)
+        L = np.ascontiguousarray(L, np.uint16)
+        out = np.zeros(self.n, np.uint16)
+        self.lib.o_root(ctypes.byref(self.p), _ptr(loc, _u16p), _ptr(L, _u16p), _ptr(out, _u16p))
+        return out
+
+    def decrypt(self, sk: bytes, cts: np.ndarray, nthreads: int = 1) -> np.ndarray:
+        """cts: uint8 [count, ct_bytes] -> error bytes uint8 [count, n/8]."""
+        cts = np.ascontiguousarray(cts, np.uint8).reshape(-1, self.ct_bytes)
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        err = np.zeros((cts.shape[0], self.n // 8), np.uint8)
+        rc = self.lib.o_decrypt_batch(ctypes.byref(self.p), _ptr(skb, _u8p), _ptr(cts, _u8p),
+                                      ctypes.c_size_t(cts.shape[0]), _ptr(err, _u8p), nthreads)
+        if rc:
+            raise RuntimeError("oracle decrypt failed")
+        return err
+
+    def errorstream(self, err: np.ndarray) -> bytes:
+        err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n // 8)
+        cap = err.shape[0] * (1 + 6 * self.n // 8 * 8) + 16
+        buf = ctypes.create_string_buffer(cap)
+        got = self.lib.o_errorstream_format(ctypes.byref(self.p), _ptr(err, _u8p),
+                                            ctypes.c_size_t(err.shape[0]), buf, ctypes.c_size_t(cap))
+        if got < 0:
+            raise RuntimeError("errorstream buffer too small")
+        return buf.raw[:got]
+
+
+class RefLib:
+    """The reference's own CPU/ decoder for one set (oracle/_ref/libref_<set>.so)."""
+
+    def __init__(self, set_id: int):
+        path = os.path.join(HERE, "_ref", f"libref_{set_id}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = lib = ctypes.CDLL(path)
+        for name in ("ref_gf_mul", "ref_gf_frac", "ref_gf_inv", "ref_bitrev"):
+            getattr(lib, name).restype = ctypes.c_uint16
+        info = (ctypes.c_int * 6)()
+        lib.ref_info(info)
+        self.m, self.n, self.t, self.ct_bytes, self.sk_bytes, self.sb = list(info)
+        self.set_id = set_id
+
+    @staticmethod
+    def available(set_id: int) -> bool:
+        return os.path.exists(os.path.join(HERE, "_ref", f"libref_{set_id}.so"))
+
+    def load_sk(self, sk: bytes) -> None:
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        self.lib.ref_load_sk(_ptr(skb, _u8p))
+
+    def support(self) -> np.ndarray:
+        out = np.zeros(self.n, np.uint16)
+        self.lib.ref_get_support(_ptr(out, _u16p))
+        return out
+
+    def goppa(self) -> np.ndarray:
+        out = np.zeros(self.t + 1, np.uint16)
+        self.lib.ref_get_goppa(_ptr(out, _u16p))
+        return out
+
+    def inverse_table(self) -> np.ndarray:
+        out = np.zeros((self.sb, 2 * self.t), np.uint16)
+        self.lib.ref_get_inverse_table(_ptr(out, _u16p))
+        return out
+
+    def support_from_cond(self, cond: bytes) -> np.ndarray:
+        c = np.frombuffer(bytes(cond), np.uint8).copy()
+        out = np.zeros(self.n, np.uint16)
+        self.lib.ref_support_from_cond(_ptr(c, _u8p), _ptr(out, _u16p))
+        return out
+
+    def synd(self, ct: bytes) -> np.ndarray:
+        c = np.frombuffer(bytes(ct), np.uint8).copy()
+        s = np.zeros(2 * self.t, np.uint16)
+        self.lib.ref_synd(_ptr(c, _u8p), _ptr(s, _u16p))
+        return s
+
+    def bm(self, s: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(s, np.uint16)
+        loc = np.zeros(self.t + 1, np.uint16)
+        self.lib.ref_bm(_ptr(s, _u16p), _ptr(loc, _u16p))
+        return loc
+
+    def root(self, loc: np.ndarray) -> np.ndarray:
+        loc = np.ascontiguousarray(loc, np.uint16)
+        out = np.zeros(self.n, np.uint16)
+        self.lib.ref_root(_ptr(loc, _u16p), _ptr(out, _u16p))
+        return out
+
+    def gf_mul_row(self, a: int) -> np.ndarray:
+        out = np.zeros(1 << self.m, np.uint16)
+        self.lib.ref_gf_mul_row(a, _ptr(out, _u16p))
+        return out
+
+    def gf_frac_row(self, num: int) -> np.ndarray:
+        out = np.zeros(1 << self.m, np.uint16)
+        self.lib.ref_gf_frac_row(num, _ptr(out, _u16p))
+        return out
+
+    def decrypt(self, sk: bytes, cts: np.ndarray, nthreads: int = 1) -> np.ndarray:
+        self.load_sk(sk)
+        cts = np.ascontiguousarray(cts, np.uint8).reshape(-1, self.ct_bytes)
+        err = np.zeros((cts.shape[0], self.n // 8), np.uint8)
+        if self.lib.ref_decrypt_batch(_ptr(cts, _u8p), ctypes.c_size_t(cts.shape[0]),
+                                      _ptr(err, _u8p), nthreads):
+            raise RuntimeError("reference decrypt failed")
+        return err

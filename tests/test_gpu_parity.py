@@ -1,0 +1,243 @@
+"""GPU parity: the CUDA engine against the oracle, bit-exact, through the C ABI.
+
+Covers key expansion (support, Goppa polynomial, syndrome table), each stage
+in isolation (synd / bm / root images / root + pack), and whole decrypts on
+both kernel paths for every parameter set: the reference's own kem/ fixtures
+(errorstream byte-identical), synthetic valid weight-t ciphertexts (decode to
+the planted error vector), malformed random strings (the reference's failure
+outcome), ragged batch sizes, derived keys and mixed multi-key batches.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import numpy as np
+import pytest
+import torch
+
+import cm_decrypt__b200 as cmd
+from conftest import KEM, SETS, golden_ct, golden_errorstream, golden_sk, rng
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(a: np.ndarray) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def words_to_bytes(err_words: torch.Tensor, n: int) -> np.ndarray:
+    w = err_words.cpu().numpy().astype("<u4")
+    return w.view(np.uint8).reshape(w.shape[0], -1)[:, : n // 8]
+
+
+@pytest.fixture(scope="module")
+def keys(engine):
+    out = {s: cmd.Key(engine, s, golden_sk(s)) for s in SETS}
+    yield out
+    for k in out.values():
+        k.free()
+
+
+@pytest.mark.parametrize("s", SETS)
+def test_key_expansion(oracle_mod, keys, s):
+    g, L, tab = oracle_mod.Oracle(s).expand(golden_sk(s))
+    k = keys[s]
+    assert np.array_equal(k.goppa(), g)
+    assert np.array_equal(k.support(), L)
+    assert np.array_equal(k.synd_table(), tab)
+
+
+@pytest.mark.parametrize("s", SETS)
+def test_stages(oracle_mod, engine, keys, s):
+    o = oracle_mod.Oracle(s)
+    o.expand(golden_sk(s))
+    k = keys[s]
+    info = k.info
+    pk = cmd.PubKey(s, golden_sk(s))
+    valid, _, _ = pk.ciphertexts(seed=21, count=40)
+    junk = rng(s).integers(0, 256, (37, info.ct_bytes), dtype=np.uint8)
+    cts = np.concatenate([valid, junk])
+    n = cts.shape[0]
+    d_ct = dev(cts)
+    d_s = torch.zeros((n, 2 * info.t), dtype=torch.int16, device="cuda")
+    d_l = torch.zeros((n, info.t + 1), dtype=torch.int16, device="cuda")
+    d_img = torch.zeros((n, info.n), dtype=torch.int16, device="cuda")
+    d_e = torch.zeros((n, info.err_words), dtype=torch.int32, device="cuda")
+    d_w = torch.zeros(n, dtype=torch.int16, device="cuda")
+    cmd.synd(engine, k, d_ct.data_ptr(), n, d_s.data_ptr())
+    cmd.bm(engine, s, d_s.data_ptr(), n, d_l.data_ptr())
+    cmd.root_images(engine, k, d_l.data_ptr(), n, d_img.data_ptr())
+    cmd.root(engine, k, d_l.data_ptr(), n, d_e.data_ptr(), d_w.data_ptr())
+    torch.cuda.synchronize()
+    S = d_s.cpu().numpy().view(np.uint16)
+    Lc = d_l.cpu().numpy().view(np.uint16)
+    IMG = d_img.cpu().numpy().view(np.uint16)
+    E = words_to_bytes(d_e, info.n)
+    W = d_w.cpu().numpy().view(np.uint16)
+    for i in range(n):
+        ct = cts[i].tobytes()
+        s_ref = o.synd(ct)
+        assert np.array_equal(S[i], s_ref), ("synd", i)
+        l_ref = o.bm(s_ref)
+        assert np.array_equal(Lc[i], l_ref), ("bm", i)
+        img = o.root(l_ref)
+        assert np.array_equal(IMG[i], img), ("root", i)
+        ebits = np.zeros(info.err_bytes, np.uint8)
+        idx = np.nonzero(img == 0)[0]
+        np.bitwise_or.at(ebits, idx >> 3, (1 << (idx & 7)).astype(np.uint8))
+        assert np.array_equal(E[i], ebits), ("pack", i)
+        assert W[i] == idx.size
+    # padding bits of the last word stay zero
+    if info.n % 32:
+        tail = d_e[:, -1].cpu().numpy().astype(np.uint32) >> (info.n % 32)
+        assert not tail.any()
+
+
+@pytest.mark.parametrize("path", ["plain", "fused"])
+@pytest.mark.parametrize("s", SETS)
+def test_kem_fixture_errorstream(engine, keys, s, path):
+    info = keys[s].info
+    cts = np.frombuffer(golden_ct(s), np.uint8).reshape(-1, info.ct_bytes)
+    err, w = cmd.decrypt(engine, keys[s], cts, path=path)
+    assert cmd.errorstream(s, err) == golden_errorstream(s)
+
+
+@pytest.mark.parametrize("path", ["plain", "fused"])
+@pytest.mark.parametrize("s", SETS)
+def test_decrypt_vs_oracle(oracle_mod, engine, keys, s, path):
+    o = oracle_mod.Oracle(s)
+    info = keys[s].info
+    pk = cmd.PubKey(s, golden_sk(s))
+    for count, permille in ((1, 0), (33, 0), (300, 100), (97, 1000)):
+        cts, planted, valid = pk.ciphertexts(seed=1000 + count, count=count, malformed_permille=permille)
+        err, w = cmd.decrypt(engine, keys[s], cts, path=path)
+        ref = o.decrypt(golden_sk(s), cts, nthreads=8)
+        assert np.array_equal(err, ref), (count, permille)
+        assert np.array_equal(err[valid == 1], planted[valid == 1])
+        assert np.array_equal(w, np.unpackbits(ref, axis=1).sum(axis=1))
+        assert (w[valid == 1] == info.t).all()
+
+
+@pytest.mark.parametrize("s", [348864, 6960119])
+def test_derived_keys(oracle_mod, engine, s):
+    o = oracle_mod.Oracle(s)
+    for seed in (1, 2):
+        sk = cmd.synth_key(s, golden_sk(s), seed)
+        key = cmd.Key(engine, s, sk)
+        try:
+            g, L, tab = o.expand(sk)
+            assert np.array_equal(key.support(), L)
+            pk = cmd.PubKey(s, sk)
+            cts, planted, valid = pk.ciphertexts(seed=seed, count=70, malformed_permille=200)
+            for path in ("plain", "fused"):
+                err, _ = cmd.decrypt(engine, key, cts, path=path)
+                assert np.array_equal(err, o.decrypt(sk, cts, nthreads=8))
+        finally:
+            key.free()
+
+
+def test_mixed_batch(oracle_mod, engine):
+    """Ciphertexts of several keys and all five sets interleaved in one launch,
+    each in its own slot of a shared byte buffer and error buffer."""
+    g = rng(42)
+    ks, sks, pks = [], [], []
+    for s in SETS:
+        for seed in (0, 1):
+            sk = golden_sk(s) if seed == 0 else cmd.synth_key(s, golden_sk(s), seed)
+            ks.append(cmd.Key(engine, s, sk))
+            sks.append((s, sk))
+            pks.append(cmd.PubKey(s, sk))
+    try:
+        count = 700
+        key_idx = g.integers(0, len(ks), count).astype(np.uint32)
+        blobs = []
+        ct_off = np.zeros(count, np.uint64)
+        err_off = np.zeros(count, np.uint64)
+        off = woff = 0
+        for c in range(count):
+            s, _ = sks[key_idx[c]]
+            info = cmd.set_info(s)
+            ct, _, _ = pks[key_idx[c]].ciphertexts(seed=c, count=1, malformed_permille=100)
+            blobs.append(ct[0])
+            ct_off[c] = off
+            off += info.ct_bytes + int(g.integers(0, 5))   # ragged, unaligned placement
+            err_off[c] = woff
+            woff += info.err_words
+        buf = np.zeros(off + 16, np.uint8)
+        for c in range(count):
+            buf[int(ct_off[c]): int(ct_off[c]) + blobs[c].size] = blobs[c]
+        d_ct = dev(buf)
+        d_err = torch.zeros(woff, dtype=torch.int32, device="cuda")
+        d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+        cmd.decrypt_mixed_device(engine, ks, key_idx, d_ct.data_ptr(), ct_off, d_err.data_ptr(), err_off,
+                                 d_w.data_ptr())
+        torch.cuda.synchronize()
+        E = d_err.cpu().numpy().astype("<u4")
+        W = d_w.cpu().numpy().view(np.uint16)
+        for c in range(count):
+            s, sk = sks[key_idx[c]]
+            info = cmd.set_info(s)
+            o = oracle_mod.Oracle(s)
+            ct = buf[int(ct_off[c]): int(ct_off[c]) + info.ct_bytes]
+            ref = o.decrypt(sk, ct.reshape(1, -1))[0]
+            row = E[int(err_off[c]): int(err_off[c]) + info.err_words].view(np.uint8)[: info.err_bytes]
+            assert np.array_equal(row, ref), c
+            assert W[c] == int(np.unpackbits(ref).sum())
+    finally:
+        for k in ks:
+            k.free()
+
+
+@pytest.mark.parametrize("path", ["plain", "fused"])
+def test_full_size_properties(engine, keys, path):
+    """BASELINE-size batch at 6960119 (65,536 ciphertexts): every valid
+    ciphertext decodes to exactly its planted weight-119 error vector."""
+    s = 6960119
+    pk = cmd.PubKey(s, golden_sk(s))
+    cts, planted, valid = pk.ciphertexts(seed=77, count=65536, malformed_permille=0)
+    err, w = cmd.decrypt(engine, keys[s], cts, path=path)
+    assert np.array_equal(err, planted)
+    assert (w == 119).all()
+
+
+def test_decrypt_files_and_cli(engine, tmp_path):
+    s = 348864
+    out = str(tmp_path / "es.bin")
+    cmd.decrypt_files(engine, s, os.path.join(KEM, f"sk_{s}.bin"), os.path.join(KEM, f"ct_{s}.bin"), 5, out)
+    assert open(out, "rb").read() == golden_errorstream(s)
+    # short ct file -> KAT_FILE_OPEN_ERROR (-1); KATNUM 0 -> KAT_CRYPTO_FAILURE (-4)
+    with pytest.raises(cmd.CmdError) as ei:
+        cmd.decrypt_files(engine, s, os.path.join(KEM, f"sk_{s}.bin"), os.path.join(KEM, f"ct_{s}.bin"), 6, out)
+    assert ei.value.code == cmd.CMD_E_FILE
+    with pytest.raises(cmd.CmdError) as ei:
+        cmd.decrypt_files(engine, s, os.path.join(KEM, f"sk_{s}.bin"), os.path.join(KEM, f"ct_{s}.bin"), 0, out)
+    assert ei.value.code == cmd.CMD_E_ARG
+    # the CLI in the reference's directory layout, default relative paths
+    for st in SETS:
+        work = tmp_path / f"w{st}" / "CPU" / "param" / f"param{st}"
+        work.mkdir(parents=True)
+        (tmp_path / f"w{st}" / "CPU" / "results" / "output").mkdir(parents=True)
+        vec = tmp_path / f"w{st}" / "kem" / "test_vectors" / "Cipher_Sk"
+        vec.mkdir(parents=True)
+        for name in (f"sk_{st}.bin", f"ct_{st}.bin"):
+            (vec / name).write_bytes(open(os.path.join(KEM, name), "rb").read())
+        r = subprocess.run([cmd.CLI_PATH, str(st), "5"], cwd=work, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        got = (tmp_path / f"w{st}" / "CPU" / "results" / "output" / f"errorstream0_{st}.bin").read_bytes()
+        assert got == golden_errorstream(st)
+    r = subprocess.run([cmd.CLI_PATH, "348864", "0"], capture_output=True)
+    assert r.returncode == 256 - 4
+
+
+def test_bad_key_length_and_budget(engine):
+    with pytest.raises(cmd.CmdError) as ei:
+        cmd.Key(engine, 348864, golden_sk(348864)[:-1])
+    assert ei.value.code == cmd.CMD_E_ARG
+    small = cmd.Engine(0, hbm_budget=1 << 20)
+    try:
+        with pytest.raises(cmd.CmdError) as ei:
+            cmd.Key(small, 6960119, golden_sk(6960119))
+        assert ei.value.code == cmd.CMD_E_BUDGET
+    finally:
+        small.close()
