@@ -55,6 +55,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--count", type=int, default=COUNT)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="only the fused-kernel steps (profiling runs: no peak, plain, e2e or CPU legs)")
     return ap.parse_args()
 
 
@@ -198,8 +200,12 @@ def main() -> None:
     d_cts = [torch.from_numpy(cts).cuda() for _ in range(nbuf)]
     d_err = [torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda") for _ in range(nbuf)]
     d_w = [torch.zeros(count, dtype=torch.int16, device="cuda") for _ in range(nbuf)]
-    stream = torch.cuda.current_stream()
+    # A dedicated stream: the engine launches on it and the CUDA events are
+    # recorded on it (stream 0 would select the engine's own stream).
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sp = stream.cuda_stream
+    assert sp != 0
 
     def step(i: int, path: str) -> None:
         b = i % nbuf
@@ -241,6 +247,12 @@ def main() -> None:
             ms = float(t.item())
         return ms, launches, clk.summary()
 
+    if args.kernel_only:
+        ms, launches, _ = timed("fused", args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "decaps_per_s": world * count * args.steps / (ms * 1e-3),
+                              "ms_per_step": ms / args.steps, "gpu_launches": launches}), flush=True)
+        return
     int_peak = eng.int_peak()
     ms, launches, clocks = timed("fused", args.steps, args.warmup)
     ms_plain = None

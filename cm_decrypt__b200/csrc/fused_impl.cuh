@@ -379,24 +379,34 @@ size_t smem_limit_bytes();
 
 // Per-instantiation launch and occupancy helpers (one translation unit per
 // set mask, so the instantiations compile in parallel).
+// Raises the kernel's dynamic shared-memory limit to `smem` (never lowers
+// it; the opt-in maximum per CTA includes the kernel's static shared memory,
+// so the attribute is set to what a launch needs, not to the device limit).
+template <int SETMASK, int WPB> cudaError_t ensure_smem_attr(size_t smem)
+{
+    static size_t set_to = 0;
+    if (smem <= set_to)
+        return cudaSuccess;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_fused<SETMASK, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        set_to = smem;
+    return e;
+}
+
 template <int SETMASK, int WPB> cudaError_t launch_k(const FusedArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-    static bool attr_done = false;
-    if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused<SETMASK, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem_limit_bytes());
-        if (e != cudaSuccess)
-            return e;
-        attr_done = true;
-    }
+    cudaError_t e = ensure_smem_attr<SETMASK, WPB>(smem);
+    if (e != cudaSuccess)
+        return e;
     k_fused<SETMASK, WPB><<<grid, WPB * 32, smem, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int SETMASK, int WPB> int occupancy(size_t smem)
 {
-    cudaFuncSetAttribute(k_fused<SETMASK, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)smem_limit_bytes());
+    if (ensure_smem_attr<SETMASK, WPB>(smem) != cudaSuccess)
+        return 0;
     int n = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused<SETMASK, WPB>, WPB * 32, smem) != cudaSuccess)
         return 1;
