@@ -89,6 +89,7 @@ def lib() -> ctypes.CDLL:
         "cmd_decrypt_batch": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp]),
         "cmd_decrypt_device": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp, _vp]),
         "cmd_decrypt_mixed_device": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp]),
+        "cmd_decrypt_plain_noalloc": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp]),
         "cmd_stage_synd": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
         "cmd_stage_bm": (_i32, [_vp, _i32, _vp, _sz, _vp, _vp]),
         "cmd_stage_root": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),

@@ -131,6 +131,27 @@ int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *keys,
                              const uint64_t *h_err_off, uint16_t *d_weight,
                              void *stream);
 
+/* Allocation-free decrypt.  No counterpart in the reference: it exists for
+ * callers that must not have the library allocate device memory -- hosts whose
+ * device memory belongs to another allocator (e.g. a framework's pool), or
+ * latency-critical loops that cannot afford a cudaMalloc/cudaFree and the
+ * synchronisation it brings.  It runs the plain three-kernel path (same
+ * results as cmd_decrypt_device with CMD_PATH_PLAIN) but keeps the syndrome
+ * and locator intermediates in a fixed device array inside the library,
+ * sized for CMD_NOALLOC_MAX_CTS ciphertexts per call (about 3 MiB, held by
+ * every GPU that loads the library until the process exits).  The caller
+ * passes the expanded key, device ciphertexts (count * ct_bytes) and device
+ * outputs (count rows of err_words words; weights may be NULL).  count above
+ * the maximum returns CMD_E_ARG.  The first call on a device looks up the
+ * array's device address, so make that first call before any stream
+ * capture begins.  Calls share the array: calls that overlap on the GPU
+ * (concurrent streams or threads) race, so serialise them.  Asynchronous on
+ * `stream` (NULL = the key's engine stream). */
+#define CMD_NOALLOC_MAX_CTS 4096
+int cmd_decrypt_plain_noalloc(const cmd_key *key, const uint8_t *d_cts,
+                              size_t count, uint32_t *d_err,
+                              uint16_t *d_weight, void *stream);
+
 /* ---- per-stage parity hooks (device buffers, asynchronous) ------------- */
 /* synd(): d_synd = count rows of 2t u16 (CPU/param/param6960119/src/
  * util.c:102-114). */
