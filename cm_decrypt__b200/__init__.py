@@ -58,6 +58,26 @@ class SetInfo:
     err_words: int
 
 
+class ServerConfig(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint32) for n in
+                ("max_batch", "slots", "max_wait_us", "queue_capacity", "fused_threshold", "record_completions")]
+
+
+class Completion(ctypes.Structure):
+    _fields_ = [("tag", ctypes.c_uint64), ("status", ctypes.c_int32), ("weight", ctypes.c_uint16),
+                ("reserved", ctypes.c_uint16), ("latency_ns", ctypes.c_uint64)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("submitted", "completed", "refused", "batches", "fused_batches", "resident_keys")] + \
+               [(n, ctypes.c_double) for n in
+                ("mean_batch", "p50_us", "p99_us", "max_us", "mean_us", "decaps_per_s", "offered_per_s")]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib: ctypes.CDLL | None = None
 _vp, _sz, _u64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_uint64
 _i32 = ctypes.c_int
@@ -99,6 +119,22 @@ def lib() -> ctypes.CDLL:
         "cmd_decrypt_files": (_i32, [_vp, _i32, ctypes.c_char_p, ctypes.c_char_p, _sz, ctypes.c_char_p, _i32,
                                      ctypes.POINTER(ctypes.c_double)]),
         "cmd_bench_int_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
+        "cmd_tune": (_i32, [_vp, _vp, _sz, _i32]),
+        "cmd_engine_fused_config": (_i32, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
+                                           ctypes.POINTER(ctypes.c_double)]),
+        "cmd_engine_set_fused_config": (_i32, [_vp, _i32, _i32, _i32]),
+        "cmd_graph_capture": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp, ctypes.POINTER(_vp)]),
+        "cmd_graph_launch": (_i32, [_vp, _vp]),
+        "cmd_graph_destroy": (None, [_vp]),
+        "cmd_server_create": (_i32, [_vp, ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]),
+        "cmd_server_destroy": (None, [_vp]),
+        "cmd_server_add_key": (_i32, [_vp, _i32, _vp, _sz, ctypes.POINTER(ctypes.c_uint32)]),
+        "cmd_server_submit": (_i32, [_vp, ctypes.c_uint32, _vp, _vp, _u64]),
+        "cmd_server_poll": (_i32, [_vp, ctypes.POINTER(Completion), _sz, ctypes.POINTER(_sz), ctypes.c_uint32]),
+        "cmd_server_drain": (_i32, [_vp, ctypes.c_uint32]),
+        "cmd_server_stats_get": (_i32, [_vp, ctypes.POINTER(ServerStats), _i32]),
+        "cmd_server_loadgen": (_i32, [_vp, _vp, _vp, _sz, _vp, _sz, _sz, ctypes.c_double, ctypes.c_double, _u64,
+                                      ctypes.POINTER(ServerStats)]),
         "cmd_synth_key": (_i32, [_i32, _vp, _u64, _vp]),
         "cmd_synth_pubkey": (_i32, [_i32, _vp, ctypes.POINTER(_vp)]),
         "cmd_synth_pubkey_free": (None, [_vp]),
@@ -254,6 +290,107 @@ def decrypt_mixed_device(engine: Engine, keys: list[Key], key_idx: np.ndarray, d
     eo = np.ascontiguousarray(err_off, np.uint64)
     _check(lib().cmd_decrypt_mixed_device(engine.handle, arr, len(keys), _ptr(ki), d_cts, _ptr(co), ki.size, d_err,
                                           _ptr(eo), d_weight or None, stream or None), "cmd_decrypt_mixed_device")
+
+
+def tune(engine: Engine, key: Key, sample_count: int = 0, force: bool = False) -> dict:
+    """Autotunes the fused kernel for key's set; returns the chosen config."""
+    _check(lib().cmd_tune(engine.handle, key.handle, sample_count, int(force)), "cmd_tune")
+    return fused_config(engine, key.info.set_id)
+
+
+def fused_config(engine: Engine, set_id: int) -> dict:
+    wpb, bal, ns = _i32(), _i32(), ctypes.c_double()
+    _check(lib().cmd_engine_fused_config(engine.handle, set_index(set_id), ctypes.byref(wpb), ctypes.byref(bal),
+                                         ctypes.byref(ns)), "cmd_engine_fused_config")
+    return {"wpb": wpb.value, "balanced": bool(bal.value), "ns_per_ct": ns.value}
+
+
+def set_fused_config(engine: Engine, set_id: int, wpb: int, balanced: bool = True) -> None:
+    _check(lib().cmd_engine_set_fused_config(engine.handle, set_index(set_id), wpb, int(balanced)),
+           "cmd_engine_set_fused_config")
+
+
+class Graph:
+    """A decrypt over fixed device buffers, captured once, replayed many times."""
+
+    def __init__(self, engine: Engine, key: Key, d_cts: int, count: int, d_err: int, d_weight: int = 0,
+                 path: str = "fused"):
+        h = _vp()
+        _check(lib().cmd_graph_capture(engine.handle, key.handle, PATHS[path], d_cts, count, d_err,
+                                       d_weight or None, ctypes.byref(h)), "cmd_graph_capture")
+        self.handle = h
+
+    def launch(self, stream: int = 0) -> None:
+        _check(lib().cmd_graph_launch(self.handle, stream or None), "cmd_graph_launch")
+
+    def close(self) -> None:
+        if self.handle:
+            lib().cmd_graph_destroy(self.handle)
+            self.handle = None
+
+
+class Server:
+    """Continuous-batching decapsulation server (see cmd_server_* in the header)."""
+
+    def __init__(self, engine: Engine, max_batch: int = 2048, slots: int = 4, max_wait_us: int = 200,
+                 queue_capacity: int = 1 << 20, fused_threshold: int = 0, record_completions: bool = True):
+        cfg = ServerConfig(max_batch, slots, max_wait_us, queue_capacity, fused_threshold, int(record_completions))
+        h = _vp()
+        _check(lib().cmd_server_create(engine.handle, ctypes.byref(cfg), ctypes.byref(h)), "cmd_server_create")
+        self.handle = h
+        self.key_sets: list[int] = []
+
+    def close(self) -> None:
+        if self.handle:
+            lib().cmd_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add_key(self, set_id: int, sk: bytes) -> int:
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        kid = ctypes.c_uint32()
+        _check(lib().cmd_server_add_key(self.handle, set_index(set_id), _ptr(skb), skb.size, ctypes.byref(kid)),
+               "cmd_server_add_key")
+        self.key_sets.append(set_id)
+        return kid.value
+
+    def submit(self, key_id: int, ct: np.ndarray, err_out: np.ndarray | None, tag: int) -> int:
+        """Returns CMD_OK or CMD_E_BUSY; err_out must stay alive until completion."""
+        rc = lib().cmd_server_submit(self.handle, key_id, _ptr(ct), _ptr(err_out) if err_out is not None else None,
+                                     tag)
+        if rc not in (CMD_OK, CMD_E_BUSY):
+            raise CmdError(rc, "cmd_server_submit")
+        return rc
+
+    def poll(self, max_n: int = 4096, timeout_us: int = 0) -> list[tuple[int, int, int, int]]:
+        buf = (Completion * max_n)()
+        n = _sz()
+        _check(lib().cmd_server_poll(self.handle, buf, max_n, ctypes.byref(n), timeout_us), "cmd_server_poll")
+        return [(c.tag, c.status, c.weight, c.latency_ns) for c in buf[: n.value]]
+
+    def drain(self, timeout_ms: int = 60000) -> None:
+        _check(lib().cmd_server_drain(self.handle, timeout_ms), "cmd_server_drain")
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        _check(lib().cmd_server_stats_get(self.handle, ctypes.byref(st), int(reset)), "cmd_server_stats_get")
+        return st.as_dict()
+
+    def loadgen(self, key_ids: np.ndarray, cts: np.ndarray, err_pool: np.ndarray | None, rate: float,
+                seconds: float, seed: int = 0x5EED) -> dict:
+        ki = np.ascontiguousarray(key_ids, np.uint32)
+        c = np.ascontiguousarray(cts, np.uint8)
+        st = ServerStats()
+        _check(lib().cmd_server_loadgen(self.handle, _ptr(ki), _ptr(c), c.shape[1],
+                                        _ptr(err_pool) if err_pool is not None else None,
+                                        err_pool.shape[1] if err_pool is not None else 0, ki.size, rate, seconds,
+                                        seed, ctypes.byref(st)), "cmd_server_loadgen")
+        return st.as_dict()
 
 
 # ---- per-stage hooks (device pointers) -----------------------------------

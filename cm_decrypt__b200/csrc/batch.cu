@@ -54,13 +54,30 @@ static int grid_for(cmd_engine *eng, int single_set, int wpb, size_t smem, uint6
     return (int)std::min<uint64_t>(g, rounds);
 }
 
+// Ciphertexts per round.  `full` (every round fills all WPB warps) leaves
+// the last wave partly idle when the batch is not a multiple of the resident
+// capacity; `balanced` shrinks rounds (in whole 32-ciphertext tiles) so the
+// batch splits into equal shares per resident CTA.
+static uint32_t round_size(cmd_engine *eng, int set, int wpb, size_t count, bool balanced)
+{
+    const uint64_t full = (uint64_t)wpb * 32;
+    if (!balanced)
+        return (uint32_t)full;
+    int per_sm = fused_blocks_per_sm(set, wpb, fused_smem(set, wpb));
+    const uint64_t ctas = (uint64_t)(per_sm < 1 ? 1 : per_sm) * eng->num_sms;
+    const uint64_t waves = (count + ctas * full - 1) / (ctas * full);
+    uint64_t r = (count + ctas * waves - 1) / (ctas * waves);
+    r = (r + 31) / 32 * 32;
+    return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(r, 32), full);
+}
+
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                       uint16_t *d_weight, cudaStream_t s, uint32_t *counter)
 {
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
     const int wpb = eng->fcfg[set].wpb;
-    const uint32_t round = (uint32_t)wpb * 32;
+    const uint32_t round = round_size(eng, set, wpb, count, eng->fcfg[set].balanced);
     const uint64_t rounds = (count + round - 1) / round;
     if (rounds > 0xFFFFFFFFull)
         return CMD_E_ARG;
@@ -86,6 +103,14 @@ int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
     return e == cudaSuccess ? CMD_OK : cuda_fail(e, "fused kernel launch");
 }
 
+// Sets the fused kernel's shared-memory attribute for this set's current
+// configuration ahead of time (e.g. before a stream capture begins).
+cudaError_t fused_prepare(cmd_engine *eng, int set)
+{
+    const int wpb = eng->fcfg[set].wpb;
+    return fused_blocks_per_sm(set, wpb, fused_smem(set, wpb)) > 0 ? cudaSuccess : cudaErrorInvalidConfiguration;
+}
+
 int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                      uint16_t *d_weight, cudaStream_t s)
 {
@@ -93,6 +118,50 @@ int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
     if (rc)
         return rc;
     return run_fused_counter(eng, key, d_cts, count, d_err, d_weight, s, eng->tile_counter);
+}
+
+// Set shared by every ciphertext of a mixed batch, or -1.
+int mixed_single_set(const int *key_set, const uint32_t *key_idx, size_t count)
+{
+    if (count == 0)
+        return -1;
+    const int s0 = key_set[key_idx[0]];
+    for (size_t c = 1; c < count; c++)
+        if (key_set[key_idx[c]] != s0)
+            return -1;
+    return s0;
+}
+
+// Groups ciphertexts by key (counting sort, stable in batch order) into
+// `order` and cuts each key's run into rounds of up to R; rounds of costlier
+// sets come first so the dynamic scheduler ends with cheap rounds.
+void plan_mixed(const int *key_set, size_t nkeys, const uint32_t *key_idx, size_t count, uint32_t R,
+                std::vector<uint32_t> &order, std::vector<FusedTile> &tiles)
+{
+    std::vector<uint32_t> cnt(nkeys + 1, 0);
+    for (size_t c = 0; c < count; c++)
+        cnt[key_idx[c] + 1]++;
+    for (size_t k = 0; k < nkeys; k++)
+        cnt[k + 1] += cnt[k];
+    order.assign(count, 0);
+    std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+    for (size_t c = 0; c < count; c++)
+        order[fill[key_idx[c]]++] = (uint32_t)c;
+    tiles.clear();
+    for (size_t k = 0; k < nkeys; k++)
+        for (uint32_t r0 = cnt[k]; r0 < cnt[k + 1]; r0 += R)
+            tiles.push_back(FusedTile{(uint32_t)k, std::min(R, cnt[k + 1] - r0), r0});
+    auto cost = [&](const FusedTile &t) {
+        const SetInfo si = set_info(key_set[t.key]);
+        return (uint64_t)si.n * si.t * si.m * si.m;
+    };
+    std::stable_sort(tiles.begin(), tiles.end(),
+                     [&](const FusedTile &x, const FusedTile &y) { return cost(x) > cost(y); });
+}
+
+int fused_grid(cmd_engine *eng, int single_set, int wpb, size_t smem, uint64_t rounds)
+{
+    return grid_for(eng, single_set, wpb, smem, rounds);
 }
 
 }  // namespace cmd
@@ -116,40 +185,17 @@ extern "C" int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *k
     cudaSetDevice(eng->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : eng->stream;
 
-    // Group ciphertexts by key (counting sort, stable in batch order).
-    std::vector<uint32_t> cnt(nkeys + 1, 0);
-    for (size_t c = 0; c < count; c++) {
+    for (size_t c = 0; c < count; c++)
         if (h_key_idx[c] >= nkeys)
             return CMD_E_ARG;
-        cnt[h_key_idx[c] + 1]++;
-    }
+    std::vector<int> kset(nkeys);
     for (size_t k = 0; k < nkeys; k++)
-        cnt[k + 1] += cnt[k];
-    std::vector<uint32_t> order(count), fill(cnt.begin(), cnt.end() - 1);
-    for (size_t c = 0; c < count; c++)
-        order[fill[h_key_idx[c]]++] = (uint32_t)c;
-
-    int first_set = keys[h_key_idx[0]]->dev.set;
-    bool one_set = true;
-    for (size_t k = 0; k < nkeys; k++)
-        if (cnt[k + 1] > cnt[k] && keys[k]->dev.set != first_set)
-            one_set = false;
-    const int single = one_set ? first_set : -1;
-    const int wpb = one_set ? eng->fcfg[first_set].wpb : eng->fcfg_mixed.wpb;
-    const uint32_t R = (uint32_t)wpb * 32;
-
-    // Rounds: per key, slices of up to R ciphertexts; costlier sets first so
-    // the dynamic scheduler ends with the cheap rounds.
+        kset[k] = keys[k]->dev.set;
+    int single = mixed_single_set(kset.data(), h_key_idx, count);
+    const int wpb = single >= 0 ? eng->fcfg[single].wpb : eng->fcfg_mixed.wpb;
+    std::vector<uint32_t> order;
     std::vector<FusedTile> tiles;
-    for (size_t k = 0; k < nkeys; k++)
-        for (uint32_t r0 = cnt[k]; r0 < cnt[k + 1]; r0 += R)
-            tiles.push_back(FusedTile{(uint32_t)k, std::min(R, cnt[k + 1] - r0), r0});
-    auto cost = [&](const FusedTile &t) {
-        const SetInfo si = set_info(keys[t.key]->dev.set);
-        return (uint64_t)si.n * si.t * si.m * si.m;
-    };
-    std::stable_sort(tiles.begin(), tiles.end(),
-                     [&](const FusedTile &x, const FusedTile &y) { return cost(x) > cost(y); });
+    plan_mixed(kset.data(), nkeys, h_key_idx, count, (uint32_t)wpb * 32, order, tiles);
     std::vector<FusedKeyRef> krefs(nkeys);
     for (size_t k = 0; k < nkeys; k++)
         krefs[k] = FusedKeyRef{keys[k]->dev.set, 0, keys[k]->dev.tab, keys[k]->dev.Lbs};

@@ -183,6 +183,8 @@ void cmd_engine_destroy(cmd_engine *eng)
     cudaSetDevice(eng->device);
     cudaStreamSynchronize(eng->stream);
     eng->scratch.release(eng);
+    eng->io.release(eng);
+    eng->fused.release(eng);
     eng->host_scratch.release();
     if (eng->tile_counter)
         cudaFree(eng->tile_counter);
@@ -359,6 +361,15 @@ int cmd_stage_root_images(cmd_engine *eng, const cmd_key *key, const uint16_t *d
 
 namespace cmd {
 
+// Scratch the plain path needs for a batch: per chunk of up to 2^18
+// ciphertexts, the syndromes (t words) and locators (t+1 u16) of each.
+size_t plain_scratch_bytes(int set, size_t count)
+{
+    const SetInfo si = set_info(set);
+    const size_t chunk = std::min<size_t>(count, (size_t)1 << 18);
+    return carve_size({chunk * si.t * 4, chunk * (si.t + 1) * 2});
+}
+
 // Plain path over a device batch, in chunks so the syndrome/locator
 // intermediates stay bounded.  Caller holds eng->mu.
 static int run_plain(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
@@ -366,7 +377,7 @@ static int run_plain(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
 {
     const SetInfo si = set_info(key->dev.set);
     const size_t chunk = std::min<size_t>(count, (size_t)1 << 18);
-    const size_t need = carve_size({chunk * si.t * 4, chunk * (si.t + 1) * 2});
+    const size_t need = plain_scratch_bytes(key->dev.set, count);
     int rc = eng->scratch.reserve(eng, need);
     if (rc)
         return rc;

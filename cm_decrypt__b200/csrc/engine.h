@@ -33,10 +33,10 @@ struct HostScratch {
 
 // Fused-kernel launch configuration chosen per parameter set.
 struct FusedConfig {
-    int wpb = 8;         // warps per CTA (4 or 8)
-    int ctas_per_sm = 1; // resident CTAs per SM the grid is sized for
+    int wpb = 8;          // warps per CTA (4 or 8)
+    bool balanced = true; // equal-share rounds (see round_size in batch.cu)
     bool tuned = false;
-    double us_per_ct = 0;
+    double ns_per_ct = 0; // measured by the tuner
 };
 
 int cuda_fail(cudaError_t e, const char *what);
@@ -50,6 +50,11 @@ int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
                      uint16_t *d_weight, cudaStream_t s);
 size_t fused_smem(int set, int wpb);
 size_t smem_limit_bytes();
+int fused_blocks_per_sm(int single_set, int wpb, size_t smem);
+int fused_grid(cmd_engine *eng, int single_set, int wpb, size_t smem, uint64_t rounds);
+int mixed_single_set(const int *key_set, const uint32_t *key_idx, size_t count);
+void plan_mixed(const int *key_set, size_t nkeys, const uint32_t *key_idx, size_t count, uint32_t R,
+                std::vector<uint32_t> &order, std::vector<FusedTile> &tiles);
 
 }  // namespace cmd
 

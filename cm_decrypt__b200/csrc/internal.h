@@ -85,6 +85,12 @@ struct FusedArgs {
 cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,
                          LaunchCounter lc);
 
+// Multi-key plain path (serving loop, small batches): syndrome, BM and root
+// kernels for `count` ciphertexts of one set, each naming its own key.
+cudaError_t launch_keys_path(int set, const FusedKeyRef *d_keys, const uint32_t *d_key_idx, const uint8_t *d_cts,
+                             uint32_t ct_stride, size_t count, uint32_t *d_synd, uint16_t *d_loc, uint32_t *d_err,
+                             uint32_t err_stride, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc);
+
 void set_last_error(const std::string &msg);
 
 }  // namespace cmd

@@ -1,0 +1,682 @@
+// Serving loop: continuous batching of decapsulation requests for many keys
+// and parameter sets on one GPU.
+//
+//  * Requests (key id, ciphertext, output buffer, tag) enter a bounded queue;
+//    a full queue refuses with CMD_E_BUSY.
+//  * A dispatcher thread owns `slots` batch slots, each with its own CUDA
+//    stream, pinned staging and device buffers.  Whenever a slot is free and
+//    requests are waiting it forms a batch of up to max_batch of them -- at
+//    once if nothing is on the GPU, otherwise after batch-mates have had at most
+//    max_wait_us to arrive -- so requests that arrive while other batches run
+//    are admitted as soon as a slot frees, and the batches overlap on the
+//    device (copies and kernels of different slots run concurrently).
+//  * Expanded keys stay resident in HBM; a key is expanded on first use and
+//    the least recently used unpinned keys are evicted when the engine's HBM
+//    budget is full (admission by budget).
+//  * Small batches run the multi-key plain kernels (a short pass per
+//    ciphertext, lowest latency); batches of fused_threshold or more run the
+//    fused kernel (highest throughput).
+//  * A completer thread waits for slots in dispatch order, copies each
+//    result to its request's buffer and records arrival-to-completion
+//    latency for the p50/p99 statistics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <random>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "engine.h"
+
+namespace cmd {
+
+constexpr uint32_t CT_STRIDE = 208;   // largest ciphertext
+constexpr uint32_t ERR_STRIDE = 256;  // words: largest error row (8192 bits)
+
+static uint64_t now_ns()
+{
+    return (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct Request {
+    uint32_t key_id;
+    uint64_t tag;
+    uint8_t *err_out;
+    uint64_t t_arrive;
+    uint8_t ct[CT_STRIDE];
+};
+
+struct KeyEntry {
+    int set;
+    std::vector<uint8_t> sk;
+    cmd_key *key = nullptr;
+    uint64_t last_use = 0;
+    int pins = 0;
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    uint8_t *h_in = nullptr, *d_in = nullptr;  // packed inputs (see dispatch)
+    uint32_t *h_err = nullptr, *d_err = nullptr;
+    uint16_t *h_w = nullptr, *d_w = nullptr;
+    uint32_t *d_synd = nullptr;
+    uint16_t *d_loc = nullptr;
+    uint32_t *d_counter = nullptr;
+    std::vector<Request> reqs;
+    std::vector<uint32_t> pinned;  // key ids pinned by this batch
+    bool fused = false;
+};
+
+}  // namespace cmd
+
+using namespace cmd;
+
+struct cmd_server {
+    cmd_engine *eng = nullptr;
+    cmd_server_config cfg{};
+    size_t in_bytes = 0, device_bytes = 0;
+    std::mutex mu;
+    std::condition_variable cv_dispatch, cv_complete, cv_poll;
+    std::deque<Request> pending;
+    std::deque<KeyEntry> keys;   // deque: entries keep their address as keys are added
+    std::vector<Slot> slots;
+    std::deque<int> free_slots, inflight;
+    std::deque<cmd_completion> completions;
+    std::thread dispatcher, completer;
+    bool stop = false;
+    bool dispatch_exited = false;
+    int status = CMD_OK;
+    // statistics
+    std::vector<uint32_t> lat_ns;
+    uint64_t submitted = 0, completed = 0, refused = 0, batches = 0, fused_batches = 0, batched_cts = 0;
+    uint64_t t_first = 0, t_last = 0;
+    uint64_t tick = 0;
+    uint64_t completions_gen = 0;  // bumped each time a batch completes
+
+    void dispatch_loop();
+    void complete_loop();
+    int ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys);
+    int launch(Slot &sl);
+};
+
+namespace {
+
+// Input packing of a slot: ciphertexts at CT_STRIDE, then key index per
+// ciphertext, then (fused) ct_off, err_off, order, tiles, key table.
+struct InLayout {
+    size_t cts, key_idx, ct_off, err_off, order, tiles, keys, total;
+    InLayout(size_t B, size_t max_keys)
+    {
+        auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+        cts = 0;
+        key_idx = al(cts + B * CT_STRIDE);
+        ct_off = al(key_idx + B * 4);
+        err_off = al(ct_off + B * 8);
+        order = al(err_off + B * 8);
+        tiles = al(order + B * 4);
+        keys = al(tiles + B * sizeof(FusedTile));
+        total = al(keys + max_keys * sizeof(FusedKeyRef));
+    }
+};
+
+}  // namespace
+
+int cmd_server::ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys)
+{
+    KeyEntry &ke = keys[id];
+    ke.last_use = ++tick;
+    if (ke.key)
+        return CMD_OK;
+    while (true) {
+        int rc = cmd_key_expand(eng, (cmd_set)ke.set, ke.sk.data(), ke.sk.size(), &ke.key);
+        if (rc != CMD_E_BUDGET)
+            return rc;
+        // Evict the least recently used resident key that no batch in flight
+        // and not this batch uses.
+        int victim = -1;
+        bool held = false;  // some resident key is pinned by a batch in flight
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            for (size_t k = 0; k < keys.size(); k++) {
+                if (!keys[k].key || k == id)
+                    continue;
+                if (keys[k].pins > 0) {
+                    held = true;
+                    continue;
+                }
+                if (std::find(batch_keys.begin(), batch_keys.end(), (uint32_t)k) != batch_keys.end())
+                    continue;
+                if (victim < 0 || keys[k].last_use < keys[victim].last_use)
+                    victim = (int)k;
+            }
+        }
+        if (victim < 0)
+            return held ? CMD_E_BUSY : CMD_E_BUDGET;  // BUSY: retry once a batch completes
+        cmd_key_free(keys[victim].key);
+        keys[victim].key = nullptr;
+    }
+}
+
+int cmd_server::launch(Slot &sl)
+{
+    // Make the batch's keys resident.  When the HBM budget cannot hold all of
+    // them at once, the requests of the keys that did not fit go back to the
+    // front of the queue for the next batch (only a batch whose first key
+    // cannot be made resident fails).
+    std::vector<uint32_t> kid;
+    {
+        std::unordered_map<uint32_t, int> seen;
+        for (const Request &r : sl.reqs)
+            if (seen.emplace(r.key_id, 1).second)
+                kid.push_back(r.key_id);
+    }
+    std::vector<uint32_t> ready;
+    for (uint32_t k : kid) {
+        int rc = ensure_key(k, ready);
+        if ((rc == CMD_E_BUDGET || rc == CMD_E_BUSY) && !ready.empty())
+            break;
+        if (rc)
+            return rc;
+        ready.push_back(k);
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (uint32_t k : ready)
+            keys[k].pins++;
+        if (ready.size() < kid.size()) {
+            std::vector<Request> keep, defer;
+            for (const Request &r : sl.reqs)
+                (std::find(ready.begin(), ready.end(), r.key_id) != ready.end() ? keep : defer).push_back(r);
+            pending.insert(pending.begin(), defer.begin(), defer.end());
+            sl.reqs.swap(keep);
+        }
+    }
+    sl.pinned = ready;
+    kid = ready;
+    const size_t B = sl.reqs.size();
+    InLayout lay(B, B);
+    std::unordered_map<uint32_t, uint32_t> local;
+    for (size_t k = 0; k < kid.size(); k++)
+        local.emplace(kid[k], (uint32_t)k);
+    uint32_t *key_idx = reinterpret_cast<uint32_t *>(sl.h_in + lay.key_idx);
+    for (size_t i = 0; i < B; i++) {
+        key_idx[i] = local[sl.reqs[i].key_id];
+        memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
+    }
+    FusedKeyRef *krefs = reinterpret_cast<FusedKeyRef *>(sl.h_in + lay.keys);
+    std::vector<int> kset(kid.size());
+    for (size_t k = 0; k < kid.size(); k++) {
+        const cmd_key *key = keys[kid[k]].key;
+        krefs[k] = FusedKeyRef{key->dev.set, 0, key->dev.tab, key->dev.Lbs};
+        kset[k] = key->dev.set;
+    }
+    LaunchCounter lc{&eng->launches};
+    cudaStream_t s = sl.stream;
+    cudaError_t e;
+    sl.fused = cfg.fused_threshold > 0 && B >= cfg.fused_threshold;
+    if (!sl.fused) {
+        // Plain multi-key path, one launch group per set: reorder the batch by
+        // set so each set's ciphertexts are contiguous.
+        std::vector<uint32_t> perm(B);
+        for (size_t i = 0; i < B; i++)
+            perm[i] = (uint32_t)i;
+        std::stable_sort(perm.begin(), perm.end(),
+                         [&](uint32_t a, uint32_t b) { return kset[key_idx[a]] < kset[key_idx[b]]; });
+        std::vector<Request> sorted(B);
+        std::vector<uint32_t> ki(B);
+        for (size_t i = 0; i < B; i++) {
+            sorted[i] = sl.reqs[perm[i]];
+            ki[i] = key_idx[perm[i]];
+        }
+        sl.reqs.swap(sorted);
+        for (size_t i = 0; i < B; i++) {
+            key_idx[i] = ki[i];
+            memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
+        }
+        if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_fail(e, "server H2D");
+        const FusedKeyRef *d_keys = reinterpret_cast<const FusedKeyRef *>(sl.d_in + lay.keys);
+        size_t i = 0;
+        while (i < B) {
+            const int set = kset[key_idx[i]];
+            size_t j = i;
+            while (j < B && kset[key_idx[j]] == set)
+                j++;
+            const SetInfo si = set_info(set);
+            e = launch_keys_path(set, d_keys, reinterpret_cast<const uint32_t *>(sl.d_in + lay.key_idx) + i,
+                                 sl.d_in + lay.cts + i * CT_STRIDE, CT_STRIDE, j - i, sl.d_synd + i * 128,
+                                 sl.d_loc + i * 129, sl.d_err + i * ERR_STRIDE, ERR_STRIDE, sl.d_w + i, s, lc);
+            (void)si;
+            if (e != cudaSuccess)
+                return cuda_fail(e, "server plain launch");
+            i = j;
+        }
+    } else {
+        uint64_t *ct_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.ct_off);
+        uint64_t *err_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.err_off);
+        for (size_t i = 0; i < B; i++) {
+            ct_off[i] = i * CT_STRIDE;
+            err_off[i] = i * ERR_STRIDE;
+        }
+        const int single = mixed_single_set(kset.data(), key_idx, B);
+        const int wpb = single >= 0 ? eng->fcfg[single].wpb : eng->fcfg_mixed.wpb;
+        std::vector<uint32_t> order;
+        std::vector<FusedTile> tiles;
+        plan_mixed(kset.data(), kid.size(), key_idx, B, (uint32_t)wpb * 32, order, tiles);
+        memcpy(sl.h_in + lay.order, order.data(), B * 4);
+        memcpy(sl.h_in + lay.tiles, tiles.data(), tiles.size() * sizeof(FusedTile));
+        if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+            (e = cudaMemsetAsync(sl.d_counter, 0, 4, s)) != cudaSuccess)
+            return cuda_fail(e, "server H2D");
+        FusedArgs a;
+        memset(&a, 0, sizeof a);
+        a.tiles = reinterpret_cast<const FusedTile *>(sl.d_in + lay.tiles);
+        a.ntiles = (uint32_t)tiles.size();
+        a.keys = reinterpret_cast<const FusedKeyRef *>(sl.d_in + lay.keys);
+        a.cts = sl.d_in + lay.cts;
+        a.ct_off = reinterpret_cast<const uint64_t *>(sl.d_in + lay.ct_off);
+        a.err_off = reinterpret_cast<const uint64_t *>(sl.d_in + lay.err_off);
+        a.order = reinterpret_cast<const uint32_t *>(sl.d_in + lay.order);
+        a.err = sl.d_err;
+        a.weight = sl.d_w;
+        a.tile_counter = sl.d_counter;
+        a.single_set = single;
+        size_t smem = 0;
+        if (single >= 0)
+            smem = fused_smem(single, wpb);
+        else
+            for (int st = 0; st < NSETS; st++)
+                smem = std::max(smem, fused_smem(st, wpb));
+        const int grid = fused_grid(eng, single, wpb, smem, tiles.size());
+        if ((e = launch_fused(a, grid, wpb, s, lc)) != cudaSuccess)
+            return cuda_fail(e, "server fused launch");
+    }
+    if ((e = cudaMemcpyAsync(sl.h_err, sl.d_err, B * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(sl.h_w, sl.d_w, B * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (e = cudaEventRecord(sl.done, s)) != cudaSuccess)
+        return cuda_fail(e, "server D2H");
+    return CMD_OK;
+}
+
+void cmd_server::dispatch_loop()
+{
+    cudaSetDevice(eng->device);
+    std::unique_lock<std::mutex> lk(mu);
+    while (true) {
+        cv_dispatch.wait(lk, [&] { return stop || (!pending.empty() && !free_slots.empty()); });
+        if (stop && pending.empty())
+            break;
+        if (pending.empty() || free_slots.empty())
+            continue;
+        // Continuous batching: with batches already on the GPU, give the
+        // oldest waiting request up to max_wait_us to collect batch-mates.
+        if (!inflight.empty() && pending.size() < cfg.max_batch && !stop) {
+            const uint64_t deadline = pending.front().t_arrive + (uint64_t)cfg.max_wait_us * 1000;
+            const uint64_t t = now_ns();
+            if (t < deadline) {
+                cv_dispatch.wait_for(lk, std::chrono::nanoseconds(deadline - t), [&] {
+                    return stop || pending.size() >= cfg.max_batch || inflight.empty();
+                });
+                if (pending.empty() || free_slots.empty())
+                    continue;
+            }
+        }
+        const int si = free_slots.front();
+        free_slots.pop_front();
+        Slot &sl = slots[si];
+        const size_t take = std::min<size_t>(pending.size(), cfg.max_batch);
+        sl.reqs.assign(pending.begin(), pending.begin() + take);
+        pending.erase(pending.begin(), pending.begin() + take);
+        lk.unlock();
+        int rc = launch(sl);
+        lk.lock();
+        if (rc == CMD_E_BUSY) {
+            // Every key that could be evicted is in use by a batch in flight:
+            // requeue the batch and wait for a completion before retrying.
+            pending.insert(pending.begin(), sl.reqs.begin(), sl.reqs.end());
+            sl.reqs.clear();
+            free_slots.push_front(si);
+            const uint64_t gen = completions_gen;
+            cv_dispatch.wait(lk, [&] { return stop || completions_gen != gen || inflight.empty(); });
+            continue;
+        }
+        if (rc != CMD_OK) {
+            // Fail the batch's requests; the slot stays usable.
+            const uint64_t t = now_ns();
+            for (const Request &r : sl.reqs) {
+                if (cfg.record_completions)
+                    completions.push_back(cmd_completion{r.tag, rc, 0, 0, t - r.t_arrive});
+                completed++;
+            }
+            for (uint32_t k : sl.pinned)
+                keys[k].pins--;
+            sl.pinned.clear();
+            sl.reqs.clear();
+            free_slots.push_back(si);
+            if (status == CMD_OK)
+                status = rc;
+            cv_poll.notify_all();
+            continue;
+        }
+        batches++;
+        fused_batches += sl.fused ? 1 : 0;
+        batched_cts += sl.reqs.size();
+        inflight.push_back(si);
+        cv_complete.notify_one();
+    }
+    dispatch_exited = true;
+    cv_complete.notify_all();
+}
+
+void cmd_server::complete_loop()
+{
+    cudaSetDevice(eng->device);
+    std::unique_lock<std::mutex> lk(mu);
+    while (true) {
+        cv_complete.wait(lk, [&] { return !inflight.empty() || dispatch_exited; });
+        if (inflight.empty())
+            break;
+        const int si = inflight.front();
+        lk.unlock();
+        Slot &sl = slots[si];
+        const cudaError_t e = cudaEventSynchronize(sl.done);
+        const uint64_t t = now_ns();
+        std::vector<uint32_t> lats;
+        lats.reserve(sl.reqs.size());
+        std::vector<cmd_completion> done;
+        for (size_t i = 0; i < sl.reqs.size(); i++) {
+            const Request &r = sl.reqs[i];
+            const SetInfo info = set_info(keys[r.key_id].set);
+            if (e == cudaSuccess && r.err_out)
+                memcpy(r.err_out, sl.h_err + i * ERR_STRIDE, info.n / 8);
+            const uint64_t lat = t - r.t_arrive;
+            lats.push_back((uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu));
+            if (cfg.record_completions)
+                done.push_back(cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[i], 0, lat});
+        }
+        lk.lock();
+        if (e != cudaSuccess && status == CMD_OK) {
+            status = CMD_E_CUDA;
+            set_last_error(std::string("server batch: ") + cudaGetErrorString(e));
+        }
+        completions.insert(completions.end(), done.begin(), done.end());
+        lat_ns.insert(lat_ns.end(), lats.begin(), lats.end());
+        completed += sl.reqs.size();
+        t_last = t;
+        for (uint32_t k : sl.pinned)
+            keys[k].pins--;
+        sl.pinned.clear();
+        sl.reqs.clear();
+        inflight.pop_front();
+        free_slots.push_back(si);
+        completions_gen++;
+        cv_dispatch.notify_one();
+        cv_poll.notify_all();
+    }
+}
+
+extern "C" {
+
+int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server **out)
+{
+    if (!eng || !cfg || !out || cfg->max_batch == 0 || cfg->max_batch > 65536 || cfg->slots < 1 ||
+        cfg->slots > 16 || cfg->queue_capacity == 0)
+        return CMD_E_ARG;
+    *out = nullptr;
+    cudaSetDevice(eng->device);
+    cmd_server *srv = new cmd_server();
+    srv->eng = eng;
+    srv->cfg = *cfg;
+    const size_t B = cfg->max_batch;
+    InLayout lay(B, B);
+    srv->in_bytes = lay.total;
+    const size_t dev_per_slot = lay.total + B * ERR_STRIDE * 4 + B * 2 + B * 128 * 4 + B * 129 * 2 + 4 * 256;
+    srv->device_bytes = dev_per_slot * cfg->slots;
+    if (!budget_take(eng, srv->device_bytes)) {
+        delete srv;
+        set_last_error("server buffers exceed the engine HBM budget");
+        return CMD_E_BUDGET;
+    }
+    srv->slots.resize(cfg->slots);
+    cudaError_t e = cudaSuccess;
+    for (auto &sl : srv->slots) {
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&sl.h_in, lay.total);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&sl.h_err, B * ERR_STRIDE * 4);
+        if (e == cudaSuccess)
+            e = cudaMallocHost(&sl.h_w, B * 2);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_in, lay.total);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_err, B * ERR_STRIDE * 4);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_w, B * 2);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_synd, B * 128 * 4);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_loc, B * 129 * 2);
+        if (e == cudaSuccess)
+            e = cudaMalloc(&sl.d_counter, 256);
+    }
+    if (e != cudaSuccess) {
+        cmd_server_destroy(srv);
+        return cuda_fail(e, "server buffers");
+    }
+    for (int i = 0; i < (int)cfg->slots; i++)
+        srv->free_slots.push_back(i);
+    srv->dispatcher = std::thread([srv] { srv->dispatch_loop(); });
+    srv->completer = std::thread([srv] { srv->complete_loop(); });
+    *out = srv;
+    return CMD_OK;
+}
+
+void cmd_server_destroy(cmd_server *srv)
+{
+    if (!srv)
+        return;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->stop = true;
+    }
+    srv->cv_dispatch.notify_all();
+    if (srv->dispatcher.joinable())
+        srv->dispatcher.join();
+    srv->cv_complete.notify_all();
+    if (srv->completer.joinable())
+        srv->completer.join();
+    cudaSetDevice(srv->eng->device);
+    for (auto &sl : srv->slots) {
+        if (sl.stream)
+            cudaStreamSynchronize(sl.stream);
+        cudaFreeHost(sl.h_in);
+        cudaFreeHost(sl.h_err);
+        cudaFreeHost(sl.h_w);
+        cudaFree(sl.d_in);
+        cudaFree(sl.d_err);
+        cudaFree(sl.d_w);
+        cudaFree(sl.d_synd);
+        cudaFree(sl.d_loc);
+        cudaFree(sl.d_counter);
+        if (sl.done)
+            cudaEventDestroy(sl.done);
+        if (sl.stream)
+            cudaStreamDestroy(sl.stream);
+    }
+    for (auto &k : srv->keys)
+        if (k.key)
+            cmd_key_free(k.key);
+    if (srv->device_bytes)
+        budget_give(srv->eng, srv->device_bytes);
+    delete srv;
+}
+
+int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t sk_len, uint32_t *key_id)
+{
+    if (!srv || !h_sk || !key_id || !valid_set(set) || sk_len != (size_t)set_info(set).sk)
+        return CMD_E_ARG;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    KeyEntry ke;
+    ke.set = set;
+    ke.sk.assign(h_sk, h_sk + sk_len);
+    srv->keys.push_back(std::move(ke));
+    *key_id = (uint32_t)(srv->keys.size() - 1);
+    return CMD_OK;
+}
+
+int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uint8_t *h_err_out, uint64_t tag)
+{
+    if (!srv || !h_ct)
+        return CMD_E_ARG;
+    Request r;
+    r.key_id = key_id;
+    r.tag = tag;
+    r.err_out = h_err_out;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        if (key_id >= srv->keys.size())
+            return CMD_E_ARG;
+        if (srv->stop)
+            return CMD_E_ARG;
+        if (srv->pending.size() >= srv->cfg.queue_capacity) {
+            srv->refused++;
+            return CMD_E_BUSY;
+        }
+        const int ctb = set_info(srv->keys[key_id].set).ct;
+        memcpy(r.ct, h_ct, ctb);
+        memset(r.ct + ctb, 0, CT_STRIDE - ctb);
+        r.t_arrive = now_ns();
+        if (srv->submitted++ == 0)
+            srv->t_first = r.t_arrive;
+        srv->pending.push_back(r);
+    }
+    srv->cv_dispatch.notify_one();
+    return CMD_OK;
+}
+
+int cmd_server_poll(cmd_server *srv, cmd_completion *out, size_t max, size_t *n, uint32_t timeout_us)
+{
+    if (!srv || !n || (max && !out))
+        return CMD_E_ARG;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    if (srv->completions.empty() && timeout_us)
+        srv->cv_poll.wait_for(lk, std::chrono::microseconds(timeout_us), [&] { return !srv->completions.empty(); });
+    size_t k = 0;
+    while (k < max && !srv->completions.empty()) {
+        out[k++] = srv->completions.front();
+        srv->completions.pop_front();
+    }
+    *n = k;
+    return srv->status;
+}
+
+int cmd_server_drain(cmd_server *srv, uint32_t timeout_ms)
+{
+    if (!srv)
+        return CMD_E_ARG;
+    std::unique_lock<std::mutex> lk(srv->mu);
+    const bool ok = srv->cv_poll.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] {
+        return srv->completed + 0 >= srv->submitted;
+    });
+    if (!ok)
+        return CMD_E_TIMEOUT;
+    return srv->status;
+}
+
+int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
+{
+    if (!srv || !st)
+        return CMD_E_ARG;
+    std::lock_guard<std::mutex> lk(srv->mu);
+    memset(st, 0, sizeof *st);
+    st->submitted = srv->submitted;
+    st->completed = srv->completed;
+    st->refused = srv->refused;
+    st->batches = srv->batches;
+    st->fused_batches = srv->fused_batches;
+    st->mean_batch = srv->batches ? (double)srv->batched_cts / srv->batches : 0;
+    st->resident_keys = 0;
+    for (const auto &k : srv->keys)
+        st->resident_keys += k.key != nullptr;
+    if (!srv->lat_ns.empty()) {
+        std::vector<uint32_t> v = srv->lat_ns;
+        auto q = [&](double f) {
+            size_t i = (size_t)(f * (v.size() - 1));
+            std::nth_element(v.begin(), v.begin() + i, v.end());
+            return v[i] / 1e3;
+        };
+        st->p50_us = q(0.50);
+        st->p99_us = q(0.99);
+        st->max_us = *std::max_element(v.begin(), v.end()) / 1e3;
+        double sum = 0;
+        for (uint32_t x : v)
+            sum += x;
+        st->mean_us = sum / v.size() / 1e3;
+    }
+    if (srv->t_last > srv->t_first)
+        st->decaps_per_s = srv->completed / ((srv->t_last - srv->t_first) * 1e-9);
+    if (reset) {
+        srv->lat_ns.clear();
+        srv->submitted -= srv->completed;
+        srv->completed = 0;
+        srv->refused = srv->batches = srv->fused_batches = srv->batched_cts = 0;
+        srv->t_first = srv->t_last = 0;
+    }
+    return CMD_OK;
+}
+
+// Open-loop Poisson load: submits requests from a pool (request i uses key
+// key_ids[i % pool] and ciphertext i % pool; results land in err_pool rows)
+// at exponentially distributed inter-arrival times of mean 1/rate, for
+// `seconds`, then waits for every request to complete.
+int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *cts, size_t ct_stride,
+                       uint8_t *err_pool, size_t err_stride, size_t pool, double rate_per_s, double seconds,
+                       uint64_t seed, cmd_server_stats *out)
+{
+    if (!srv || !key_ids || !cts || !pool || rate_per_s <= 0 || seconds <= 0 || !out)
+        return CMD_E_ARG;
+    cmd_server_stats dummy;
+    cmd_server_stats_get(srv, &dummy, 1);
+    std::mt19937_64 rng(seed);
+    std::exponential_distribution<double> gap(rate_per_s);
+    const uint64_t t0 = now_ns();
+    const uint64_t t_end = t0 + (uint64_t)(seconds * 1e9);
+    double next = (double)t0;
+    size_t i = 0;
+    uint64_t busy = 0;
+    while (true) {
+        next += gap(rng) * 1e9;
+        if (next >= (double)t_end)
+            break;
+        while ((double)now_ns() < next) {
+        }
+        const size_t k = i % pool;
+        int rc = cmd_server_submit(srv, key_ids[k], cts + k * ct_stride, err_pool ? err_pool + k * err_stride : nullptr,
+                                   i);
+        if (rc == CMD_E_BUSY)
+            busy++;
+        else if (rc != CMD_OK)
+            return rc;
+        i++;
+    }
+    int rc = cmd_server_drain(srv, 60000);
+    cmd_server_stats_get(srv, out, 0);
+    out->offered_per_s = i / seconds;
+    (void)busy;
+    return rc;
+}
+
+}  // extern "C"

@@ -193,6 +193,87 @@ int cmd_decrypt_files(cmd_engine *eng, cmd_set set, const char *sk_path,
                       const char *errorstream_path, cmd_path path,
                       double *out_seconds);
 
+/* ---- serving loop (no reference counterpart) ---------------------------- */
+/* Continuous batching of single-ciphertext decapsulation requests over many
+ * keys and parameter sets.  A dispatcher forms a batch whenever one of
+ * `slots` batch slots is free and requests wait: at once when nothing is on
+ * the GPU, otherwise after the oldest request has waited max_wait_us for
+ * batch-mates (or the batch is full).  Batches of different slots overlap on
+ * the device.  Keys registered with cmd_server_add_key are expanded on first
+ * use and stay resident; least recently used keys are evicted when the
+ * engine's HBM budget is full.  Batches of at least fused_threshold requests
+ * run the fused kernel, smaller ones the multi-key plain kernels
+ * (fused_threshold 0: always plain). */
+typedef struct cmd_server cmd_server;
+typedef struct {
+    uint32_t max_batch;          /* requests per batch, 1..65536              */
+    uint32_t slots;              /* batches in flight, 1..16                  */
+    uint32_t max_wait_us;        /* batching delay bound while the GPU is busy */
+    uint32_t queue_capacity;     /* waiting requests before CMD_E_BUSY        */
+    uint32_t fused_threshold;    /* batch size from which the fused kernel runs */
+    uint32_t record_completions; /* 1: queue a cmd_completion per request     */
+} cmd_server_config;
+typedef struct {
+    uint64_t tag;        /* caller's tag from cmd_server_submit           */
+    int32_t status;      /* CMD_OK or the batch's error                   */
+    uint16_t weight;     /* flagged positions                             */
+    uint16_t reserved;
+    uint64_t latency_ns; /* submit -> result in the caller's buffer        */
+} cmd_completion;
+typedef struct {
+    uint64_t submitted, completed, refused, batches, fused_batches, resident_keys;
+    double mean_batch, p50_us, p99_us, max_us, mean_us;
+    double decaps_per_s;  /* completed / (last completion - first arrival)  */
+    double offered_per_s; /* cmd_server_loadgen: arrival rate actually offered */
+} cmd_server_stats;
+
+int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server **out);
+/* Finishes every accepted request, then releases the server and its keys. */
+void cmd_server_destroy(cmd_server *srv);
+int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t sk_len,
+                       uint32_t *key_id);
+/* Queues one ciphertext (ct_bytes of key_id's set); on completion err_bytes
+ * of packed error bits are written to h_err_out (may be NULL).  Non-blocking;
+ * CMD_E_BUSY when queue_capacity requests are waiting. */
+int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uint8_t *h_err_out,
+                      uint64_t tag);
+/* Up to max completions (waits up to timeout_us for the first).  Returns the
+ * server's sticky status (CMD_OK unless a batch failed). */
+int cmd_server_poll(cmd_server *srv, cmd_completion *out, size_t max, size_t *n, uint32_t timeout_us);
+/* Waits until every accepted request has completed (CMD_E_TIMEOUT after timeout_ms). */
+int cmd_server_drain(cmd_server *srv, uint32_t timeout_ms);
+int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *out, int reset);
+/* Open-loop Poisson load for `seconds` at rate_per_s: request i uses
+ * key_ids[i % pool] and ciphertext i % pool (ct_stride bytes apart) and writes
+ * its result to err_pool row i % pool (err_stride bytes apart; may be NULL).
+ * Statistics are reset first and returned in *out after a full drain. */
+int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *cts, size_t ct_stride,
+                       uint8_t *err_pool, size_t err_stride, size_t pool, double rate_per_s,
+                       double seconds, uint64_t seed, cmd_server_stats *out);
+
+/* ---- fused-kernel tuning and graph replay (no reference counterpart) --- */
+/* Picks the fused kernel's launch configuration for key's set on this GPU
+ * (warps per CTA 4|8, equal-share or full rounds) by timing the candidates on
+ * sample_count ciphertexts (0 = about three waves).  Results are cached in the
+ * engine and in $CMD_TUNE_CACHE (JSON keyed by GPU name and set); a cached
+ * entry is reused unless force != 0. */
+int cmd_tune(cmd_engine *eng, const cmd_key *key, size_t sample_count, int force);
+int cmd_engine_fused_config(cmd_engine *eng, cmd_set set, int *wpb, int *balanced,
+                            double *ns_per_ct);
+int cmd_engine_set_fused_config(cmd_engine *eng, cmd_set set, int wpb, int balanced);
+
+/* A decrypt over fixed device buffers captured as a CUDA graph and replayed
+ * with cmd_graph_launch (asynchronous on `stream`, NULL = engine stream).
+ * A fused-path graph owns its work counter; a plain-path graph uses the
+ * engine's scratch, so do not replay it concurrently with other plain-path
+ * work of the same engine. */
+typedef struct cmd_graph cmd_graph;
+int cmd_graph_capture(cmd_engine *eng, const cmd_key *key, cmd_path path,
+                      const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                      uint16_t *d_weight, cmd_graph **out);
+int cmd_graph_launch(cmd_graph *graph, void *stream);
+void cmd_graph_destroy(cmd_graph *graph);
+
 /* ---- measurement (no reference counterpart) ---------------------------- */
 /* Integer-ALU roofline denominator: the device's sustained lop3.b32 rate in
  * lane-operations per second (32 per warp instruction), measured with
