@@ -172,7 +172,7 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
         planted[idx, : e.shape[1]] = e
         valid[idx] = v
     out = {"keys": len(keys), "keygen_s": keygen_s, "malformed_fraction": float(1 - valid.mean()), "points": []}
-    with cmd.Server(eng, max_batch=4096, slots=4, max_wait_us=150, fused_threshold=4096,
+    with cmd.Server(eng, max_batch=8192, slots=4, max_wait_us=100, fused_threshold=0,
                     record_completions=False) as srv:
         ids = np.array([srv.add_key(s, sk) for s, sk, _ in keys], np.uint32)
         err_pool = np.zeros((pool, 1024), np.uint8)
@@ -400,7 +400,7 @@ def main() -> None:
         g_.close()
     if world == 1 and not args.no_serve:
         fused_rate = value
-        rates = sorted({2e4, 1e5, 3e5, 6e5, min(2e6, 0.5 * fused_rate), min(2e6, 0.8 * fused_rate)})
+        rates = sorted({1e4, 1e5, 5e5, 1e6, min(2e6, 0.5 * fused_rate), min(2e6, 0.7 * fused_rate), 2e6})
         line["serving"] = serving_leg(cmd, eng, args.serve_keys, rates, args.serve_seconds)
         line["serving"]["fused_batch_decaps_per_s"] = fused_rate
         best = line["serving"]["max_decaps_per_s_p99_under_1ms"]

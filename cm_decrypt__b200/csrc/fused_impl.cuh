@@ -17,7 +17,11 @@
 //  4. Berlekamp-Massey (bm.c:12-68) bitsliced across the 32 ciphertexts: lane
 //     l owns locator coefficients l, l+32, ... in registers, the discrepancy is
 //     a shuffle-XOR reduction, B lives in a shared ring buffer whose rotation
-//     implements the x*B shift, d/b uses a bitsliced inversion chain;
+//     implements the x*B shift.  The update is the scaled form C <- b*C +
+//     d*x*B instead of bm()'s C <- C + (d/b)*x*B: same decisions (d != 0,
+//     N >= 2L), same truncation, and by induction the result is lambda times
+//     bm()'s locator with lambda a product of nonzero b values -- the same
+//     roots, so the same flagged positions, with no inversion chain per step;
 //  5. root search (root_13.c:216-240) per ciphertext: lanes take 32-point
 //     support words, coefficients become broadcast plane masks, Horner runs
 //     bitsliced; the zero test gives the packed error word directly and the
@@ -201,10 +205,10 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
                 C[j][k] = (j == 0 && k == 0 && lane == 0) ? FULLMASK : 0u;
         for (int v = lane; v < R * M; v += 32)
             ring[v] = (v == M) ? FULLMASK : 0u;  // B = x
-        uint32_t binv[M];
+        uint32_t bb[M];
 #pragma unroll
         for (int k = 0; k < M; k++)
-            binv[k] = k == 0 ? FULLMASK : 0u;     // 1/b with b = 1
+            bb[k] = k == 0 ? FULLMASK : 0u;       // b = 1
         int Lq = 0;                               // L of ciphertext `lane`
         __syncwarp();
 #pragma unroll 1
@@ -231,22 +235,15 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
             uint32_t mne = 0;
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                uint32_t v = p[k];
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1)
-                    v ^= __shfl_xor_sync(FULLMASK, v, off);
+                const uint32_t v = __reduce_xor_sync(FULLMASK, p[k]);
                 d[k] = v;
                 mne |= v;
             }
             const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
             const uint32_t mle = __ballot_sync(FULLMASK, my_mle);
             Lq = my_mle ? N + 1 - Lq : Lq;
-            uint32_t f[M], dinv[M];
-            bs_mul<M>(f, d, binv);        // f = d / b (0 where d = 0)
-            bs_inv<M>(dinv, d);
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                binv[k] = (binv[k] & ~mle) | (dinv[k] & mle);
+            // Scaled update C <- b*C + d*x*B (see the note at the top of the
+            // file): both products accumulate unreduced, one reduction.
             int off = (R - (N % R)) % R;  // slot(i) = (i - N) mod R
 #pragma unroll
             for (int j = 0; j < NJ; j++) {
@@ -255,19 +252,27 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
                     int slot = i + off;
                     slot = slot >= R ? slot - R : slot;
                     uint32_t *bp = ring + slot * M;
-                    uint32_t bv[M], tv[M];
+                    uint32_t bv[M], q[2 * M - 1];
 #pragma unroll
                     for (int k = 0; k < M; k++)
                         bv[k] = bp[k];
-                    bs_mul<M>(tv, f, bv);
+#pragma unroll
+                    for (int k = 0; k < 2 * M - 1; k++)
+                        q[k] = 0;
+                    bs_mul_acc<M>(q, bb, C[j]);
+                    bs_mul_acc<M>(q, d, bv);
+                    bs_reduce<M>(q);
 #pragma unroll
                     for (int k = 0; k < M; k++) {
                         const uint32_t oc = C[j][k];
-                        C[j][k] = oc ^ tv[k];
+                        C[j][k] = q[k];
                         bp[k] = (bv[k] & ~mle) | (oc & mle);
                     }
                 }
             }
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bb[k] = (bb[k] & ~mle) | (d[k] & mle);
             // Slot of B_{t+1} at this N becomes B_0 = 0 at N+1.
             const int freeslot = (R - ((N + 1) % R)) % R;
             if (lane < M)

@@ -85,11 +85,19 @@ struct FusedArgs {
 cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,
                          LaunchCounter lc);
 
-// Multi-key plain path (serving loop, small batches): syndrome, BM and root
-// kernels for `count` ciphertexts of one set, each naming its own key.
-cudaError_t launch_keys_path(int set, const FusedKeyRef *d_keys, const uint32_t *d_key_idx, const uint8_t *d_cts,
-                             uint32_t ct_stride, size_t count, uint32_t *d_synd, uint16_t *d_loc, uint32_t *d_err,
-                             uint32_t err_stride, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc);
+// Latency path (serving loop; latency.cu): one work item per ciphertext.
+struct LatItem {
+    const uint32_t *tab;  // key's syndrome table
+    const uint32_t *Lbs;  // key's bitsliced support
+    uint32_t ct_off;      // byte offset of the ciphertext in the batch
+    uint32_t err_off;     // word offset of the error row in the batch
+    int32_t set;
+    int32_t pad;
+};
+// Tile path: ntiles tiles of 32 item slots (LatItem.pad = tile count, padding
+// slots set -1); d_loc_bs holds ntiles * 130 * 16 words.
+cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_loc_bs,
+                             uint32_t *d_err, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc);
 
 void set_last_error(const std::string &msg);
 

@@ -120,10 +120,7 @@ template <int S> __global__ void __launch_bounds__(256) k_bm_plain(const uint16_
             if (i <= lim)
                 part ^= gf_mul<M>(C[j], s[N - i]);
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-            part ^= __shfl_xor_sync(FULL, part, off);
-        const uint32_t d = part;
+        const uint32_t d = __reduce_xor_sync(FULL, part);
         const uint32_t mne = 0u - (uint32_t)(d != 0);
         const uint32_t mle = mne & (0u - (uint32_t)((uint32_t)N >= 2 * L));
         const uint32_t f = gf_frac<M>(b, d);
@@ -248,137 +245,6 @@ template <int S> __global__ void __launch_bounds__(256) k_root_images(const uint
     for (int j = P::T - 1; j >= 0; j--)
         r = gf_mul<P::M>(r, a) ^ f[j];
     images[idx] = (uint16_t)r;
-}
-
-// ------------------------------------------------- multi-key latency path
-// Used by the serving loop for small batches: every ciphertext may name a
-// different key (of this launch's set).  Syndrome: warp per ciphertext,
-// reading its own key's table rows straight from L2 (coalesced across the
-// lanes).  Root search: one CTA per ciphertext so a lone ciphertext finishes
-// in one short pass over its support words.  Ciphertexts sit at a fixed
-// stride (ct_stride bytes), error rows at err_stride words.
-template <int S> __global__ void __launch_bounds__(256) k_synd_keys(const FusedKeyRef *__restrict__ keys,
-                                                                    const uint32_t *__restrict__ key_idx,
-                                                                    const uint8_t *__restrict__ cts,
-                                                                    uint32_t ct_stride, size_t count,
-                                                                    uint32_t *__restrict__ synd)
-{
-    using P = Set<S>;
-    constexpr int TW = P::TW, TWP = P::TWP, KW = (TW + 31) / 32;
-    __shared__ __align__(16) uint8_t s_ct[8][(P::CT + 15) / 16 * 16];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const size_t c = (size_t)blockIdx.x * 8 + warp;
-    if (c >= count)
-        return;
-    for (int v = lane; v < P::CT; v += 32)
-        s_ct[warp][v] = cts[c * ct_stride + v];
-    __syncwarp();
-    const uint32_t *tab = keys[key_idx[c]].tab;
-    uint32_t acc[KW];
-#pragma unroll
-    for (int k = 0; k < KW; k++)
-        acc[k] = 0;
-#pragma unroll 4
-    for (int b = 0; b < P::SB; b++) {
-        const uint32_t mask = 0u - ((s_ct[warp][b >> 3] >> (b & 7)) & 1u);
-        const uint32_t *row = tab + (size_t)b * TWP;
-#pragma unroll
-        for (int k = 0; k < KW; k++) {
-            const int w = lane + 32 * k;
-            if (w < TW)
-                acc[k] ^= __ldg(row + w) & mask;
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < KW; k++) {
-        const int w = lane + 32 * k;
-        if (w < TW)
-            synd[c * TW + w] = acc[k];
-    }
-}
-
-template <int S>
-__global__ void __launch_bounds__(root_threads<S>()) k_root_keys(const FusedKeyRef *__restrict__ keys,
-                                                                 const uint32_t *__restrict__ key_idx,
-                                                                 const uint16_t *__restrict__ loc, size_t count,
-                                                                 uint32_t *__restrict__ err, uint32_t err_stride,
-                                                                 uint16_t *__restrict__ weight)
-{
-    using P = Set<S>;
-    constexpr int M = P::M, T = P::T, NW = P::NW;
-    constexpr int NWARP = root_threads<S>() / 32;
-    __shared__ __align__(16) uint32_t s_mask[T + 1][16];
-    __shared__ int s_cnt[NWARP];
-    const int w = threadIdx.x, lane = w & 31, warp = w >> 5;
-    const size_t c = blockIdx.x;
-    if (c >= count)
-        return;
-    const uint32_t *Lbs = keys[key_idx[c]].Lbs;
-    const uint16_t *f = loc + c * (T + 1);
-    for (int e = threadIdx.x; e < (T + 1) * 16; e += blockDim.x) {
-        const int i = e >> 4, k = e & 15;
-        s_mask[i][k] = k < M ? 0u - ((uint32_t)(__ldg(f + i) >> k) & 1u) : 0u;
-    }
-    uint32_t a[M];
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        a[k] = w < NW ? __ldg(Lbs + k * NW + w) : 0u;
-    __syncthreads();
-    uint32_t r[M];
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        r[k] = s_mask[T][k];
-    for (int i = T - 1; i >= 0; i--) {
-        uint32_t p[2 * M - 1];
-#pragma unroll
-        for (int k = 0; k < 2 * M - 1; k++)
-            p[k] = k < M ? s_mask[i][k] : 0u;
-        bs_mul_acc<M>(p, r, a);
-        bs_reduce<M>(p);
-#pragma unroll
-        for (int k = 0; k < M; k++)
-            r[k] = p[k];
-    }
-    uint32_t any = 0;
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        any |= r[k];
-    const int left = P::N - 32 * w;
-    const uint32_t valid = w >= NW ? 0u : (left >= 32 ? FULL : ((1u << left) - 1u));
-    const uint32_t z = ~any & valid;
-    if (w < NW)
-        err[c * err_stride + w] = z;
-    int cnt = __popc(z);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-        cnt += __shfl_xor_sync(FULL, cnt, off);
-    if (lane == 0)
-        s_cnt[warp] = cnt;
-    __syncthreads();
-    if (w == 0 && weight) {
-        int tot = 0;
-#pragma unroll
-        for (int q = 0; q < NWARP; q++)
-            tot += s_cnt[q];
-        weight[c] = (uint16_t)tot;
-    }
-}
-
-cudaError_t launch_keys_path(int set, const FusedKeyRef *d_keys, const uint32_t *d_key_idx, const uint8_t *d_cts,
-                             uint32_t ct_stride, size_t count, uint32_t *d_synd, uint16_t *d_loc, uint32_t *d_err,
-                             uint32_t err_stride, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc)
-{
-    if (count == 0)
-        return cudaSuccess;
-    return dispatch_set(set, [&]<int S>() -> cudaError_t {
-        const unsigned g8 = (unsigned)((count + 7) / 8);
-        k_synd_keys<S><<<g8, 256, 0, s>>>(d_keys, d_key_idx, d_cts, ct_stride, count, d_synd);
-        k_bm_plain<S><<<g8, 256, 0, s>>>(reinterpret_cast<const uint16_t *>(d_synd), count, d_loc);
-        k_root_keys<S><<<(unsigned)count, root_threads<S>(), 0, s>>>(d_keys, d_key_idx, d_loc, count, d_err,
-                                                                     err_stride, d_weight);
-        lc.bump(3);
-        return cudaGetLastError();
-    });
 }
 
 // ------------------------------------------------------------------ launch

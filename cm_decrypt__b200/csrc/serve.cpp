@@ -13,9 +13,9 @@
 //  * Expanded keys stay resident in HBM; a key is expanded on first use and
 //    the least recently used unpinned keys are evicted when the engine's HBM
 //    budget is full (admission by budget).
-//  * Small batches run the multi-key plain kernels (a short pass per
-//    ciphertext, lowest latency); batches of fused_threshold or more run the
-//    fused kernel (highest throughput).
+//  * Small batches run the latency kernels of latency.cu (any mix of keys and
+//    sets in three launches, a short pass per ciphertext); batches of
+//    fused_threshold or more run the fused kernel (highest throughput).
 //  * A completer thread waits for slots in dispatch order, copies each
 //    result to its request's buffer and records arrival-to-completion
 //    latency for the p50/p99 statistics.
@@ -68,8 +68,9 @@ struct Slot {
     uint8_t *h_in = nullptr, *d_in = nullptr;  // packed inputs (see dispatch)
     uint32_t *h_err = nullptr, *d_err = nullptr;
     uint16_t *h_w = nullptr, *d_w = nullptr;
-    uint32_t *d_synd = nullptr;
-    uint16_t *d_loc = nullptr;
+    uint32_t *d_locbs = nullptr;        // tile path: bitsliced locators
+    std::vector<uint32_t> slot_of;      // request i -> result row (item slot)
+    size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
     std::vector<Request> reqs;
     std::vector<uint32_t> pinned;  // key ids pinned by this batch
@@ -110,10 +111,16 @@ struct cmd_server {
 
 namespace {
 
+// Result rows a batch of B requests may need: the tile path pads each set's
+// run of requests to whole 32-request tiles.
+size_t row_cap(size_t B) { return B + NSETS * 32; }
+size_t tile_cap(size_t B) { return B / 32 + NSETS + 1; }
+
 // Input packing of a slot: ciphertexts at CT_STRIDE, then key index per
-// ciphertext, then (fused) ct_off, err_off, order, tiles, key table.
+// ciphertext, then (fused) ct_off, err_off, order, tiles, key table, then
+// (tile path) the work items.
 struct InLayout {
-    size_t cts, key_idx, ct_off, err_off, order, tiles, keys, total;
+    size_t cts, key_idx, ct_off, err_off, order, tiles, keys, items, total;
     InLayout(size_t B, size_t max_keys)
     {
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -124,7 +131,8 @@ struct InLayout {
         order = al(err_off + B * 8);
         tiles = al(order + B * 4);
         keys = al(tiles + B * sizeof(FusedTile));
-        total = al(keys + max_keys * sizeof(FusedKeyRef));
+        items = al(keys + max_keys * sizeof(FusedKeyRef));
+        total = al(items + row_cap(B) * sizeof(LatItem));
     }
 };
 
@@ -223,49 +231,51 @@ int cmd_server::launch(Slot &sl)
     cudaStream_t s = sl.stream;
     cudaError_t e;
     sl.fused = cfg.fused_threshold > 0 && B >= cfg.fused_threshold;
+    sl.slot_of.resize(B);
     if (!sl.fused) {
-        // Plain multi-key path, one launch group per set: reorder the batch by
-        // set so each set's ciphertexts are contiguous.
-        std::vector<uint32_t> perm(B);
+        // Tile path: requests grouped by set into tiles of up to 32 (any keys
+        // within a tile); item slot 32*t + q is request q of tile t.
+        LatItem *items = reinterpret_cast<LatItem *>(sl.h_in + lay.items);
+        std::vector<uint32_t> by_set(B);
         for (size_t i = 0; i < B; i++)
-            perm[i] = (uint32_t)i;
-        std::stable_sort(perm.begin(), perm.end(),
+            by_set[i] = (uint32_t)i;
+        std::stable_sort(by_set.begin(), by_set.end(),
                          [&](uint32_t a, uint32_t b) { return kset[key_idx[a]] < kset[key_idx[b]]; });
-        std::vector<Request> sorted(B);
-        std::vector<uint32_t> ki(B);
-        for (size_t i = 0; i < B; i++) {
-            sorted[i] = sl.reqs[perm[i]];
-            ki[i] = key_idx[perm[i]];
-        }
-        sl.reqs.swap(sorted);
-        for (size_t i = 0; i < B; i++) {
-            key_idx[i] = ki[i];
-            memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
-        }
-        if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-            return cuda_fail(e, "server H2D");
-        const FusedKeyRef *d_keys = reinterpret_cast<const FusedKeyRef *>(sl.d_in + lay.keys);
+        uint32_t ntiles = 0;
         size_t i = 0;
         while (i < B) {
-            const int set = kset[key_idx[i]];
+            const int set = kset[key_idx[by_set[i]]];
             size_t j = i;
-            while (j < B && kset[key_idx[j]] == set)
+            while (j < B && kset[key_idx[by_set[j]]] == set && j - i < 32)
                 j++;
-            const SetInfo si = set_info(set);
-            e = launch_keys_path(set, d_keys, reinterpret_cast<const uint32_t *>(sl.d_in + lay.key_idx) + i,
-                                 sl.d_in + lay.cts + i * CT_STRIDE, CT_STRIDE, j - i, sl.d_synd + i * 128,
-                                 sl.d_loc + i * 129, sl.d_err + i * ERR_STRIDE, ERR_STRIDE, sl.d_w + i, s, lc);
-            (void)si;
-            if (e != cudaSuccess)
-                return cuda_fail(e, "server plain launch");
+            const uint32_t cnt = (uint32_t)(j - i);
+            for (uint32_t q = 0; q < 32; q++) {
+                const uint32_t slot = 32 * ntiles + q;
+                if (q < cnt) {
+                    const uint32_t r = by_set[i + q];
+                    const FusedKeyRef &kr = krefs[key_idx[r]];
+                    items[slot] = LatItem{kr.tab, kr.Lbs, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE, kr.set, cnt};
+                    sl.slot_of[r] = slot;
+                } else {
+                    items[slot] = LatItem{krefs[0].tab, krefs[0].Lbs, 0, slot * ERR_STRIDE, -1, cnt};
+                }
+            }
+            ntiles++;
             i = j;
         }
+        sl.rows_used = (size_t)ntiles * 32;
+        if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            return cuda_fail(e, "server H2D");
+        e = launch_tile_path(sl.d_in + lay.items, sl.d_in + lay.cts, ntiles, sl.d_locbs, sl.d_err, sl.d_w, s, lc);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "server tile-path launch");
     } else {
         uint64_t *ct_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.ct_off);
         uint64_t *err_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.err_off);
         for (size_t i = 0; i < B; i++) {
             ct_off[i] = i * CT_STRIDE;
             err_off[i] = i * ERR_STRIDE;
+            sl.slot_of[i] = (uint32_t)i;
         }
         const int single = mixed_single_set(kset.data(), key_idx, B);
         const int wpb = single >= 0 ? eng->fcfg[single].wpb : eng->fcfg_mixed.wpb;
@@ -300,8 +310,11 @@ int cmd_server::launch(Slot &sl)
         if ((e = launch_fused(a, grid, wpb, s, lc)) != cudaSuccess)
             return cuda_fail(e, "server fused launch");
     }
-    if ((e = cudaMemcpyAsync(sl.h_err, sl.d_err, B * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (e = cudaMemcpyAsync(sl.h_w, sl.d_w, B * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+    if (sl.fused)
+        sl.rows_used = B;
+    if ((e = cudaMemcpyAsync(sl.h_err, sl.d_err, sl.rows_used * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) !=
+            cudaSuccess ||
+        (e = cudaMemcpyAsync(sl.h_w, sl.d_w, sl.rows_used * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaEventRecord(sl.done, s)) != cudaSuccess)
         return cuda_fail(e, "server D2H");
     return CMD_OK;
@@ -397,11 +410,12 @@ void cmd_server::complete_loop()
             const Request &r = sl.reqs[i];
             const SetInfo info = set_info(keys[r.key_id].set);
             if (e == cudaSuccess && r.err_out)
-                memcpy(r.err_out, sl.h_err + i * ERR_STRIDE, info.n / 8);
+                memcpy(r.err_out, sl.h_err + (size_t)sl.slot_of[i] * ERR_STRIDE, info.n / 8);
             const uint64_t lat = t - r.t_arrive;
             lats.push_back((uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu));
             if (cfg.record_completions)
-                done.push_back(cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[i], 0, lat});
+                done.push_back(
+                    cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[sl.slot_of[i]], 0, lat});
         }
         lk.lock();
         if (e != cudaSuccess && status == CMD_OK) {
@@ -439,7 +453,8 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
     const size_t B = cfg->max_batch;
     InLayout lay(B, B);
     srv->in_bytes = lay.total;
-    const size_t dev_per_slot = lay.total + B * ERR_STRIDE * 4 + B * 2 + B * 128 * 4 + B * 129 * 2 + 4 * 256;
+    const size_t rows = row_cap(B), locbs = tile_cap(B) * 130 * 16 * 4;
+    const size_t dev_per_slot = lay.total + rows * ERR_STRIDE * 4 + rows * 2 + locbs + 4 * 256;
     srv->device_bytes = dev_per_slot * cfg->slots;
     if (!budget_take(eng, srv->device_bytes)) {
         delete srv;
@@ -456,19 +471,17 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
         if (e == cudaSuccess)
             e = cudaMallocHost(&sl.h_in, lay.total);
         if (e == cudaSuccess)
-            e = cudaMallocHost(&sl.h_err, B * ERR_STRIDE * 4);
+            e = cudaMallocHost(&sl.h_err, rows * ERR_STRIDE * 4);
         if (e == cudaSuccess)
-            e = cudaMallocHost(&sl.h_w, B * 2);
+            e = cudaMallocHost(&sl.h_w, rows * 2);
         if (e == cudaSuccess)
             e = cudaMalloc(&sl.d_in, lay.total);
         if (e == cudaSuccess)
-            e = cudaMalloc(&sl.d_err, B * ERR_STRIDE * 4);
+            e = cudaMalloc(&sl.d_err, rows * ERR_STRIDE * 4);
         if (e == cudaSuccess)
-            e = cudaMalloc(&sl.d_w, B * 2);
+            e = cudaMalloc(&sl.d_w, rows * 2);
         if (e == cudaSuccess)
-            e = cudaMalloc(&sl.d_synd, B * 128 * 4);
-        if (e == cudaSuccess)
-            e = cudaMalloc(&sl.d_loc, B * 129 * 2);
+            e = cudaMalloc(&sl.d_locbs, locbs);
         if (e == cudaSuccess)
             e = cudaMalloc(&sl.d_counter, 256);
     }
@@ -508,8 +521,7 @@ void cmd_server_destroy(cmd_server *srv)
         cudaFree(sl.d_in);
         cudaFree(sl.d_err);
         cudaFree(sl.d_w);
-        cudaFree(sl.d_synd);
-        cudaFree(sl.d_loc);
+        cudaFree(sl.d_locbs);
         cudaFree(sl.d_counter);
         if (sl.done)
             cudaEventDestroy(sl.done);

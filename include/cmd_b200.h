@@ -201,9 +201,11 @@ int cmd_decrypt_files(cmd_engine *eng, cmd_set set, const char *sk_path,
  * batch-mates (or the batch is full).  Batches of different slots overlap on
  * the device.  Keys registered with cmd_server_add_key are expanded on first
  * use and stay resident; least recently used keys are evicted when the
- * engine's HBM budget is full.  Batches of at least fused_threshold requests
- * run the fused kernel, smaller ones the multi-key plain kernels
- * (fused_threshold 0: always plain). */
+ * engine's HBM budget is full; when one batch needs more keys than fit at
+ * once, the requests of the keys that did not fit wait for the next batch.
+ * Batches of at least fused_threshold requests run the fused kernel, smaller
+ * ones the latency kernels (one short pass per ciphertext; fused_threshold 0:
+ * always the latency kernels). */
 typedef struct cmd_server cmd_server;
 typedef struct {
     uint32_t max_batch;          /* requests per batch, 1..65536              */
