@@ -88,12 +88,13 @@ int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
     a.round_cts = round;
     a.total = count;
     a.keys = nullptr;
-    a.key0 = FusedKeyRef{set, 0, key->dev.tab, key->dev.Lbs};
+    a.key0 = key_ref(key->dev);
     a.cts = d_cts;
     a.err = d_err;
     a.weight = d_weight;
     a.tile_counter = counter;
     a.single_set = set;
+    fill_fft(a, eng);
     a.err_stride = (uint32_t)si.nw;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess)
@@ -198,7 +199,7 @@ extern "C" int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *k
     plan_mixed(kset.data(), nkeys, h_key_idx, count, (uint32_t)wpb * 32, order, tiles);
     std::vector<FusedKeyRef> krefs(nkeys);
     for (size_t k = 0; k < nkeys; k++)
-        krefs[k] = FusedKeyRef{keys[k]->dev.set, 0, keys[k]->dev.tab, keys[k]->dev.Lbs};
+        krefs[k] = key_ref(keys[k]->dev);
 
     std::lock_guard<std::mutex> lk(eng->mu);
     int rc = 0;
@@ -244,6 +245,7 @@ extern "C" int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *k
     a.weight = d_weight;
     a.tile_counter = eng->tile_counter;
     a.single_set = single;
+    fill_fft(a, eng);
     size_t smem = 0;
     if (single >= 0)
         smem = fused_smem(single, wpb);

@@ -172,6 +172,11 @@ int cmd_engine_create(int device, size_t hbm_budget_bytes, cmd_engine **out)
         return cuda_fail(e, "cudaStreamCreate");
     }
     snprintf(eng->gpu_name, sizeof eng->gpu_name, "%s", prop.name);
+    if (int rc = upload_fft_plans(eng)) {
+        cudaStreamDestroy(eng->stream);
+        delete eng;
+        return rc;
+    }
     *out = eng;
     return CMD_OK;
 }
@@ -186,6 +191,7 @@ void cmd_engine_destroy(cmd_engine *eng)
     eng->io.release(eng);
     eng->fused.release(eng);
     eng->host_scratch.release();
+    release_fft_plans(eng);
     if (eng->tile_counter)
         cudaFree(eng->tile_counter);
     cudaStreamDestroy(eng->stream);
@@ -219,7 +225,8 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
         return CMD_E_ARG;
     }
     const size_t bytes = carve_size({(size_t)si.n * 2, (size_t)(si.t + 1) * 2, (size_t)si.n * 2,
-                                     (size_t)si.sb * si.twp() * 4, (size_t)si.m * si.nw * 4, (size_t)si.sk});
+                                     (size_t)si.sb * si.twp() * 4, (size_t)si.m * si.nw * 4,
+                                     benes_mask_words(si) * 4, (size_t)si.sk});
     if (!budget_take(eng, bytes)) {
         set_last_error("key does not fit the engine HBM budget");
         return CMD_E_BUDGET;
@@ -245,6 +252,7 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
     key->dev.ginv2 = cv.take<uint16_t>(si.n);
     key->dev.tab = cv.take<uint32_t>((size_t)si.sb * si.twp());
     key->dev.Lbs = cv.take<uint32_t>((size_t)si.m * si.nw);
+    key->dev.bctl = cv.take<uint32_t>(benes_mask_words(si));
     key->dev.sk = cv.take<uint8_t>(si.sk);
     std::lock_guard<std::mutex> lk(eng->mu);
     if ((e = cudaMemcpyAsync(key->dev.sk, h_sk, si.sk, cudaMemcpyHostToDevice, eng->stream)) != cudaSuccess ||

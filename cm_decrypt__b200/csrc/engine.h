@@ -55,6 +55,10 @@ int fused_grid(cmd_engine *eng, int single_set, int wpb, size_t smem, uint64_t r
 int mixed_single_set(const int *key_set, const uint32_t *key_idx, size_t count);
 void plan_mixed(const int *key_set, size_t nkeys, const uint32_t *key_idx, size_t count, uint32_t R,
                 std::vector<uint32_t> &order, std::vector<FusedTile> &tiles);
+// Root-search tables (fft_plan.cpp): uploaded once per engine, budget-charged.
+int upload_fft_plans(cmd_engine *eng);
+void release_fft_plans(cmd_engine *eng);
+inline FusedKeyRef key_ref(const KeyDev &k) { return FusedKeyRef{k.set, 0, k.tab, k.Lbs, k.bctl}; }
 
 }  // namespace cmd
 
@@ -74,7 +78,18 @@ struct cmd_engine {
     std::atomic<uint64_t> launches{0};
     cmd::FusedConfig fcfg[cmd::NSETS];
     cmd::FusedConfig fcfg_mixed;
+    cmd::FftPlanDev fft[cmd::NSETS] = {};  // per-set root-search tables
+    void *fft_mem = nullptr;
+    size_t fft_bytes = 0;
 };
+
+namespace cmd {
+inline void fill_fft(FusedArgs &a, const cmd_engine *eng)
+{
+    for (int s = 0; s < NSETS; s++)
+        a.fft[s] = eng->fft[s];
+}
+}  // namespace cmd
 
 struct cmd_key {
     cmd_engine *eng = nullptr;

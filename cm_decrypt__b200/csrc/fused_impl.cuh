@@ -22,10 +22,20 @@
 //     N >= 2L), same truncation, and by induction the result is lambda times
 //     bm()'s locator with lambda a product of nonzero b values -- the same
 //     roots, so the same flagged positions, with no inversion chain per step;
-//  5. root search (root_13.c:216-240) per ciphertext: lanes take 32-point
-//     support words, coefficients become broadcast plane masks, Horner runs
-//     bitsliced; the zero test gives the packed error word directly and the
-//     flagged-position count is reduced per ciphertext.
+//  5. root search (root_13.c:216-240 evaluates the locator at each support
+//     point): the locator is evaluated at all 2^m field elements by an
+//     additive FFT, then the key's support network (the Benes layers that
+//     generate the support, root_13.c:95-177) carries the zero flags to
+//     support order:
+//     a. radix conversion (scalings g(x) = f(b_d x) and Taylor expansions in
+//        x^2 + x, depth by depth), bitsliced across the 32 ciphertexts;
+//     b. per ciphertext: a 2^m-element bitsliced array (m planes of 2^(m-5)
+//        words) starts from the D-th-level constants and takes D levels of
+//        butterflies A' = A + w*B, B' = A' + B between whole words;
+//     c. zero flags -> the key's 2m-1 swap layers (word swaps across lanes
+//        by shuffle, inside a lane by register, inside a word by shifts) ->
+//        the packed error row and its weight.
+//     The tables of the recursion are per set (fft_plan.cpp).
 #pragma once
 #include "gf.cuh"
 #include "internal.h"
@@ -43,13 +53,19 @@ template <int S> struct Fz {
     static constexpr int M = P::M, T = P::T, NJ = (T + 1 + 31) / 32;
     static constexpr int TWP = (T + 3) / 4 * 4;      // padded table row (words)
     static constexpr int RING = T + 2;               // B ring slots
+    static constexpr int D = fft_depth(T);           // FFT recursion depth
+    static constexpr int NX = 1 << D;                // radix-conversion entries
+    static constexpr int NWD = 1 << (M - 5);         // words of a 2^m-bit array
+    static constexpr int R = NWD / 32;               // of them per lane
     static constexpr int RAW_B = 32 * P::CT;
     static constexpr int RING_B = RING * M * 4;
-    static constexpr int MASK_B = (T + 1) * 16 * 4;
-    static constexpr int A_B = al16(cmax(RAW_B + 16, cmax(RING_B, MASK_B)));
+    static constexpr int FA_B = M * NWD * 4;         // FFT array, plane-major
+    static constexpr int A_B = al16(cmax(cmax(RAW_B + 16, RING_B), FA_B));
     static constexpr int S_B = al16(2 * T * M * 4);  // bitsliced syndromes / locator
     static constexpr int WARP_B = A_B + S_B;
     static constexpr int TAB_B = TAB_ROWS * TWP * 4;  // one chunk buffer
+    static_assert(NX * M * 4 <= S_B, "conversion array must fit the syndrome region");
+    static_assert(D <= M - 5, "butterflies must pair whole words");
 };
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src)
@@ -100,9 +116,9 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     uint8_t *wbase = smem + 2 * Z::TAB_B + warp * Z::WARP_B;
     uint8_t *raw = wbase;                                            // phase 1-2
     uint32_t *ring = reinterpret_cast<uint32_t *>(wbase);            // phase 4
-    uint32_t *masks = reinterpret_cast<uint32_t *>(wbase);           // phase 5
+    uint32_t *fa = reinterpret_cast<uint32_t *>(wbase);              // phase 5
     uint32_t *sS = reinterpret_cast<uint32_t *>(wbase + Z::A_B);     // phase 3-4
-    uint32_t *sC = sS;                                               // phase 4-5
+    uint32_t *cv = sS;                                               // phase 4-5
     const uint32_t *tab = rc.key.tab;
 
     // ---- 1. stage ciphertexts --------------------------------------------
@@ -279,64 +295,176 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
                 ring[freeslot * M + lane] = 0;
             __syncwarp();
         }
+        // The reference's root search evaluates sum_x C[T-x] a^x
+        // (bm.c:62-65 reverses the locator): entry x of the conversion array
+        // is C[T-x], zero for T < x < 2^D.
 #pragma unroll
         for (int j = 0; j < NJ; j++) {
             const int i = lane + 32 * j;
             if (i <= T)
 #pragma unroll
                 for (int k = 0; k < M; k++)
-                    sC[i * M + k] = C[j][k];
+                    cv[(T - i) * M + k] = C[j][k];
         }
+        for (int v = lane; v < (Z::NX - T - 1) * M; v += 32)
+            cv[(T + 1) * M + v] = 0u;
         __syncwarp();
     }
 
-    // ---- 5. root search + pack, one ciphertext at a time ------------------
-    const uint32_t *Lbs = rc.key.Lbs;
-    for (int q = 0; q < ntile; q++) {
-        for (int v = lane; v < (T + 1) * M; v += 32) {
-            const int i = v / M, k = v - (v / M) * M;
-            masks[i * 16 + k] = 0u - ((sC[v] >> q) & 1u);
-        }
-        __syncwarp();
-        const uint64_t c = ct_index(rc, warp, q);
-        uint32_t *erow = a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride);
-        int cnt = 0;
-        for (int w = lane; w < NW; w += 32) {
-            uint32_t av[M], r[M];
-#pragma unroll
-            for (int k = 0; k < M; k++) {
-                av[k] = __ldg(Lbs + k * NW + w);
-                r[k] = masks[k];  // coefficient C[0] = f[t]
-            }
+    // ---- 5. root search ----------------------------------------------------
+    constexpr int D = Z::D, NX = Z::NX, NWD = Z::NWD, R = Z::R;
+    const FftPlanDev pl = a.fft[S];
+    // 5a. radix conversion of the 32 locators at once.  Depth d: scale entry
+    // x by b_d^(x >> d) (b_0 = 1), then expand every stride-2^d sub-array in
+    // x^2 + x: for block sizes n = 2^k down to 4, third quarter ^= fourth,
+    // then second ^= third.  Afterwards entry s is the depth-D constant of
+    // the sub-problem whose Taylor choices are the bits of s.
 #pragma unroll 1
-            for (int i = 1; i <= T; i++) {
-                uint32_t p[2 * M - 1];
-                const uint32_t *mrow = masks + i * 16;
+    for (int d = 0; d < D; d++) {
+        if (d > 0) {
+            for (int x = lane; x < NX; x += 32) {
+                const uint32_t c = __ldg(pl.scalpow + d * 256 + (x >> d));
+                uint32_t v[M], cm[M], p[2 * M - 1];
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    v[k] = cv[x * M + k];
+                    cm[k] = 0u - ((c >> k) & 1u);
+                }
 #pragma unroll
                 for (int k = 0; k < 2 * M - 1; k++)
-                    p[k] = k < M ? mrow[k] : 0u;
-                bs_mul_acc<M>(p, r, av);
+                    p[k] = 0;
+                bs_mul_acc<M>(p, v, cm);
                 bs_reduce<M>(p);
 #pragma unroll
                 for (int k = 0; k < M; k++)
-                    r[k] = p[k];
+                    cv[x * M + k] = p[k];
             }
+            __syncwarp();
+        }
+#pragma unroll 1
+        for (int kb = D - d; kb >= 2; kb--) {
+            const int Q = 1 << (kb - 2);
+#pragma unroll 1
+            for (int h = 2; h >= 1; h--) {  // h = 2: third ^= fourth; h = 1: second ^= third
+                for (int u = lane; u < (NX / 4) * M; u += 32) {
+                    const int e = u / M, k = u - e * M;
+                    const int sub = e & ((1 << d) - 1), rest = e >> d;
+                    const int i = (rest >> (kb - 2)) * 4 * Q + h * Q + (rest & (Q - 1));
+                    cv[((i << d) + sub) * M + k] ^= cv[(((i + Q) << d) + sub) * M + k];
+                }
+                __syncwarp();
+            }
+        }
+    }
+
+    const uint32_t *bctl = rc.key.bctl;
+    for (int q = 0; q < ntile; q++) {
+        // 5b. position Y of the array holds f at the field element
+        // bitrev_m(Y); at depth D it holds the constant of sub-problem
+        // bitrev_D(Y >> (m - D)), one constant per group of words.
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int w = lane + 32 * j;
+            const int sidx = (int)(__brev((uint32_t)(w >> (M - D - 5))) >> (32 - D));
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                fa[k * NWD + w] = 0u - ((cv[sidx * M + k] >> q) & 1u);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int d = D - 1; d >= 0; d--) {
+            const int sbit = M - d - 6, Sw = 1 << sbit;
+            const uint32_t *twd = pl.tw + (size_t)((1 << (M - 5)) - (1 << (M - 5 - d))) * 16;
+#pragma unroll 1
+            for (int j = 0; j < R / 2; j++) {
+                const int P2 = lane + 32 * j;
+                const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
+                const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+                uint32_t A[M], B[M], G[M], p[2 * M - 1];
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    A[k] = fa[k * NWD + wa];
+                    B[k] = fa[k * NWD + wa + Sw];
+                    G[k] = __ldg(g + k);
+                }
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    p[k] = 0;
+                bs_mul_acc<M>(p, G, B);
+                bs_reduce<M>(p);
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    const uint32_t na = A[k] ^ p[k];
+                    fa[k * NWD + wa] = na;
+                    fa[k * NWD + wa + Sw] = na ^ B[k];
+                }
+            }
+            __syncwarp();
+        }
+        // 5c. zero flags, the key's swap layers, the error row.
+        uint32_t z[R];
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int w = lane + 32 * j;
             uint32_t any = 0;
 #pragma unroll
             for (int k = 0; k < M; k++)
-                any |= r[k];
-            const int left = P::N - 32 * w;
-            const uint32_t valid = left >= 32 ? FULLMASK : ((1u << left) - 1u);
-            const uint32_t z = ~any & valid;
-            erow[w] = z;
-            cnt += __popc(z);
+                any |= fa[k * NWD + w];
+            z[j] = ~any;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int l = 0; l < 2 * M - 1; l++) {
+            const int e = l < M ? l : 2 * M - 2 - l;
+            const uint32_t *ml = bctl + l * NWD;
+            if (e < 5) {  // pairs inside a word
+                const int sh = 1 << e;
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    const uint32_t mk = __ldg(ml + lane + 32 * j);
+                    const uint32_t t = ((z[j] >> sh) ^ z[j]) & mk;
+                    z[j] ^= t ^ (t << sh);
+                }
+            } else if (e < 10) {  // pairs across lanes
+                const int ls = 1 << (e - 5);
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    const uint32_t other = __shfl_xor_sync(FULLMASK, z[j], ls);
+                    const uint32_t mk = __ldg(ml + ((lane & ~ls) + 32 * j));
+                    z[j] ^= (z[j] ^ other) & mk;
+                }
+            } else {  // pairs inside a lane
+                const int js = 1 << (e - 10);
+#pragma unroll
+                for (int j = 0; j < R; j++) {
+                    if (!(j & js)) {
+                        const uint32_t mk = __ldg(ml + lane + 32 * j);
+                        const uint32_t t = (z[j] ^ z[j | js]) & mk;
+                        z[j] ^= t;
+                        z[j | js] ^= t;
+                    }
+                }
+            }
+        }
+        const uint64_t c = ct_index(rc, warp, q);
+        uint32_t *erow = a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride);
+        int cnt = 0;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int w = lane + 32 * j;
+            if (w < NW) {
+                const int left = P::N - 32 * w;
+                const uint32_t valid = left >= 32 ? FULLMASK : ((1u << left) - 1u);
+                const uint32_t v = z[j] & valid;
+                erow[w] = v;
+                cnt += __popc(v);
+            }
         }
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1)
             cnt += __shfl_xor_sync(FULLMASK, cnt, off);
         if (lane == 0 && a.weight)
             a.weight[c] = (uint16_t)cnt;
-        __syncwarp();
     }
 }
 

@@ -25,6 +25,10 @@ struct KeyDev {
                                 // util.c:86-100 values, rows 16-byte aligned
     uint32_t *Lbs = nullptr;    // bitsliced support, plane-major [m][nw]:
                                 // bit p of Lbs[k*nw+w] = bit k of L[32w+p]
+    uint32_t *bctl = nullptr;   // Benes network as swap masks, [2m-1][2^(m-5)]:
+                                // bit b of bctl[l*2^(m-5)+w] set when layer l
+                                // exchanges position 32w+b (the pair's lower
+                                // element) with its partner
     uint8_t *sk = nullptr;      // device copy of the secret key bytes
 };
 
@@ -39,6 +43,8 @@ struct LaunchCounter {
 };
 
 cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc);
+// Words of KeyDev::bctl for one set.
+inline size_t benes_mask_words(const SetInfo &si) { return (size_t)(2 * si.m - 1) << (si.m - 5); }
 
 cudaError_t launch_synd_plain(const KeyDev &k, const uint8_t *d_cts, size_t count,
                               uint32_t *d_synd, cudaStream_t s, LaunchCounter lc);
@@ -62,6 +68,17 @@ struct FusedKeyRef {
     int32_t pad;
     const uint32_t *tab;
     const uint32_t *Lbs;
+    const uint32_t *bctl;
+};
+
+// Additive-FFT evaluation plan of one parameter set (fft_plan.cpp): constant
+// tables shared by every key of the set.
+//   scalpow[d*256 + i]: b_d^i, the radix-conversion scale of depth d;
+//   tw[(off_d + u)*16 + k]: plane k of twiddle word u of depth d (off_d =
+//   sum of the word counts 2^(m-e-6) of the depths e < d).
+struct FftPlanDev {
+    const uint16_t *scalpow;
+    const uint32_t *tw;
 };
 struct FusedArgs {
     const FusedTile *tiles;        // device list of rounds; null = implicit
@@ -81,6 +98,7 @@ struct FusedArgs {
     uint32_t *tile_counter;        // zeroed before the launch
     int single_set;                // >= 0: every round has this set
     uint32_t err_stride;           // words per error row when err_off is null
+    FftPlanDev fft[NSETS];         // root-search plans, indexed by set
 };
 cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,
                          LaunchCounter lc);

@@ -108,6 +108,33 @@ template <int S> __global__ void __launch_bounds__(256) k_bitslice_support(KeyDe
     }
 }
 
+// The support network of k_support as per-word swap masks for the fused
+// root search, which runs the same layers over a 2^m-bit array of zero flags
+// (one bit per field element) instead of over 16-bit support entries.  Thread
+// (layer, w) builds word w of layer l: bit b is control bit l*2^(m-1) + q of
+// the pair whose lower element is p = 32w + b (bit e of p clear, q = p with
+// bit e deleted), zero where bit e of p is set.
+template <int S> __global__ void __launch_bounds__(256) k_benes_masks(KeyDev k)
+{
+    using P = Set<S>;
+    constexpr int M = P::M, NWD = 1 << (M - 5), HALF = 1 << (M - 1);
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (2 * M - 1) * NWD)
+        return;
+    const int layer = idx / NWD, w = idx % NWD;
+    const int e = layer < M ? layer : 2 * M - 2 - layer;
+    const uint8_t *cond = k.sk + 40 + 2 * P::T;
+    uint32_t mask = 0;
+    for (int b = 0; b < 32; b++) {
+        const uint32_t p = 32u * w + b;
+        const uint32_t q = ((p >> (e + 1)) << e) | (p & ((1u << e) - 1u));
+        const uint32_t bit = (uint32_t)layer * HALF + q;
+        const uint32_t c = (cond[bit >> 3] >> (bit & 7)) & 1u;
+        mask |= (c & ~(p >> e)) << b;
+    }
+    k.bctl[idx] = mask;
+}
+
 cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc)
 {
     return dispatch_set(k.set, [&]<int S>() -> cudaError_t {
@@ -115,7 +142,8 @@ cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc)
         k_support<S><<<1, 1024, 0, s>>>(k);
         k_key_tables<S><<<(P::N + 255) / 256, 256, 0, s>>>(k);
         k_bitslice_support<S><<<(P::NW * 32 + 255) / 256, 256, 0, s>>>(k);
-        lc.bump(3);
+        k_benes_masks<S><<<((2 * P::M - 1) * (1 << (P::M - 5)) + 255) / 256, 256, 0, s>>>(k);
+        lc.bump(4);
         return cudaGetLastError();
     });
 }

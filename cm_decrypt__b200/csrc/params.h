@@ -17,6 +17,16 @@ namespace cmd {
 enum : int { S348864 = 0, S460896 = 1, S6688128 = 2, S6960119 = 3, S8192128 = 4, NSETS = 5 };
 
 template <int S> struct Set;
+
+// Depth of the additive-FFT recursion for a degree-t locator: the smallest D
+// with 2^D >= t + 1 (7 for t = 64, 96, 119; 8 for t = 128).
+constexpr CMD_HD int fft_depth(int t)
+{
+    int d = 0;
+    while ((1 << d) < t + 1)
+        d++;
+    return d;
+}
 // M: GFBITS, N: SYS_N, T: SYS_T, CT: ciphertext = SYND_BYTES, SK: secret key.
 #define CMD_DEFINE_SET(ID, ID_NUM, M_, N_, T_, CT_, SK_)                               \
     template <> struct Set<ID> {                                                       \

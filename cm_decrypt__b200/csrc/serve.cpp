@@ -224,7 +224,7 @@ int cmd_server::launch(Slot &sl)
     std::vector<int> kset(kid.size());
     for (size_t k = 0; k < kid.size(); k++) {
         const cmd_key *key = keys[kid[k]].key;
-        krefs[k] = FusedKeyRef{key->dev.set, 0, key->dev.tab, key->dev.Lbs};
+        krefs[k] = key_ref(key->dev);
         kset[k] = key->dev.set;
     }
     LaunchCounter lc{&eng->launches};
@@ -300,6 +300,7 @@ int cmd_server::launch(Slot &sl)
         a.weight = sl.d_w;
         a.tile_counter = sl.d_counter;
         a.single_set = single;
+        fill_fft(a, eng);
         size_t smem = 0;
         if (single >= 0)
             smem = fused_smem(single, wpb);
