@@ -1,0 +1,201 @@
+// Additive-FFT root search shared by the fused kernel and the serving tile
+// path.  It replaces the reference's per-support-point Horner evaluation
+// (CPU/src/common/root_13.c:216-240, eval at every L[i]) with an evaluation
+// at all 2^m field elements followed by the key's support network, which is
+// the permutation that generated L (root_13.c:95-177 applies it to the table
+// bitrev(0..2^m-1)):
+//
+//  * fft_convert: radix conversion of up to 32 locators at once, bitsliced
+//    across them (bit q of a word = locator q).  Entry x of the array holds
+//    coefficient x of f(a) = sum_x C[T-x] a^x (the reversed locator the
+//    reference evaluates).  Depth d: scale entry x by b_d^(x >> d), then
+//    expand every stride-2^d sub-array in x^2 + x -- for block sizes n = 2^k
+//    down to 4, third quarter ^= fourth, then second ^= third.  Afterwards
+//    entry s holds the depth-D constant of the sub-problem whose Taylor
+//    choices are the bits of s.
+//  * fft_root_one: one warp, one locator q.  A 2^m-element bitsliced array
+//    (plane-major, m planes of 2^(m-5) words, in shared memory) starts from
+//    the depth-D constants -- position Y gets constant bitrev_D(Y >> (m-D))
+//    -- and takes D levels of butterflies A' = A + w*B, B' = A' + B between
+//    whole words; position Y then holds f(bitrev_m(Y)), which is where the
+//    support network expects element Y's value.  Zero flags (one bit per
+//    element) go through the 2m-1 swap layers: pairs inside a word by
+//    shifts, across lanes by shuffles, inside a lane by registers.  Bit j of
+//    the result is "f(L[j]) == 0", the reference's error bit j.
+//
+// Tables: scalpow and the twiddle words come from fft_plan.cpp (per set),
+// the swap masks from k_benes_masks (per key).
+#pragma once
+#include "gf.cuh"
+#include "internal.h"
+
+namespace cmd {
+
+template <int S> struct FftDims {
+    static constexpr int M = Set<S>::M, T = Set<S>::T, N = Set<S>::N, NW = Set<S>::NW;
+    static constexpr int D = fft_depth(T);     // recursion depth, 2^D > T
+    static constexpr int NX = 1 << D;          // radix-conversion entries
+    static constexpr int NWD = 1 << (M - 5);   // words of a 2^m-bit array
+    static constexpr int R = NWD / 32;         // of them per lane
+    static constexpr int FA_WORDS = M * NWD;   // per-warp butterfly array
+    static_assert(D <= M - 5, "butterflies must pair whole words");
+};
+
+// Radix conversion of the bitsliced array cv[x * CVS + k] (x < 2^D, k < M),
+// by NT cooperating threads (tid in [0, NT)); `sync` orders the steps.
+template <int S, int CVS, int NT, class Sync>
+__device__ __forceinline__ void fft_convert(uint32_t *cv, const uint16_t *__restrict__ scalpow, int tid, Sync sync)
+{
+    using F = FftDims<S>;
+    constexpr int M = F::M, D = F::D, NX = F::NX;
+#pragma unroll 1
+    for (int d = 0; d < D; d++) {
+        if (d > 0) {  // b_0 = 1: depth 0 needs no scaling
+            for (int x = tid; x < NX; x += NT) {
+                const uint32_t c = __ldg(scalpow + d * 256 + (x >> d));
+                uint32_t v[M], cm[M], p[2 * M - 1];
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    v[k] = cv[x * CVS + k];
+                    cm[k] = 0u - ((c >> k) & 1u);
+                }
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    p[k] = 0;
+                bs_mul_acc<M>(p, v, cm);
+                bs_reduce<M>(p);
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    cv[x * CVS + k] = p[k];
+            }
+            sync();
+        }
+#pragma unroll 1
+        for (int kb = D - d; kb >= 2; kb--) {
+            const int Q = 1 << (kb - 2);
+#pragma unroll 1
+            for (int h = 2; h >= 1; h--) {  // h = 2: third ^= fourth; h = 1: second ^= third
+                for (int u = tid; u < (NX / 4) * M; u += NT) {
+                    const int e = u / M, k = u - e * M;
+                    const int sub = e & ((1 << d) - 1), rest = e >> d;
+                    const int i = (rest >> (kb - 2)) * 4 * Q + h * Q + (rest & (Q - 1));
+                    cv[((i << d) + sub) * CVS + k] ^= cv[(((i + Q) << d) + sub) * CVS + k];
+                }
+                sync();
+            }
+        }
+    }
+}
+
+// One warp: error row (and weight) of locator q from the converted array cv
+// (bitsliced, cv[s * CVS + k]).  fa: this warp's FA_WORDS words of shared
+// memory.  erow: NW words.  Returns the weight (all lanes).
+template <int S, int CVS>
+__device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t *fa, const uint32_t *__restrict__ tw,
+                                            const uint32_t *__restrict__ bctl, uint32_t *erow, int lane)
+{
+    using F = FftDims<S>;
+    constexpr int M = F::M, D = F::D, NWD = F::NWD, R = F::R, NW = F::NW;
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const int w = lane + 32 * j;
+        const int sidx = (int)(__brev((uint32_t)(w >> (M - D - 5))) >> (32 - D));
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            fa[k * NWD + w] = 0u - ((cv[sidx * CVS + k] >> q) & 1u);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int d = D - 1; d >= 0; d--) {
+        const int sbit = M - d - 6, Sw = 1 << sbit;
+        const uint32_t *twd = tw + (size_t)((1 << (M - 5)) - (1 << (M - 5 - d))) * 16;
+#pragma unroll 1
+        for (int j = 0; j < R / 2; j++) {
+            const int P2 = lane + 32 * j;
+            const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
+            const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+            uint32_t A[M], B[M], G[M], p[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                A[k] = fa[k * NWD + wa];
+                B[k] = fa[k * NWD + wa + Sw];
+                G[k] = __ldg(g + k);
+            }
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            bs_mul_acc<M>(p, G, B);
+            bs_reduce<M>(p);
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const uint32_t na = A[k] ^ p[k];
+                fa[k * NWD + wa] = na;
+                fa[k * NWD + wa + Sw] = na ^ B[k];
+            }
+        }
+        __syncwarp();
+    }
+    uint32_t z[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const int w = lane + 32 * j;
+        uint32_t any = 0;
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            any |= fa[k * NWD + w];
+        z[j] = ~any;
+    }
+    __syncwarp();  // fa may be refilled right after this call
+#pragma unroll
+    for (int l = 0; l < 2 * M - 1; l++) {
+        const int e = l < M ? l : 2 * M - 2 - l;
+        const uint32_t *ml = bctl + l * NWD;
+        if (e < 5) {  // pairs inside a word
+            const int sh = 1 << e;
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                const uint32_t mk = __ldg(ml + lane + 32 * j);
+                const uint32_t t = ((z[j] >> sh) ^ z[j]) & mk;
+                z[j] ^= t ^ (t << sh);
+            }
+        } else if (e < 10) {  // pairs across lanes
+            const int ls = 1 << (e - 5);
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                const uint32_t other = __shfl_xor_sync(FULL, z[j], ls);
+                const uint32_t mk = __ldg(ml + ((lane & ~ls) + 32 * j));
+                z[j] ^= (z[j] ^ other) & mk;
+            }
+        } else {  // pairs inside a lane
+            const int js = 1 << (e - 10);
+#pragma unroll
+            for (int j = 0; j < R; j++) {
+                if (!(j & js)) {
+                    const uint32_t mk = __ldg(ml + lane + 32 * j);
+                    const uint32_t t = (z[j] ^ z[j | js]) & mk;
+                    z[j] ^= t;
+                    z[j | js] ^= t;
+                }
+            }
+        }
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        const int w = lane + 32 * j;
+        if (w < NW) {
+            const int left = F::N - 32 * w;
+            const uint32_t valid = left >= 32 ? FULL : ((1u << left) - 1u);
+            const uint32_t v = z[j] & valid;
+            erow[w] = v;
+            cnt += __popc(v);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+        cnt += __shfl_xor_sync(FULL, cnt, off);
+    return cnt;
+}
+
+}  // namespace cmd

@@ -15,8 +15,9 @@
 //     row is masked by the ciphertext bit, never branched on;
 //  3. ballot-transpose the syndromes to bitsliced form (bit q = ciphertext q);
 //  4. Berlekamp-Massey (bm.c:12-68) bitsliced across the 32 ciphertexts: lane
-//     l owns locator coefficients l, l+32, ... in registers, the discrepancy is
-//     a shuffle-XOR reduction, B lives in a shared ring buffer whose rotation
+//     l owns locator coefficients l, l+32, ... (kept in shared memory, so the
+//     per-step loop over them stays rolled and small), the discrepancy is a
+//     redux XOR reduction, B lives in a shared ring buffer whose rotation
 //     implements the x*B shift.  The update is the scaled form C <- b*C +
 //     d*x*B instead of bm()'s C <- C + (d/b)*x*B: same decisions (d != 0,
 //     N >= 2L), same truncation, and by induction the result is lambda times
@@ -37,6 +38,7 @@
 //        the packed error row and its weight.
 //     The tables of the recursion are per set (fft_plan.cpp).
 #pragma once
+#include "fft_root.cuh"
 #include "gf.cuh"
 #include "internal.h"
 
@@ -53,19 +55,16 @@ template <int S> struct Fz {
     static constexpr int M = P::M, T = P::T, NJ = (T + 1 + 31) / 32;
     static constexpr int TWP = (T + 3) / 4 * 4;      // padded table row (words)
     static constexpr int RING = T + 2;               // B ring slots
-    static constexpr int D = fft_depth(T);           // FFT recursion depth
-    static constexpr int NX = 1 << D;                // radix-conversion entries
-    static constexpr int NWD = 1 << (M - 5);         // words of a 2^m-bit array
-    static constexpr int R = NWD / 32;               // of them per lane
+    static constexpr int NX = FftDims<S>::NX;        // radix-conversion entries
     static constexpr int RAW_B = 32 * P::CT;
     static constexpr int RING_B = RING * M * 4;
-    static constexpr int FA_B = M * NWD * 4;         // FFT array, plane-major
-    static constexpr int A_B = al16(cmax(cmax(RAW_B + 16, RING_B), FA_B));
+    static constexpr int FA_B = FftDims<S>::FA_WORDS * 4;  // root-search array
+    static constexpr int CM_B = (T + 1) * M * 4;     // BM locator, after the ring
+    static constexpr int A_B = al16(cmax(cmax(RAW_B + 16, RING_B + CM_B), FA_B));
     static constexpr int S_B = al16(2 * T * M * 4);  // bitsliced syndromes / locator
     static constexpr int WARP_B = A_B + S_B;
     static constexpr int TAB_B = TAB_ROWS * TWP * 4;  // one chunk buffer
     static_assert(NX * M * 4 <= S_B, "conversion array must fit the syndrome region");
-    static_assert(D <= M - 5, "butterflies must pair whole words");
 };
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src)
@@ -213,12 +212,9 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     // ---- 4. Berlekamp-Massey, bitsliced across the 32 ciphertexts --------
     {
         constexpr int NJ = Z::NJ, R = Z::RING;
-        uint32_t C[NJ][M];
-#pragma unroll
-        for (int j = 0; j < NJ; j++)
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                C[j][k] = (j == 0 && k == 0 && lane == 0) ? FULLMASK : 0u;
+        uint32_t *sCm = ring + R * M;  // locator coefficients [T+1][M]
+        for (int v = lane; v < (T + 1) * M; v += 32)
+            sCm[v] = (v == 0) ? FULLMASK : 0u;  // C = 1
         for (int v = lane; v < R * M; v += 32)
             ring[v] = (v == M) ? FULLMASK : 0u;  // B = x
         uint32_t bb[M];
@@ -234,16 +230,19 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
                 p[k] = 0;
-#pragma unroll
-            for (int j = 0; j < NJ; j++) {
+#pragma unroll 1
+            for (int j = 0; 32 * j <= lim; j++) {
                 const int i = lane + 32 * j;
                 if (i <= lim) {
                     const uint32_t *sv = sS + (N - i) * M;
-                    uint32_t s[M];
+                    const uint32_t *cp = sCm + i * M;
+                    uint32_t s[M], c[M];
 #pragma unroll
-                    for (int k = 0; k < M; k++)
+                    for (int k = 0; k < M; k++) {
                         s[k] = sv[k];
-                    bs_mul_acc<M>(p, C[j], s);
+                        c[k] = cp[k];
+                    }
+                    bs_mul_acc<M>(p, c, s);
                 }
             }
             bs_reduce<M>(p);
@@ -260,36 +259,40 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
             Lq = my_mle ? N + 1 - Lq : Lq;
             // Scaled update C <- b*C + d*x*B (see the note at the top of the
             // file): both products accumulate unreduced, one reduction.
+            // Before the update deg C <= N and deg x*B <= N + 1, so slots
+            // whose coefficients all exceed N + 1 hold zeros (their ring
+            // entries were never written) and are skipped.
             int off = (R - (N % R)) % R;  // slot(i) = (i - N) mod R
-#pragma unroll
-            for (int j = 0; j < NJ; j++) {
+#pragma unroll 1
+            for (int j = 0; j < NJ && 32 * j <= N + 1; j++) {
                 const int i = lane + 32 * j;
                 if (i <= T) {
                     int slot = i + off;
                     slot = slot >= R ? slot - R : slot;
                     uint32_t *bp = ring + slot * M;
-                    uint32_t bv[M], q[2 * M - 1];
+                    uint32_t *cp = sCm + i * M;
+                    uint32_t bv[M], oc[M], q[2 * M - 1];
 #pragma unroll
-                    for (int k = 0; k < M; k++)
+                    for (int k = 0; k < M; k++) {
                         bv[k] = bp[k];
+                        oc[k] = cp[k];
+                    }
 #pragma unroll
                     for (int k = 0; k < 2 * M - 1; k++)
                         q[k] = 0;
-                    bs_mul_acc<M>(q, bb, C[j]);
+                    bs_mul_acc<M>(q, bb, oc);
                     bs_mul_acc<M>(q, d, bv);
                     bs_reduce<M>(q);
 #pragma unroll
                     for (int k = 0; k < M; k++) {
-                        const uint32_t oc = C[j][k];
-                        C[j][k] = q[k];
-                        bp[k] = (bv[k] & ~mle) | (oc & mle);
+                        cp[k] = q[k];
+                        bp[k] = (bv[k] & ~mle) | (oc[k] & mle);
                     }
                 }
             }
 #pragma unroll
             for (int k = 0; k < M; k++)
                 bb[k] = (bb[k] & ~mle) | (d[k] & mle);
-            // Slot of B_{t+1} at this N becomes B_0 = 0 at N+1.
             const int freeslot = (R - ((N + 1) % R)) % R;
             if (lane < M)
                 ring[freeslot * M + lane] = 0;
@@ -298,171 +301,22 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
         // The reference's root search evaluates sum_x C[T-x] a^x
         // (bm.c:62-65 reverses the locator): entry x of the conversion array
         // is C[T-x], zero for T < x < 2^D.
-#pragma unroll
-        for (int j = 0; j < NJ; j++) {
-            const int i = lane + 32 * j;
-            if (i <= T)
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    cv[(T - i) * M + k] = C[j][k];
+        for (int v = lane; v < (T + 1) * M; v += 32) {
+            const int i = v / M, k = v - i * M;
+            cv[(T - i) * M + k] = sCm[v];
         }
         for (int v = lane; v < (Z::NX - T - 1) * M; v += 32)
             cv[(T + 1) * M + v] = 0u;
         __syncwarp();
     }
 
-    // ---- 5. root search ----------------------------------------------------
-    constexpr int D = Z::D, NX = Z::NX, NWD = Z::NWD, R = Z::R;
+    // ---- 5. root search (fft_root.cuh) -------------------------------------
     const FftPlanDev pl = a.fft[S];
-    // 5a. radix conversion of the 32 locators at once.  Depth d: scale entry
-    // x by b_d^(x >> d) (b_0 = 1), then expand every stride-2^d sub-array in
-    // x^2 + x: for block sizes n = 2^k down to 4, third quarter ^= fourth,
-    // then second ^= third.  Afterwards entry s is the depth-D constant of
-    // the sub-problem whose Taylor choices are the bits of s.
-#pragma unroll 1
-    for (int d = 0; d < D; d++) {
-        if (d > 0) {
-            for (int x = lane; x < NX; x += 32) {
-                const uint32_t c = __ldg(pl.scalpow + d * 256 + (x >> d));
-                uint32_t v[M], cm[M], p[2 * M - 1];
-#pragma unroll
-                for (int k = 0; k < M; k++) {
-                    v[k] = cv[x * M + k];
-                    cm[k] = 0u - ((c >> k) & 1u);
-                }
-#pragma unroll
-                for (int k = 0; k < 2 * M - 1; k++)
-                    p[k] = 0;
-                bs_mul_acc<M>(p, v, cm);
-                bs_reduce<M>(p);
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    cv[x * M + k] = p[k];
-            }
-            __syncwarp();
-        }
-#pragma unroll 1
-        for (int kb = D - d; kb >= 2; kb--) {
-            const int Q = 1 << (kb - 2);
-#pragma unroll 1
-            for (int h = 2; h >= 1; h--) {  // h = 2: third ^= fourth; h = 1: second ^= third
-                for (int u = lane; u < (NX / 4) * M; u += 32) {
-                    const int e = u / M, k = u - e * M;
-                    const int sub = e & ((1 << d) - 1), rest = e >> d;
-                    const int i = (rest >> (kb - 2)) * 4 * Q + h * Q + (rest & (Q - 1));
-                    cv[((i << d) + sub) * M + k] ^= cv[(((i + Q) << d) + sub) * M + k];
-                }
-                __syncwarp();
-            }
-        }
-    }
-
-    const uint32_t *bctl = rc.key.bctl;
+    fft_convert<S, M, 32>(cv, pl.scalpow, lane, [] { __syncwarp(); });
     for (int q = 0; q < ntile; q++) {
-        // 5b. position Y of the array holds f at the field element
-        // bitrev_m(Y); at depth D it holds the constant of sub-problem
-        // bitrev_D(Y >> (m - D)), one constant per group of words.
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            const int w = lane + 32 * j;
-            const int sidx = (int)(__brev((uint32_t)(w >> (M - D - 5))) >> (32 - D));
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                fa[k * NWD + w] = 0u - ((cv[sidx * M + k] >> q) & 1u);
-        }
-        __syncwarp();
-#pragma unroll
-        for (int d = D - 1; d >= 0; d--) {
-            const int sbit = M - d - 6, Sw = 1 << sbit;
-            const uint32_t *twd = pl.tw + (size_t)((1 << (M - 5)) - (1 << (M - 5 - d))) * 16;
-#pragma unroll 1
-            for (int j = 0; j < R / 2; j++) {
-                const int P2 = lane + 32 * j;
-                const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
-                const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
-                uint32_t A[M], B[M], G[M], p[2 * M - 1];
-#pragma unroll
-                for (int k = 0; k < M; k++) {
-                    A[k] = fa[k * NWD + wa];
-                    B[k] = fa[k * NWD + wa + Sw];
-                    G[k] = __ldg(g + k);
-                }
-#pragma unroll
-                for (int k = 0; k < 2 * M - 1; k++)
-                    p[k] = 0;
-                bs_mul_acc<M>(p, G, B);
-                bs_reduce<M>(p);
-#pragma unroll
-                for (int k = 0; k < M; k++) {
-                    const uint32_t na = A[k] ^ p[k];
-                    fa[k * NWD + wa] = na;
-                    fa[k * NWD + wa + Sw] = na ^ B[k];
-                }
-            }
-            __syncwarp();
-        }
-        // 5c. zero flags, the key's swap layers, the error row.
-        uint32_t z[R];
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            const int w = lane + 32 * j;
-            uint32_t any = 0;
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                any |= fa[k * NWD + w];
-            z[j] = ~any;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int l = 0; l < 2 * M - 1; l++) {
-            const int e = l < M ? l : 2 * M - 2 - l;
-            const uint32_t *ml = bctl + l * NWD;
-            if (e < 5) {  // pairs inside a word
-                const int sh = 1 << e;
-#pragma unroll
-                for (int j = 0; j < R; j++) {
-                    const uint32_t mk = __ldg(ml + lane + 32 * j);
-                    const uint32_t t = ((z[j] >> sh) ^ z[j]) & mk;
-                    z[j] ^= t ^ (t << sh);
-                }
-            } else if (e < 10) {  // pairs across lanes
-                const int ls = 1 << (e - 5);
-#pragma unroll
-                for (int j = 0; j < R; j++) {
-                    const uint32_t other = __shfl_xor_sync(FULLMASK, z[j], ls);
-                    const uint32_t mk = __ldg(ml + ((lane & ~ls) + 32 * j));
-                    z[j] ^= (z[j] ^ other) & mk;
-                }
-            } else {  // pairs inside a lane
-                const int js = 1 << (e - 10);
-#pragma unroll
-                for (int j = 0; j < R; j++) {
-                    if (!(j & js)) {
-                        const uint32_t mk = __ldg(ml + lane + 32 * j);
-                        const uint32_t t = (z[j] ^ z[j | js]) & mk;
-                        z[j] ^= t;
-                        z[j | js] ^= t;
-                    }
-                }
-            }
-        }
         const uint64_t c = ct_index(rc, warp, q);
         uint32_t *erow = a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride);
-        int cnt = 0;
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            const int w = lane + 32 * j;
-            if (w < NW) {
-                const int left = P::N - 32 * w;
-                const uint32_t valid = left >= 32 ? FULLMASK : ((1u << left) - 1u);
-                const uint32_t v = z[j] & valid;
-                erow[w] = v;
-                cnt += __popc(v);
-            }
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1)
-            cnt += __shfl_xor_sync(FULLMASK, cnt, off);
+        const int cnt = fft_root_one<S, M>(cv, q, fa, pl.tw, rc.key.bctl, erow, lane);
         if (lane == 0 && a.weight)
             a.weight[c] = (uint16_t)cnt;
     }

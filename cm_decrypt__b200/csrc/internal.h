@@ -106,16 +106,26 @@ cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cuda
 // Latency path (serving loop; latency.cu): one work item per ciphertext.
 struct LatItem {
     const uint32_t *tab;  // key's syndrome table
-    const uint32_t *Lbs;  // key's bitsliced support
+    const uint32_t *bctl; // key's support-network swap masks
     uint32_t ct_off;      // byte offset of the ciphertext in the batch
     uint32_t err_off;     // word offset of the error row in the batch
     int32_t set;
     int32_t pad;
 };
 // Tile path: ntiles tiles of 32 item slots (LatItem.pad = tile count, padding
-// slots set -1); d_loc_bs holds ntiles * 130 * 16 words.
-cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_loc_bs,
-                             uint32_t *d_err, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc);
+// slots set -1).  d_scratch holds ntiles * TILE_SCRATCH_WORDS words: each
+// tile's radix-converted locators (bitsliced, 16 words per entry), then the
+// partial syndromes (SYN_PARTS rows of SYN_ROWW words per item slot).
+constexpr int TILE_LOC_WORDS = 256 * 16;
+constexpr int SYN_PARTS = 4;
+constexpr int SYN_ROWW = 128;
+constexpr int TILE_SCRATCH_WORDS = TILE_LOC_WORDS + 32 * SYN_PARTS * SYN_ROWW;
+struct FftPlans {
+    FftPlanDev p[NSETS];
+};
+cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_scratch,
+                             uint32_t *d_err, uint16_t *d_weight, const FftPlans &plans, cudaStream_t s,
+                             LaunchCounter lc);
 
 void set_last_error(const std::string &msg);
 

@@ -13,6 +13,7 @@
 // included.  (The per-stage hook cmd_stage_bm keeps bm()'s exact output.)
 #include <algorithm>
 
+#include "fft_root.cuh"
 #include "gf.cuh"
 #include "internal.h"
 
@@ -29,88 +30,113 @@ static_assert(sizeof(LatItem) == 32, "LatItem layout");
 // 32*t + q is ciphertext q of tile t (LatItem.pad = the tile's count, padding
 // slots have set -1).
 //
+// k_tile_synd: SYN_PARTS CTAs per ciphertext, each over a contiguous quarter
+//   of the syndrome-table rows of the ciphertext's own key (util.c:102-114):
+//   warp w takes rows w, w+8, ...; lane l owns table words 4l..4l+3 (one
+//   128-bit load per row), every row masked by the ciphertext bit; the eight
+//   warps' sums meet in shared memory and the CTA writes one partial
+//   syndrome row.  A batch's tables stream through every SM at once instead
+//   of through one SM per tile.
 // k_tile_bm: one CTA of 8 warps per tile.
-//   1. syndrome: warp w computes ciphertexts 4w..4w+3; lane l owns table words
-//      4l..4l+3 (one 128-bit load per row from the ciphertext's key table),
-//      every row masked by the ciphertext bit;
+//   1. syndromes: XOR of each ciphertext's SYN_PARTS partial rows;
 //   2. ballot transpose to bitsliced syndromes (bit q = ciphertext q);
 //   3. scaled Berlekamp-Massey bitsliced across the 32 ciphertexts with thread
 //      i owning coefficient i, so one step costs about one bitsliced multiply
 //      per thread: partial discrepancies meet in shared memory, B lives in a
 //      shared ring buffer whose rotation is the x*B shift;
-//   4. the bitsliced locator (t+1 coefficients x 16 words) goes to global.
-// k_root_tile: one CTA per ciphertext, bitsliced Horner over its support.
-constexpr int TILE_LOC_WORDS = 130 * 16;
+//   4. radix conversion of the 32 locators by the whole CTA (fft_root.cuh);
+//      the converted array (2^D entries x 16 words) goes to global.
+// k_root_tile: 8 warps per CTA, four CTAs per tile, warp = one ciphertext:
+// additive-FFT evaluation and the ciphertext's own key's support network.
+
+template <int S>
+__device__ __forceinline__ void tile_synd(const LatItem &it, const uint8_t *cts, int part, uint32_t *out,
+                                          uint32_t (*red)[SYN_ROWW], uint8_t *ct)
+{
+    using P = Set<S>;
+    constexpr int TWP = P::TWP, RPP = (P::SB + SYN_PARTS - 1) / SYN_PARTS;
+    static_assert(TWP <= SYN_ROWW, "partial syndrome row");
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int v = tid; v < P::CT; v += blockDim.x)
+        ct[v] = cts[it.ct_off + v];
+    __syncthreads();
+    const int b0 = part * RPP, b1 = b0 + RPP < P::SB ? b0 + RPP : P::SB;
+    const bool live = 4 * lane < TWP;
+    const uint4 *tab = reinterpret_cast<const uint4 *>(it.tab) + lane;
+    uint4 acc = make_uint4(0, 0, 0, 0);
+#pragma unroll 8
+    for (int b = b0 + warp; b < b1; b += 8) {
+        const uint32_t m = 0u - ((ct[b >> 3] >> (b & 7)) & 1u);
+        if (live) {
+            const uint4 x = __ldg(tab + (size_t)b * (TWP / 4));
+            acc.x ^= x.x & m;
+            acc.y ^= x.y & m;
+            acc.z ^= x.z & m;
+            acc.w ^= x.w & m;
+        }
+    }
+    if (live)
+        *reinterpret_cast<uint4 *>(&red[warp][4 * lane]) = acc;
+    __syncthreads();
+    for (int w = tid; w < TWP; w += blockDim.x) {
+        uint32_t v = 0;
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+            v ^= red[k][w];
+        out[w] = v;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_tile_synd(const LatItem *__restrict__ items, const uint8_t *__restrict__ cts,
+                                                   uint32_t *__restrict__ synp)
+{
+    __shared__ __align__(16) uint32_t red[8][SYN_ROWW];
+    __shared__ uint8_t ct[208];
+    const int slot = blockIdx.x / SYN_PARTS, part = blockIdx.x % SYN_PARTS, t = slot >> 5, q = slot & 31;
+    const LatItem it = items[slot];
+    if (it.set < 0 || q >= (int)items[(size_t)t * 32].pad)
+        return;  // whole CTA
+    uint32_t *out = synp + ((size_t)slot * SYN_PARTS + part) * SYN_ROWW;
+    switch (it.set) {
+    case S348864: tile_synd<S348864>(it, cts, part, out, red, ct); break;
+    case S460896: tile_synd<S460896>(it, cts, part, out, red, ct); break;
+    case S6688128: tile_synd<S6688128>(it, cts, part, out, red, ct); break;
+    case S6960119: tile_synd<S6960119>(it, cts, part, out, red, ct); break;
+    default: tile_synd<S8192128>(it, cts, part, out, red, ct); break;
+    }
+}
 
 template <int S> struct TileSmem {
     using P = Set<S>;
     static constexpr int SYN_STRIDE = P::TW | 1;  // odd stride: conflict-free column reads
-    uint8_t ct[32][(P::CT + 15) / 16 * 16];
     uint32_t syn[32 * SYN_STRIDE];
     uint32_t S_[2 * P::T * P::M];
     uint32_t ring[(P::T + 2) * P::M];
     uint32_t part[2][8][16];  // per-warp partial discrepancies, double-buffered by step parity
 };
 
-template <int S> __device__ __forceinline__ void tile_bm(const LatItem *items, int count, const uint8_t *cts,
-                                                         uint32_t *loc_bs, uint8_t *smem_raw)
+template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32_t *synp, uint32_t *loc_bs,
+                                                         const uint16_t *scalpow, uint8_t *smem_raw)
 {
     using P = Set<S>;
     using Sm = TileSmem<S>;
-    constexpr int M = P::M, T = P::T, TW = P::TW, TWP = P::TWP, R = T + 2;
+    constexpr int M = P::M, T = P::T, TW = P::TW, R = T + 2;
     constexpr int NWB = (T + 1 + 31) / 32;  // warps that own coefficients
     constexpr int SYN = Sm::SYN_STRIDE;
     Sm &sm = *reinterpret_cast<Sm *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-    // ---- 1. syndromes, four ciphertexts at a time -------------------------
-    // All 8 warps work on each group of 4, warp w taking table rows w, w+8,
-    // ...: a lone ciphertext gets the whole CTA's memory parallelism (its
-    // key's table is usually in HBM, not L2).  Lane l owns table words
-    // 4l..4l+3 (one 128-bit load per row); partial syndromes meet in shared
-    // memory by XOR.
-    for (int v = tid; v < 32 * P::CT; v += blockDim.x) {
-        const int q = v / P::CT, o = v - q * P::CT;
-        sm.ct[q][o] = q < count ? cts[items[q].ct_off + o] : 0;
-    }
-    for (int v = tid; v < 32 * SYN; v += blockDim.x)
-        sm.syn[v] = 0;
-    __syncthreads();
-    const bool live = 4 * lane < TWP;
-    for (int g = 0; 4 * g < count; g++) {
-        const uint32_t *tab[4];
+    // ---- 1. syndromes: XOR of the partial rows from k_tile_synd ------------
+    for (int v = tid; v < 32 * TW; v += blockDim.x) {
+        const int q = v / TW, w = v - q * TW;
+        uint32_t x = 0;
+        if (q < count) {
+            const uint32_t *src = synp + (size_t)q * SYN_PARTS * SYN_ROWW + w;
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int q = 4 * g + u;
-            tab[u] = items[q < count ? q : 0].tab;
+            for (int p = 0; p < SYN_PARTS; p++)
+                x ^= src[p * SYN_ROWW];
         }
-        uint4 acc[4];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-            acc[u] = make_uint4(0, 0, 0, 0);
-#pragma unroll 4
-        for (int b = warp; b < P::SB; b += 8) {
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const uint32_t m = 0u - ((sm.ct[4 * g + u][b >> 3] >> (b & 7)) & 1u);
-                if (live) {
-                    const uint4 x = __ldg(reinterpret_cast<const uint4 *>(tab[u] + (size_t)b * TWP) + lane);
-                    acc[u].x ^= x.x & m;
-                    acc[u].y ^= x.y & m;
-                    acc[u].z ^= x.z & m;
-                    acc[u].w ^= x.w & m;
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int q = 4 * g + u;
-            const uint32_t v4[4] = {acc[u].x, acc[u].y, acc[u].z, acc[u].w};
-#pragma unroll
-            for (int e = 0; e < 4; e++)
-                if (q < count && 4 * lane + e < TW)
-                    atomicXor(&sm.syn[q * SYN + 4 * lane + e], v4[e]);
-        }
+        sm.syn[q * SYN + w] = x;
     }
     __syncthreads();
 
@@ -185,7 +211,9 @@ template <int S> __device__ __forceinline__ void tile_bm(const LatItem *items, i
         const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
         const uint32_t mle = __ballot_sync(FULL, my_mle);
         Lq = my_mle ? N + 1 - Lq : Lq;
-        if (i <= T) {
+        // Coefficients above N + 1 of C and x*B are still zero (their ring
+        // entries were never written): whole warps past that bound skip.
+        if (i <= T && i <= N + 1) {
             int slot = i + (R - (N % R)) % R;
             slot = slot >= R ? slot - R : slot;
             uint32_t *bp = sm.ring + slot * M;
@@ -215,102 +243,77 @@ template <int S> __device__ __forceinline__ void tile_bm(const LatItem *items, i
             partial(N + 1);  // writes part[(N+1)&1]; part[N&1] was read above
         __syncthreads();
     }
-    // ---- 4. bitsliced locator out -----------------------------------------
+    // ---- 4. radix conversion, converted locators out -----------------------
+    // Entry x of the conversion array is C[T-x] (bm.c:62-65 reverses the
+    // locator before root() evaluates it), zero for T < x < 2^D; S_ is free.
+    using F = FftDims<S>;
+    static_assert(F::NX * M <= 2 * T * M && F::NX * 16 <= TILE_LOC_WORDS, "conversion array size");
     if (i <= T)
 #pragma unroll
         for (int k = 0; k < M; k++)
-            loc_bs[i * 16 + k] = C[k];
+            sm.S_[(T - i) * M + k] = C[k];
+    for (int v = tid; v < (F::NX - T - 1) * M; v += blockDim.x)
+        sm.S_[(T + 1) * M + v] = 0u;
+    __syncthreads();
+    fft_convert<S, M, 256>(sm.S_, scalpow, tid, [] { __syncthreads(); });
+    for (int v = tid; v < F::NX * M; v += blockDim.x) {
+        const int x = v / M, k = v - x * M;
+        loc_bs[x * 16 + k] = sm.S_[v];
+    }
 }
 
-__global__ void __launch_bounds__(256) k_tile_bm(const LatItem *__restrict__ items, const uint8_t *__restrict__ cts,
-                                                 uint32_t *__restrict__ loc_bs)
+__global__ void __launch_bounds__(256) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
+                                                 uint32_t *__restrict__ loc_bs, FftPlans plans)
 {
     extern __shared__ __align__(16) uint8_t smem_tile[];
     const LatItem *ti = items + (size_t)blockIdx.x * 32;
     const int count = (int)ti[0].pad;
+    const uint32_t *sp = synp + (size_t)blockIdx.x * 32 * SYN_PARTS * SYN_ROWW;
     uint32_t *out = loc_bs + (size_t)blockIdx.x * TILE_LOC_WORDS;
     switch (ti[0].set) {
-    case S348864: tile_bm<S348864>(ti, count, cts, out, smem_tile); break;
-    case S460896: tile_bm<S460896>(ti, count, cts, out, smem_tile); break;
-    case S6688128: tile_bm<S6688128>(ti, count, cts, out, smem_tile); break;
-    case S6960119: tile_bm<S6960119>(ti, count, cts, out, smem_tile); break;
-    default: tile_bm<S8192128>(ti, count, cts, out, smem_tile); break;
+    case S348864: tile_bm<S348864>(count, sp, out, plans.p[S348864].scalpow, smem_tile); break;
+    case S460896: tile_bm<S460896>(count, sp, out, plans.p[S460896].scalpow, smem_tile); break;
+    case S6688128: tile_bm<S6688128>(count, sp, out, plans.p[S6688128].scalpow, smem_tile); break;
+    case S6960119: tile_bm<S6960119>(count, sp, out, plans.p[S6960119].scalpow, smem_tile); break;
+    default: tile_bm<S8192128>(count, sp, out, plans.p[S8192128].scalpow, smem_tile); break;
     }
 }
 
-template <int S> __device__ __forceinline__ void root_tile(const LatItem &it, const uint32_t *loc_tile, int q,
-                                                           uint32_t *err, uint16_t *weight, uint32_t (*s_mask)[16],
-                                                           int *s_cnt)
+constexpr int ROOT_WARPS = 8;
+constexpr size_t ROOT_FA_WORDS = 13 * 256;  // FftDims<S>::FA_WORDS, largest set
+
+template <int S>
+__device__ __forceinline__ void root_tile(const LatItem &it, const uint32_t *cv, int q, uint32_t *err,
+                                          uint16_t *weight, const FftPlanDev &pl, uint32_t *fa)
 {
-    using P = Set<S>;
-    constexpr int M = P::M, T = P::T, NW = P::NW;
-    const int w = threadIdx.x, lane = w & 31, warp = w >> 5;
-    for (int e = threadIdx.x; e < (T + 1) * 16; e += blockDim.x) {
-        const int i = e >> 4, k = e & 15;
-        s_mask[i][k] = k < M ? 0u - ((loc_tile[i * 16 + k] >> q) & 1u) : 0u;
-    }
-    uint32_t a[M];
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        a[k] = w < NW ? __ldg(it.Lbs + k * NW + w) : 0u;
-    __syncthreads();
-    uint32_t r[M];
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        r[k] = s_mask[0][k];  // C[0] = f[t]
-    for (int i = 1; i <= T; i++) {
-        uint32_t p[2 * M - 1];
-#pragma unroll
-        for (int k = 0; k < 2 * M - 1; k++)
-            p[k] = k < M ? s_mask[i][k] : 0u;
-        bs_mul_acc<M>(p, r, a);
-        bs_reduce<M>(p);
-#pragma unroll
-        for (int k = 0; k < M; k++)
-            r[k] = p[k];
-    }
-    uint32_t any = 0;
-#pragma unroll
-    for (int k = 0; k < M; k++)
-        any |= r[k];
-    const int left = P::N - 32 * w;
-    const uint32_t valid = w >= NW ? 0u : (left >= 32 ? FULL : ((1u << left) - 1u));
-    const uint32_t z = ~any & valid;
-    if (w < NW)
-        err[it.err_off + w] = z;
-    int cnt = __popc(z);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-        cnt += __shfl_xor_sync(FULL, cnt, off);
-    if (lane == 0)
-        s_cnt[warp] = cnt;
-    __syncthreads();
-    if (w == 0 && weight) {
-        int tot = 0;
-        for (int qq = 0; qq < 8; qq++)
-            tot += s_cnt[qq];
-        *weight = (uint16_t)tot;
-    }
+    static_assert(FftDims<S>::FA_WORDS <= ROOT_FA_WORDS, "root array");
+    const int lane = threadIdx.x & 31;
+    const int cnt = fft_root_one<S, 16>(cv, q, fa, pl.tw, it.bctl, err + it.err_off, lane);
+    if (lane == 0 && weight)
+        *weight = (uint16_t)cnt;
 }
 
-__global__ void __launch_bounds__(256) k_root_tile(const LatItem *__restrict__ items,
-                                                   const uint32_t *__restrict__ loc_bs, uint32_t *__restrict__ err,
-                                                   uint16_t *__restrict__ weight)
+// Four CTAs per tile; warp w of CTA c handles ciphertext 8c + w of the tile.
+__global__ void __launch_bounds__(ROOT_WARPS * 32) k_root_tile(const LatItem *__restrict__ items,
+                                                               const uint32_t *__restrict__ loc_bs,
+                                                               uint32_t *__restrict__ err,
+                                                               uint16_t *__restrict__ weight, FftPlans plans)
 {
-    __shared__ __align__(16) uint32_t s_mask[129][16];
-    __shared__ int s_cnt[8];
-    const int slot = blockIdx.x, t = slot >> 5, q = slot & 31;
+    extern __shared__ __align__(16) uint32_t smem_root[];
+    const int warp = threadIdx.x >> 5;
+    const int t = blockIdx.x >> 2, q = ROOT_WARPS * (blockIdx.x & 3) + warp, slot = 32 * t + q;
     const LatItem it = items[slot];
     if (it.set < 0 || q >= (int)items[(size_t)t * 32].pad)
-        return;
-    const uint32_t *lt = loc_bs + (size_t)t * TILE_LOC_WORDS;
+        return;  // whole warp: no block-wide barrier follows
+    const uint32_t *cv = loc_bs + (size_t)t * TILE_LOC_WORDS;
+    uint32_t *fa = smem_root + (size_t)warp * ROOT_FA_WORDS;
     uint16_t *wp = weight ? weight + slot : nullptr;
     switch (it.set) {
-    case S348864: root_tile<S348864>(it, lt, q, err, wp, s_mask, s_cnt); break;
-    case S460896: root_tile<S460896>(it, lt, q, err, wp, s_mask, s_cnt); break;
-    case S6688128: root_tile<S6688128>(it, lt, q, err, wp, s_mask, s_cnt); break;
-    case S6960119: root_tile<S6960119>(it, lt, q, err, wp, s_mask, s_cnt); break;
-    default: root_tile<S8192128>(it, lt, q, err, wp, s_mask, s_cnt); break;
+    case S348864: root_tile<S348864>(it, cv, q, err, wp, plans.p[S348864], fa); break;
+    case S460896: root_tile<S460896>(it, cv, q, err, wp, plans.p[S460896], fa); break;
+    case S6688128: root_tile<S6688128>(it, cv, q, err, wp, plans.p[S6688128], fa); break;
+    case S6960119: root_tile<S6960119>(it, cv, q, err, wp, plans.p[S6960119], fa); break;
+    default: root_tile<S8192128>(it, cv, q, err, wp, plans.p[S8192128], fa); break;
     }
 }
 
@@ -326,23 +329,30 @@ size_t tile_smem_bytes()
 }
 
 // ntiles tiles of 32 item slots; weights are indexed by item slot.
-cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_loc_bs,
-                             uint32_t *d_err, uint16_t *d_weight, cudaStream_t s, LaunchCounter lc)
+cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_scratch,
+                             uint32_t *d_err, uint16_t *d_weight, const FftPlans &plans, cudaStream_t s,
+                             LaunchCounter lc)
 {
     if (ntiles == 0)
         return cudaSuccess;
     static size_t attr = 0;
     const size_t smem = tile_smem_bytes();
+    const size_t root_smem = ROOT_WARPS * ROOT_FA_WORDS * 4;
     if (attr < smem) {
         cudaError_t e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)root_smem);
         if (e != cudaSuccess)
             return e;
         attr = smem;
     }
     const LatItem *items = static_cast<const LatItem *>(d_items);
-    k_tile_bm<<<ntiles, 256, smem, s>>>(items, d_cts, d_loc_bs);
-    k_root_tile<<<ntiles * 32, 256, 0, s>>>(items, d_loc_bs, d_err, d_weight);
-    lc.bump(2);
+    uint32_t *d_loc_bs = d_scratch;
+    uint32_t *d_synp = d_scratch + (size_t)ntiles * TILE_LOC_WORDS;
+    k_tile_synd<<<ntiles * 32 * SYN_PARTS, 256, 0, s>>>(items, d_cts, d_synp);
+    k_tile_bm<<<ntiles, 256, smem, s>>>(items, d_synp, d_loc_bs, plans);
+    k_root_tile<<<ntiles * 4, ROOT_WARPS * 32, root_smem, s>>>(items, d_loc_bs, d_err, d_weight, plans);
+    lc.bump(3);
     return cudaGetLastError();
 }
 

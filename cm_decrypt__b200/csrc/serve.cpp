@@ -64,11 +64,12 @@ struct KeyEntry {
 
 struct Slot {
     cudaStream_t stream = nullptr;
-    cudaEvent_t done = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr;  // bracket the batch's device work
+    uint64_t t_launch = 0;
     uint8_t *h_in = nullptr, *d_in = nullptr;  // packed inputs (see dispatch)
     uint32_t *h_err = nullptr, *d_err = nullptr;
     uint16_t *h_w = nullptr, *d_w = nullptr;
-    uint32_t *d_locbs = nullptr;        // tile path: bitsliced locators
+    uint32_t *d_locbs = nullptr;        // tile path scratch (TILE_SCRATCH_WORDS per tile)
     std::vector<uint32_t> slot_of;      // request i -> result row (item slot)
     size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
@@ -98,6 +99,8 @@ struct cmd_server {
     int status = CMD_OK;
     // statistics
     std::vector<uint32_t> lat_ns;
+    std::vector<uint32_t> gpu_ns;   // per batch
+    std::vector<uint32_t> wait_ns;  // per request: arrival -> launch
     uint64_t submitted = 0, completed = 0, refused = 0, batches = 0, fused_batches = 0, batched_cts = 0;
     uint64_t t_first = 0, t_last = 0;
     uint64_t tick = 0;
@@ -230,6 +233,9 @@ int cmd_server::launch(Slot &sl)
     LaunchCounter lc{&eng->launches};
     cudaStream_t s = sl.stream;
     cudaError_t e;
+    sl.t_launch = now_ns();
+    if ((e = cudaEventRecord(sl.start, s)) != cudaSuccess)
+        return cuda_fail(e, "server event");
     sl.fused = cfg.fused_threshold > 0 && B >= cfg.fused_threshold;
     sl.slot_of.resize(B);
     if (!sl.fused) {
@@ -239,8 +245,12 @@ int cmd_server::launch(Slot &sl)
         std::vector<uint32_t> by_set(B);
         for (size_t i = 0; i < B; i++)
             by_set[i] = (uint32_t)i;
-        std::stable_sort(by_set.begin(), by_set.end(),
-                         [&](uint32_t a, uint32_t b) { return kset[key_idx[a]] < kset[key_idx[b]]; });
+        // by set, then by key: requests of one key sit side by side, so their
+        // syndrome CTAs read the same table rows close together in time
+        std::stable_sort(by_set.begin(), by_set.end(), [&](uint32_t a, uint32_t b) {
+            const int sa = kset[key_idx[a]], sb = kset[key_idx[b]];
+            return sa != sb ? sa < sb : key_idx[a] < key_idx[b];
+        });
         uint32_t ntiles = 0;
         size_t i = 0;
         while (i < B) {
@@ -254,10 +264,10 @@ int cmd_server::launch(Slot &sl)
                 if (q < cnt) {
                     const uint32_t r = by_set[i + q];
                     const FusedKeyRef &kr = krefs[key_idx[r]];
-                    items[slot] = LatItem{kr.tab, kr.Lbs, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE, kr.set, cnt};
+                    items[slot] = LatItem{kr.tab, kr.bctl, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE, kr.set, cnt};
                     sl.slot_of[r] = slot;
                 } else {
-                    items[slot] = LatItem{krefs[0].tab, krefs[0].Lbs, 0, slot * ERR_STRIDE, -1, cnt};
+                    items[slot] = LatItem{krefs[0].tab, krefs[0].bctl, 0, slot * ERR_STRIDE, -1, cnt};
                 }
             }
             ntiles++;
@@ -266,7 +276,10 @@ int cmd_server::launch(Slot &sl)
         sl.rows_used = (size_t)ntiles * 32;
         if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
             return cuda_fail(e, "server H2D");
-        e = launch_tile_path(sl.d_in + lay.items, sl.d_in + lay.cts, ntiles, sl.d_locbs, sl.d_err, sl.d_w, s, lc);
+        FftPlans plans;
+        for (int st = 0; st < NSETS; st++)
+            plans.p[st] = eng->fft[st];
+        e = launch_tile_path(sl.d_in + lay.items, sl.d_in + lay.cts, ntiles, sl.d_locbs, sl.d_err, sl.d_w, plans, s, lc);
         if (e != cudaSuccess)
             return cuda_fail(e, "server tile-path launch");
     } else {
@@ -404,8 +417,12 @@ void cmd_server::complete_loop()
         Slot &sl = slots[si];
         const cudaError_t e = cudaEventSynchronize(sl.done);
         const uint64_t t = now_ns();
-        std::vector<uint32_t> lats;
+        float gpu_ms = 0;
+        if (e == cudaSuccess)
+            cudaEventElapsedTime(&gpu_ms, sl.start, sl.done);
+        std::vector<uint32_t> lats, waits;
         lats.reserve(sl.reqs.size());
+        waits.reserve(sl.reqs.size());
         std::vector<cmd_completion> done;
         for (size_t i = 0; i < sl.reqs.size(); i++) {
             const Request &r = sl.reqs[i];
@@ -414,6 +431,7 @@ void cmd_server::complete_loop()
                 memcpy(r.err_out, sl.h_err + (size_t)sl.slot_of[i] * ERR_STRIDE, info.n / 8);
             const uint64_t lat = t - r.t_arrive;
             lats.push_back((uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu));
+            waits.push_back((uint32_t)std::min<uint64_t>(sl.t_launch - r.t_arrive, 0xFFFFFFFFu));
             if (cfg.record_completions)
                 done.push_back(
                     cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[sl.slot_of[i]], 0, lat});
@@ -425,6 +443,8 @@ void cmd_server::complete_loop()
         }
         completions.insert(completions.end(), done.begin(), done.end());
         lat_ns.insert(lat_ns.end(), lats.begin(), lats.end());
+        wait_ns.insert(wait_ns.end(), waits.begin(), waits.end());
+        gpu_ns.push_back((uint32_t)(gpu_ms * 1e6f));
         completed += sl.reqs.size();
         t_last = t;
         for (uint32_t k : sl.pinned)
@@ -454,7 +474,7 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
     const size_t B = cfg->max_batch;
     InLayout lay(B, B);
     srv->in_bytes = lay.total;
-    const size_t rows = row_cap(B), locbs = tile_cap(B) * 130 * 16 * 4;
+    const size_t rows = row_cap(B), locbs = tile_cap(B) * (size_t)TILE_SCRATCH_WORDS * 4;
     const size_t dev_per_slot = lay.total + rows * ERR_STRIDE * 4 + rows * 2 + locbs + 4 * 256;
     srv->device_bytes = dev_per_slot * cfg->slots;
     if (!budget_take(eng, srv->device_bytes)) {
@@ -468,7 +488,9 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
         if (e == cudaSuccess)
             e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess)
-            e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
+            e = cudaEventCreate(&sl.done);
+        if (e == cudaSuccess)
+            e = cudaEventCreate(&sl.start);
         if (e == cudaSuccess)
             e = cudaMallocHost(&sl.h_in, lay.total);
         if (e == cudaSuccess)
@@ -526,6 +548,8 @@ void cmd_server_destroy(cmd_server *srv)
         cudaFree(sl.d_counter);
         if (sl.done)
             cudaEventDestroy(sl.done);
+        if (sl.start)
+            cudaEventDestroy(sl.start);
         if (sl.stream)
             cudaStreamDestroy(sl.stream);
     }
@@ -624,6 +648,17 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
     st->resident_keys = 0;
     for (const auto &k : srv->keys)
         st->resident_keys += k.key != nullptr;
+    auto quantile = [](std::vector<uint32_t> v, double f) {
+        if (v.empty())
+            return 0.0;
+        size_t i = (size_t)(f * (v.size() - 1));
+        std::nth_element(v.begin(), v.begin() + i, v.end());
+        return v[i] / 1e3;
+    };
+    st->gpu_p50_us = quantile(srv->gpu_ns, 0.50);
+    st->gpu_p99_us = quantile(srv->gpu_ns, 0.99);
+    st->wait_p50_us = quantile(srv->wait_ns, 0.50);
+    st->wait_p99_us = quantile(srv->wait_ns, 0.99);
     if (!srv->lat_ns.empty()) {
         std::vector<uint32_t> v = srv->lat_ns;
         auto q = [&](double f) {
@@ -643,6 +678,8 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
         st->decaps_per_s = srv->completed / ((srv->t_last - srv->t_first) * 1e-9);
     if (reset) {
         srv->lat_ns.clear();
+        srv->gpu_ns.clear();
+        srv->wait_ns.clear();
         srv->submitted -= srv->completed;
         srv->completed = 0;
         srv->refused = srv->batches = srv->fused_batches = srv->batched_cts = 0;

@@ -1,20 +1,32 @@
-"""Algorithmic work per decryption, the fixed yardstick for the int-ALU
-roofline of the decrypt kernels.
+"""Algorithmic work per decryption: the int-ALU roofline of the decrypt kernels.
 
 A GF(2^m) multiply is counted as m^2 fused AND-XOR bit operations plus R_m
 reduction XORs (R_12 = 22 for the trinomial x^12+x^3+1, R_13 = 48 for the
-pentanomial x^13+x^4+x^3+x+1); one 32-bit lop3 performs 32 bit operations.
-Per decryption:
+pentanomial x^13+x^4+x^3+x+1); one 32-bit lop3 performs 32 bit operations,
+so every figure below is bit operations / 32 ("lane-ops").
 
-  W_synd  = sb * 2t * m / 32                     masked XOR of table rows
-  W_bm    = [sum_{N<2t} (min(N,t)+1) + 2t(t+1) + 8*2t] * (m^2 + R_m) / 32
-            (discrepancies, C updates, d/b counted as 8 multiplies)
-  W_chien = n * t * (m^2 + R_m + m) / 32          Horner at every support point
+Work of the algorithm the fused kernel executes, per decryption:
 
-so ``achieved = decaps/s * W`` lane-ops/s, compared with the measured lop3
-rate.  A root finder that does less work than Horner still divides by the
-same W.  Bytes per decryption that must cross HBM: the ciphertext in and the
-n-bit error vector out.
+  W_synd = sb * 2t * m / 32                      masked XOR of table rows
+  W_bm   = [sum_{N<2t} (min(N,t)+1) + 2t(t+1) + 8*2t] * (m^2 + R_m) / 32
+           (discrepancies, C updates, d/b counted as 8 multiplies)
+  W_root = additive FFT at all 2^m field elements, D = ceil(log2(t+1)):
+           [ (D-1) 2^D (m^2+R_m)                   radix-conversion scalings
+           + 2^(D-2) m D(D-1)                      Taylor-expansion XORs
+           + D 2^(m-1) (m^2 + R_m + 2m)            butterflies
+           + 2^m m                                 zero flags
+           + (2m-1) 2^(m-1) 3 ] / 32               support network swaps
+
+``achieved = decaps/s * (W_synd + W_bm + W_root)`` lane-ops/s against the
+measured lop3 rate.
+
+The fixed yardstick of the reference's algorithm (Horner at every support
+point, root_13.c:216-240) is kept beside it:
+
+  W_chien = n * t * (m^2 + R_m + m) / 32
+
+Bytes per decryption that must cross HBM: the ciphertext in and the n-bit
+error vector out.
 """
 from __future__ import annotations
 
@@ -22,15 +34,27 @@ SETS = {348864: (12, 3488, 64, 96), 460896: (13, 4608, 96, 156), 6688128: (13, 6
         6960119: (13, 6960, 119, 194), 8192128: (13, 8192, 128, 208)}
 
 
+def fft_depth(t: int) -> int:
+    d = 0
+    while (1 << d) < t + 1:
+        d += 1
+    return d
+
+
 def work_per_decap(set_id: int) -> dict:
     m, n, t, ct = SETS[set_id]
     r = 22 if m == 12 else 48
+    mul = m * m + r
     sb = 8 * ct
     w_synd = sb * 2 * t * m / 32
     disc = sum(min(N, t) + 1 for N in range(2 * t))
-    w_bm = (disc + 2 * t * (t + 1) + 8 * 2 * t) * (m * m + r) / 32
-    w_chien = n * t * (m * m + r + m) / 32
-    return {"synd": w_synd, "bm": w_bm, "chien": w_chien, "total": w_synd + w_bm + w_chien}
+    w_bm = (disc + 2 * t * (t + 1) + 8 * 2 * t) * mul / 32
+    D = fft_depth(t)
+    w_root = ((D - 1) * (1 << D) * mul + (1 << (D - 2)) * m * D * (D - 1)
+              + D * (1 << (m - 1)) * (mul + 2 * m) + (1 << m) * m + (2 * m - 1) * (1 << (m - 1)) * 3) / 32
+    w_chien = n * t * (mul + m) / 32
+    return {"synd": w_synd, "bm": w_bm, "root_fft": w_root, "total": w_synd + w_bm + w_root,
+            "yardstick_chien": w_chien, "yardstick_total": w_synd + w_bm + w_chien}
 
 
 def hbm_bytes_per_decap(set_id: int) -> int:

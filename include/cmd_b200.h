@@ -227,6 +227,9 @@ typedef struct {
     double mean_batch, p50_us, p99_us, max_us, mean_us;
     double decaps_per_s;  /* completed / (last completion - first arrival)  */
     double offered_per_s; /* cmd_server_loadgen: arrival rate actually offered */
+    double gpu_p50_us, gpu_p99_us; /* per batch: device time from the input copy
+                                      to the end of the result copy          */
+    double wait_p50_us, wait_p99_us; /* per request: arrival -> batch launch  */
 } cmd_server_stats;
 
 int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server **out);
