@@ -15,10 +15,12 @@
 //    choices are the bits of s.
 //  * fft_root_one: one warp, one locator q.  A 2^m-element bitsliced array
 //    (plane-major, m planes of 2^(m-5) words, in shared memory) starts from
-//    the depth-D constants -- position Y gets constant bitrev_D(Y >> (m-D))
-//    -- and takes D levels of butterflies A' = A + w*B, B' = A' + B between
-//    whole words; position Y then holds f(bitrev_m(Y)), which is where the
-//    support network expects element Y's value.  Zero flags (one bit per
+//    the depth-D constants -- position Y gets constant bitrev_D(Y >> (m-D)),
+//    folded into the first butterfly level -- and takes D levels of
+//    butterflies A' = A + w*B, B' = A' + B between whole words; position Y
+//    then holds f(bitrev_m(Y)), which is where the support network expects
+//    element Y's value (the last level feeds the zero test directly, without
+//    storing the evaluations).  Zero flags (one bit per
 //    element) go through the 2m-1 swap layers: pairs inside a word by
 //    shifts, across lanes by shuffles, inside a lane by registers.  Bit j of
 //    the result is "f(L[j]) == 0", the reference's error bit j.
@@ -97,17 +99,39 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
     using F = FftDims<S>;
     constexpr int M = F::M, D = F::D, NWD = F::NWD, R = F::R, NW = F::NW;
     constexpr uint32_t FULL = 0xFFFFFFFFu;
+    // Depth D-1: both operands are depth-D constants, read straight from cv.
+    {
+        constexpr int sbit = M - D - 5, Sw = 1 << sbit;
+        const uint32_t *twd = tw + (size_t)((1 << (M - 5)) - (1 << (M - 5 - (D - 1)))) * 16;
+#pragma unroll 1
+        for (int j = 0; j < R / 2; j++) {
+            const int P2 = lane + 32 * j;
+            const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
+            const int sa = (int)(__brev((uint32_t)(wa >> sbit)) >> (32 - D));
+            const int sb = (int)(__brev((uint32_t)((wa + Sw) >> sbit)) >> (32 - D));
+            const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+            uint32_t B[M], G[M], p[2 * M - 1];
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        const int w = lane + 32 * j;
-        const int sidx = (int)(__brev((uint32_t)(w >> (M - D - 5))) >> (32 - D));
+            for (int k = 0; k < M; k++) {
+                B[k] = 0u - ((cv[sb * CVS + k] >> q) & 1u);
+                G[k] = __ldg(g + k);
+            }
 #pragma unroll
-        for (int k = 0; k < M; k++)
-            fa[k * NWD + w] = 0u - ((cv[sidx * CVS + k] >> q) & 1u);
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            bs_mul_acc<M>(p, G, B);
+            bs_reduce<M>(p);
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const uint32_t na = (0u - ((cv[sa * CVS + k] >> q) & 1u)) ^ p[k];
+                fa[k * NWD + wa] = na;
+                fa[k * NWD + wa + Sw] = na ^ B[k];
+            }
+        }
+        __syncwarp();
     }
-    __syncwarp();
 #pragma unroll
-    for (int d = D - 1; d >= 0; d--) {
+    for (int d = D - 2; d >= 1; d--) {
         const int sbit = M - d - 6, Sw = 1 << sbit;
         const uint32_t *twd = tw + (size_t)((1 << (M - 5)) - (1 << (M - 5 - d))) * 16;
 #pragma unroll 1
@@ -136,15 +160,38 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
         }
         __syncwarp();
     }
+    // Depth 0 pairs word w = lane + 32j with w + 2^(m-6): exactly the words
+    // z[j] and z[j + R/2] of this lane, so the zero flags come straight from
+    // the butterfly (no store of the evaluations).
     uint32_t z[R];
+    {
+        constexpr int Sw = 1 << (M - 6);
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        const int w = lane + 32 * j;
-        uint32_t any = 0;
+        for (int j = 0; j < R / 2; j++) {
+            const int wa = lane + 32 * j;
+            const uint32_t *g = tw + (size_t)wa * 16;  // depth 0: offset 0
+            uint32_t A[M], B[M], G[M], p[2 * M - 1];
 #pragma unroll
-        for (int k = 0; k < M; k++)
-            any |= fa[k * NWD + w];
-        z[j] = ~any;
+            for (int k = 0; k < M; k++) {
+                A[k] = fa[k * NWD + wa];
+                B[k] = fa[k * NWD + wa + Sw];
+                G[k] = __ldg(g + k);
+            }
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            bs_mul_acc<M>(p, G, B);
+            bs_reduce<M>(p);
+            uint32_t anya = 0, anyb = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const uint32_t na = A[k] ^ p[k];
+                anya |= na;
+                anyb |= na ^ B[k];
+            }
+            z[j] = ~anya;
+            z[j + R / 2] = ~anyb;
+        }
     }
     __syncwarp();  // fa may be refilled right after this call
 #pragma unroll
