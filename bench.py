@@ -140,7 +140,7 @@ SERVE_SETS = (348864, 460896, 6688128, 6960119, 8192128)
 SERVE_WEIGHTS = (30, 15, 20, 20, 15)
 
 
-SERVER_CONFIG = {"max_batch": 8192, "slots": 4, "max_wait_us": 100, "fused_threshold": 0}
+SERVER_CONFIG = {"max_batch": 8192, "slots": 6, "max_wait_us": 150, "fused_threshold": 0}
 
 
 def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: int = 16384,

@@ -112,8 +112,13 @@ template <int S> struct TileSmem {
     uint32_t syn[32 * SYN_STRIDE];
     uint32_t S_[2 * P::T * P::M];
     uint32_t ring[(P::T + 2) * P::M];
-    uint32_t part[2][8][16];  // per-warp partial discrepancies, double-buffered by step parity
+    uint32_t cs[(P::T + 1) * P::M];       // C after each update, for the discrepancy warps
+    alignas(16) uint32_t part[2][8][16];  // per-warp partial discrepancies, double-buffered by step parity
 };
+
+// Threads of k_tile_bm: two roles of up to five warps each (t+1 <= 129
+// coefficients per role).
+constexpr int TILE_THREADS = 320;
 
 template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32_t *synp, uint32_t *loc_bs,
                                                          const uint16_t *scalpow, uint8_t *smem_raw)
@@ -141,7 +146,7 @@ template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32
     __syncthreads();
 
     // ---- 2. transpose: S_[j*M + k] bit q = bit k of syndrome j of ct q ----
-    for (int w = warp; w < TW; w += 8) {
+    for (int w = warp; w < TW; w += TILE_THREADS / 32) {
         const uint32_t v = sm.syn[lane * SYN + w];
 #pragma unroll
         for (int h = 0; h < 2; h++) {
@@ -158,22 +163,31 @@ template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32
         sm.ring[v] = (v == M) ? FULL : 0u;  // B = x
     __syncthreads();
 
-    // ---- 3. scaled Berlekamp-Massey, thread i owns coefficient i ----------
-    // One barrier per step: right after updating its coefficient a thread
-    // already computes its share of the next step's discrepancy.
-    const int i = tid;
-    uint32_t C[M], bb[M];
+    // ---- 3. scaled Berlekamp-Massey, two warps per 32 coefficients ---------
+    // Warps [NWB, 2 NWB) own the coefficients (thread i of the role owns C_i
+    // and its B ring slot) and do the update C <- b*C + d*x*B; warps
+    // [0, NWB) compute the shares C_i * S_{N-i} of the next discrepancy.
+    // Per step: (A) update: d*x*B, the one product that needs this step's
+    // discrepancy (b*C was formed in the previous step); barrier; (B) the
+    // discrepancy warps multiply the new C by the syndromes while the
+    // update warps form b*C for the next step; barrier.  Two warps per
+    // scheduler share the work and hide each other's latency.
+    const bool dsc = warp < NWB;
+    const bool upd = warp >= NWB && warp < 2 * NWB;
+    const int i = upd ? tid - 32 * NWB : tid;
+    uint32_t C[M], bb[M], q1[2 * M - 1];
 #pragma unroll
     for (int k = 0; k < M; k++) {
         C[k] = (i == 0 && k == 0) ? FULL : 0u;
         bb[k] = k == 0 ? FULL : 0u;
     }
-    int Lq = 0;  // L of ciphertext `lane` (every warp keeps a copy)
-    // share of discrepancy N (N = 0 here): C_i * S_{N-i} for i <= min(N, t),
-    // XOR-reduced over the warp into part[warp]
+#pragma unroll
+    for (int k = 0; k < 2 * M - 1; k++)
+        q1[k] = k < M ? C[k] : 0u;  // b*C with b = 1
+    int Lq = 0;  // L of ciphertext `lane` (update warps)
+    // discrepancy warps: share of discrepancy N, C_i * S_{N-i} for
+    // i <= min(N, t), XOR-reduced over the warp into part[N & 1][warp]
     auto partial = [&](int N) {
-        if (warp >= NWB)
-            return;
         const int lim = N < T ? N : T;
         uint32_t p[2 * M - 1];
 #pragma unroll
@@ -194,75 +208,103 @@ template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32
                 sm.part[N & 1][warp][k] = v;
         }
     };
-    partial(0);
+    if (dsc)
+        partial(0);
     __syncthreads();
 #pragma unroll 1
     for (int N = 0; N < 2 * T; N++) {
-        uint32_t d[M], mne = 0;
+        if (upd) {
+            // (A) the discrepancy, then the update
+            uint32_t dd[16];
 #pragma unroll
-        for (int k = 0; k < M; k++) {
-            uint32_t v = 0;
+            for (int k = 0; k < 16; k++)
+                dd[k] = 0;
 #pragma unroll
-            for (int w = 0; w < NWB; w++)
-                v ^= sm.part[N & 1][w][k];
-            d[k] = v;
-            mne |= v;
-        }
-        const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
-        const uint32_t mle = __ballot_sync(FULL, my_mle);
-        Lq = my_mle ? N + 1 - Lq : Lq;
-        // Coefficients above N + 1 of C and x*B are still zero (their ring
-        // entries were never written): whole warps past that bound skip.
-        if (i <= T && i <= N + 1) {
-            int slot = i + (R - (N % R)) % R;
-            slot = slot >= R ? slot - R : slot;
-            uint32_t *bp = sm.ring + slot * M;
-            uint32_t bv[M], q[2 * M - 1];
+            for (int w = 0; w < NWB; w++) {
+                const uint4 *pr = reinterpret_cast<const uint4 *>(sm.part[N & 1][w]);
 #pragma unroll
-            for (int k = 0; k < M; k++)
-                bv[k] = bp[k];
-#pragma unroll
-            for (int k = 0; k < 2 * M - 1; k++)
-                q[k] = 0;
-            bs_mul_acc<M>(q, bb, C);
-            bs_mul_acc<M>(q, d, bv);
-            bs_reduce<M>(q);
+                for (int v = 0; v < 4; v++) {
+                    const uint4 x = pr[v];
+                    dd[4 * v] ^= x.x;
+                    dd[4 * v + 1] ^= x.y;
+                    dd[4 * v + 2] ^= x.z;
+                    dd[4 * v + 3] ^= x.w;
+                }
+            }
+            uint32_t d[M], mne = 0;
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                bp[k] = (bv[k] & ~mle) | (C[k] & mle);
-                C[k] = q[k];
+                d[k] = dd[k];
+                mne |= dd[k];
             }
-        }
-        const int freeslot = (R - ((N + 1) % R)) % R;
-        if (tid < M)
-            sm.ring[freeslot * M + tid] = 0;
+            const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
+            const uint32_t mle = __ballot_sync(FULL, my_mle);
+            Lq = my_mle ? N + 1 - Lq : Lq;
+            // Coefficients above N + 1 of C and x*B are still zero (their
+            // ring entries were never written): whole warps past that skip.
+            if (i <= T && i <= N + 1) {
+                int slot = i + (R - (N % R)) % R;
+                slot = slot >= R ? slot - R : slot;
+                uint32_t *bp = sm.ring + slot * M;
+                uint32_t bv[M];
 #pragma unroll
-        for (int k = 0; k < M; k++)
-            bb[k] = (bb[k] & ~mle) | (d[k] & mle);
-        if (N + 1 < 2 * T)
-            partial(N + 1);  // writes part[(N+1)&1]; part[N&1] was read above
+                for (int k = 0; k < M; k++)
+                    bv[k] = bp[k];
+                bs_mul_acc<M>(q1, d, bv);
+                bs_reduce<M>(q1);
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    bp[k] = (bv[k] & ~mle) | (C[k] & mle);
+                    C[k] = q1[k];
+                    sm.cs[i * M + k] = q1[k];
+                }
+            }
+            const int freeslot = (R - ((N + 1) % R)) % R;
+            if (i < M)
+                sm.ring[freeslot * M + i] = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bb[k] = (bb[k] & ~mle) | (d[k] & mle);
+        }
         __syncthreads();
+        if (N + 1 < 2 * T) {
+            // (B) next discrepancy shares; b*C for the next update
+            if (dsc) {
+                const int lim = N + 1 < T ? N + 1 : T;
+                if (i <= lim)
+#pragma unroll
+                    for (int k = 0; k < M; k++)
+                        C[k] = sm.cs[i * M + k];
+                partial(N + 1);
+            } else if (upd && i <= T && i <= N + 2) {
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    q1[k] = 0;
+                bs_mul_acc<M>(q1, bb, C);
+            }
+            __syncthreads();
+        }
     }
     // ---- 4. radix conversion, converted locators out -----------------------
     // Entry x of the conversion array is C[T-x] (bm.c:62-65 reverses the
     // locator before root() evaluates it), zero for T < x < 2^D; S_ is free.
     using F = FftDims<S>;
     static_assert(F::NX * M <= 2 * T * M && F::NX * 16 <= TILE_LOC_WORDS, "conversion array size");
-    if (i <= T)
+    if (upd && i <= T)
 #pragma unroll
         for (int k = 0; k < M; k++)
             sm.S_[(T - i) * M + k] = C[k];
     for (int v = tid; v < (F::NX - T - 1) * M; v += blockDim.x)
         sm.S_[(T + 1) * M + v] = 0u;
     __syncthreads();
-    fft_convert<S, M, 256>(sm.S_, scalpow, tid, [] { __syncthreads(); });
+    fft_convert<S, M, TILE_THREADS>(sm.S_, scalpow, tid, [] { __syncthreads(); });
     for (int v = tid; v < F::NX * M; v += blockDim.x) {
         const int x = v / M, k = v - x * M;
         loc_bs[x * 16 + k] = sm.S_[v];
     }
 }
 
-__global__ void __launch_bounds__(256) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
+__global__ void __launch_bounds__(TILE_THREADS) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
                                                  uint32_t *__restrict__ loc_bs, FftPlans plans)
 {
     extern __shared__ __align__(16) uint8_t smem_tile[];
@@ -350,7 +392,7 @@ cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t
     uint32_t *d_loc_bs = d_scratch;
     uint32_t *d_synp = d_scratch + (size_t)ntiles * TILE_LOC_WORDS;
     k_tile_synd<<<ntiles * 32 * SYN_PARTS, 256, 0, s>>>(items, d_cts, d_synp);
-    k_tile_bm<<<ntiles, 256, smem, s>>>(items, d_synp, d_loc_bs, plans);
+    k_tile_bm<<<ntiles, TILE_THREADS, smem, s>>>(items, d_synp, d_loc_bs, plans);
     k_root_tile<<<ntiles * 4, ROOT_WARPS * 32, root_smem, s>>>(items, d_loc_bs, d_err, d_weight, plans);
     lc.bump(3);
     return cudaGetLastError();
