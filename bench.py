@@ -62,6 +62,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--serve-keys", type=int, default=1024)
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the all-sets (2^20 each) and mixed-batch (2^18) measurements")
     return ap.parse_args()
 
 
@@ -202,6 +204,112 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
     under = [p for p in out["points"] if p["p99_ms"] < 1.0]
     out["max_decaps_per_s_p99_under_1ms"] = max((p["decaps_per_s"] for p in under), default=None)
     return out
+
+
+def _time_stream(fn, stream, reps: int, warmup: int) -> float:
+    """ms per call of fn(), CUDA events on `stream` after `warmup` untimed calls."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3) -> dict:
+    """each parameter set in turn, `count` ciphertexts of one
+    seeded key (the reference kem/ key of the set), autotuned fused kernel
+    replayed as a CUDA graph; every output checked against its planted error
+    vector and weight t.  Inputs (>= 100 MB per set) exceed L2.  The plain
+    path is timed beside it for 6960119."""
+    import torch
+    out = {}
+    sp = stream.cuda_stream
+    for s in SERVE_SETS:
+        sk = open(os.path.join(REPO, "tests", "golden", "kem", f"sk_{s}.bin"), "rb").read()
+        key = cmd.Key(eng, s, sk)
+        info = key.info
+        cts, planted, _ = cmd.PubKey(s, sk).ciphertexts(seed=77, count=count)
+        d_ct = torch.from_numpy(cts).cuda()
+        d_err = torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda")
+        d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+        tuned = cmd.tune(eng, key)
+        g = cmd.Graph(eng, key, d_ct.data_ptr(), count, d_err.data_ptr(), d_w.data_ptr(), path="fused")
+        ms = _time_stream(lambda: g.launch(sp), stream, reps, 2)
+        g.close()
+        ok = bool(np.array_equal(d_err.cpu().numpy().astype("<u4").view(np.uint8).reshape(count, -1)
+                                 [:, : info.err_bytes], planted)
+                  and (d_w.cpu().numpy().view(np.uint16) == info.t).all())
+        row = {"ciphertexts": count, "fused_ms": ms, "fused_decaps_per_s": count / (ms * 1e-3),
+               "tuned": tuned, "results_match_planted": ok}
+        if s == SET:
+            msp = _time_stream(lambda: cmd.decrypt_device(eng, key, d_ct.data_ptr(), count, d_err.data_ptr(),
+                                                          d_w.data_ptr(), sp, "plain"), stream, 1, 1)
+            row["plain_ms"] = msp
+            row["plain_decaps_per_s"] = count / (msp * 1e-3)
+            row["fused_speedup"] = msp / ms
+        out[str(s)] = row
+        del d_ct, d_err, d_w
+        key.free()
+    return out
+
+
+def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3) -> dict:
+    """64 seeded keys spread 13/13/13/13/12 over the five
+    sets, `count` ciphertexts with the set drawn uniformly per ciphertext (key
+    uniform within the set), 10% uniformly random mt-bit strings, all in one
+    cmd_decrypt_mixed_device launch.  Valid ciphertexts are checked against
+    their planted vectors; malformed ones must not decode to weight t."""
+    import torch
+    golden = {s: open(os.path.join(REPO, "tests", "golden", "kem", f"sk_{s}.bin"), "rb").read() for s in SERVE_SETS}
+    per_set = [nkeys // 5 + (1 if i < nkeys % 5 else 0) for i in range(5)]
+    ring = [(s, cmd.synth_key(s, golden[s], 0xC0FFEE + 97 * i + j)) for i, s in enumerate(SERVE_SETS)
+            for j in range(per_set[i])]
+    keys = [cmd.Key(eng, s, sk) for s, sk in ring]
+    g = np.random.default_rng(0x5EED4)
+    set_of = g.integers(0, 5, count)
+    first = np.cumsum([0] + per_set[:-1])
+    key_idx = (first[set_of] + (g.random(count) * np.array(per_set)[set_of]).astype(np.int64)).astype(np.uint32)
+    CT, EW = 208, 256
+    buf = np.zeros((count, CT), np.uint8)
+    planted = np.zeros((count, 1024), np.uint8)
+    valid = np.zeros(count, np.uint8)
+    for k in range(len(keys)):
+        idx = np.nonzero(key_idx == k)[0]
+        if idx.size == 0:
+            continue
+        c, e, v = cmd.PubKey(*ring[k]).ciphertexts(seed=1000 + k, count=idx.size, malformed_permille=100)
+        buf[idx, : c.shape[1]] = c
+        planted[idx, : e.shape[1]] = e
+        valid[idx] = v
+    ct_off = np.arange(count, dtype=np.uint64) * CT
+    err_off = np.arange(count, dtype=np.uint64) * EW
+    d_ct = torch.from_numpy(buf.reshape(-1)).cuda()
+    d_err = torch.zeros(count * EW, dtype=torch.int32, device="cuda")
+    d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+    sp = stream.cuda_stream
+    ms = _time_stream(lambda: cmd.decrypt_mixed_device(eng, keys, key_idx, d_ct.data_ptr(), ct_off, d_err.data_ptr(),
+                                                       err_off, d_w.data_ptr(), sp), stream, reps, 2)
+    E = d_err.cpu().numpy().astype("<u4").view(np.uint8).reshape(count, 1024)
+    W = d_w.cpu().numpy().view(np.uint16)
+    ok = True
+    t_of = np.array([cmd.set_info(s).t for s, _ in ring])[key_idx]
+    for i, s in enumerate(SERVE_SETS):
+        rows = np.nonzero((valid == 1) & (set_of == i))[0]
+        nb = cmd.set_info(s).err_bytes
+        ok = ok and bool(np.array_equal(E[rows, :nb], planted[rows, :nb]) and (W[rows] == t_of[rows]).all())
+    bad = np.nonzero(valid == 0)[0]
+    for k in keys:
+        k.free()
+    return {"keys": len(keys), "ciphertexts": count, "malformed_fraction": float(1 - valid.mean()),
+            "ms_per_launch": ms, "decaps_per_s": count / (ms * 1e-3),
+            "valid_match_planted": ok, "malformed_below_weight_t": bool((W[bad] < t_of[bad]).all()),
+            "timed": "whole cmd_decrypt_mixed_device call: host round planning, plan upload and the fused kernel"}
 
 
 def run_reference(args) -> None:
@@ -412,6 +520,9 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(sk, cts)
+    if world == 1 and not args.no_configs:
+        line["configs"] = {"all_sets_2^20": config_all_sets(cmd, eng, stream),
+                           "mixed_64keys_2^18": config_mixed(cmd, eng, stream)}
     for g_ in graphs:
         g_.close()
     if world == 1 and not args.no_serve:
