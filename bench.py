@@ -474,6 +474,29 @@ def main() -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    # The same through cmd_decrypt_positions (binary wire format: t+1 u16 per
+    # ciphertext come back instead of n/8 bytes).
+    h_pos = torch.empty((count, info.t + 1), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    L = cmd.lib()
+    pos_call = lambda: cmd._check(L.cmd_decrypt_positions(eng.handle, key.handle, h_cts.ctypes.data, count,
+                                                          h_pos.ctypes.data), "cmd_decrypt_positions")
+    pos_call()
+    if not (h_pos[:, 0] == info.t).all():
+        raise SystemExit("bench: positions weights differ from t")
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        pos_call()
+    torch.cuda.synchronize()
+    pos_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([pos_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        pos_s = float(t.item())
+    pos_ok = bool(np.array_equal(h_pos[:512], cmd.positions_from_errors(SET, planted[:512])))
+
     value = world * count * args.steps / (ms * 1e-3)
     per_rank = count * args.steps / (ms * 1e-3)
     w = work_per_decap(SET)
@@ -504,6 +527,10 @@ def main() -> None:
         "e2e": {"value": world * count * args.steps / e2e_s, "unit": "decaps/s",
                 "h2d_bytes_per_step": count * info.ct_bytes,
                 "d2h_bytes_per_step": count * (info.err_bytes + 2)},
+        "e2e_positions": {"value": world * count * args.steps / pos_s, "unit": "decaps/s",
+                          "call": "cmd_decrypt_positions (error positions, binary errorstream rows)",
+                          "h2d_bytes_per_step": count * info.ct_bytes,
+                          "d2h_bytes_per_step": count * (info.t + 1) * 2, "results_match_planted": pos_ok},
         "roofline": {"bound": "int_alu", "achieved": achieved / 1e12, "peak": int_peak / 1e12,
                      "unit": "Tlane-ops/s (lop3)", "frac": achieved / int_peak,
                      "peak_source": "measured on this GPU: lop3.b32 chains (cmd_bench_int_peak)",

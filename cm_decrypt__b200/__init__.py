@@ -117,6 +117,13 @@ def lib() -> ctypes.CDLL:
         "cmd_stage_root_images": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
         "cmd_errorstream_format": (_i32, [_i32, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz)]),
         "cmd_errorstream_write": (_i32, [_i32, _vp, _sz, ctypes.c_char_p, _i32]),
+        "cmd_decrypt_positions": (_i32, [_vp, _vp, _vp, _sz, _vp]),
+        "cmd_decrypt_positions_device": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_positions_format": (_i32, [_i32, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz)]),
+        "cmd_positions_write": (_i32, [_i32, _vp, _sz, ctypes.c_char_p, _i32]),
+        "cmd_positions_to_errorstream": (_i32, [ctypes.c_char_p, ctypes.c_char_p]),
+        "cmd_decrypt_files_binary": (_i32, [_vp, _i32, ctypes.c_char_p, ctypes.c_char_p, _sz, ctypes.c_char_p,
+                                            ctypes.POINTER(ctypes.c_double)]),
         "cmd_decrypt_files": (_i32, [_vp, _i32, ctypes.c_char_p, ctypes.c_char_p, _sz, ctypes.c_char_p, _i32,
                                      ctypes.POINTER(ctypes.c_double)]),
         "cmd_bench_int_peak": (_i32, [_vp, ctypes.POINTER(ctypes.c_double)]),
@@ -438,6 +445,66 @@ def decrypt_files(engine: Engine, set_id: int, sk_path: str, ct_path: str, katnu
     _check(lib().cmd_decrypt_files(engine.handle, set_index(set_id), sk_path.encode(), ct_path.encode(), katnum,
                                    out_path.encode(), PATHS[path], ctypes.byref(secs)), "cmd_decrypt_files")
     return secs.value
+
+
+# ---- error positions and the binary errorstream ------------------------------
+def decrypt_positions(engine: Engine, key: Key, cts: np.ndarray) -> np.ndarray:
+    """Host buffers -> uint16 [count, t+1]: weight, positions ascending, 0xFFFF."""
+    info = key.info
+    c = np.ascontiguousarray(cts, np.uint8).reshape(-1, info.ct_bytes)
+    out = np.zeros((c.shape[0], info.t + 1), np.uint16)
+    _check(lib().cmd_decrypt_positions(engine.handle, key.handle, _ptr(c), c.shape[0], _ptr(out)),
+           "cmd_decrypt_positions")
+    return out
+
+
+def decrypt_positions_device(engine: Engine, key: Key, d_cts: int, count: int, d_pos: int, stream: int = 0) -> None:
+    _check(lib().cmd_decrypt_positions_device(engine.handle, key.handle, d_cts, count, d_pos, stream or None),
+           "cmd_decrypt_positions_device")
+
+
+def positions_text(set_id: int, pos: np.ndarray) -> bytes:
+    info = set_info(set_id)
+    p = np.ascontiguousarray(pos, np.uint16).reshape(-1, info.t + 1)
+    need = _sz()
+    lib().cmd_positions_format(set_index(set_id), _ptr(p), p.shape[0], None, 0, ctypes.byref(need))
+    buf = ctypes.create_string_buffer(need.value + 1)
+    _check(lib().cmd_positions_format(set_index(set_id), _ptr(p), p.shape[0], buf, need.value + 1,
+                                      ctypes.byref(need)), "cmd_positions_format")
+    return buf.raw[:need.value]
+
+
+def write_positions(set_id: int, pos: np.ndarray, path: str, append: bool = False) -> None:
+    info = set_info(set_id)
+    p = np.ascontiguousarray(pos, np.uint16).reshape(-1, info.t + 1)
+    _check(lib().cmd_positions_write(set_index(set_id), _ptr(p), p.shape[0], path.encode(), int(append)),
+           "cmd_positions_write")
+
+
+def positions_to_errorstream(binary_path: str, text_path: str) -> None:
+    _check(lib().cmd_positions_to_errorstream(binary_path.encode(), text_path.encode()),
+           "cmd_positions_to_errorstream")
+
+
+def decrypt_files_binary(engine: Engine, set_id: int, sk_path: str, ct_path: str, katnum: int,
+                         out_path: str) -> float:
+    secs = ctypes.c_double()
+    _check(lib().cmd_decrypt_files_binary(engine.handle, set_index(set_id), sk_path.encode(), ct_path.encode(),
+                                          katnum, out_path.encode(), ctypes.byref(secs)), "cmd_decrypt_files_binary")
+    return secs.value
+
+
+def positions_from_errors(set_id: int, err: np.ndarray) -> np.ndarray:
+    """Reference conversion (host, numpy): packed error vectors -> positions rows."""
+    info = set_info(set_id)
+    e = np.ascontiguousarray(err, np.uint8).reshape(-1, info.err_bytes)
+    bits = np.unpackbits(e, axis=1, bitorder="little")
+    out = np.full((e.shape[0], info.t + 1), 0xFFFF, np.uint16)
+    for r in range(e.shape[0]):
+        idx = np.nonzero(bits[r])[0]
+        out[r, 0] = idx.size
+        out[r, 1: 1 + min(idx.size, info.t)] = idx[: info.t]
+    return out
 
 
 # ---- synthetic workloads -----------------------------------------------------

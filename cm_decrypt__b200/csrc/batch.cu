@@ -72,7 +72,7 @@ static uint32_t round_size(cmd_engine *eng, int set, int wpb, size_t count, bool
 }
 
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter)
+                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos)
 {
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
@@ -96,6 +96,8 @@ int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
     a.single_set = set;
     fill_fft(a, eng);
     a.err_stride = (uint32_t)si.nw;
+    a.pos = d_pos;
+    a.pos_stride = (uint32_t)(si.t + 1);
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaMemsetAsync(counter)");
@@ -113,12 +115,12 @@ cudaError_t fused_prepare(cmd_engine *eng, int set)
 }
 
 int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                     uint16_t *d_weight, cudaStream_t s)
+                     uint16_t *d_weight, cudaStream_t s, uint16_t *d_pos)
 {
     int rc = ensure_counter(eng);
     if (rc)
         return rc;
-    return run_fused_counter(eng, key, d_cts, count, d_err, d_weight, s, eng->tile_counter);
+    return run_fused_counter(eng, key, d_cts, count, d_err, d_weight, s, eng->tile_counter, d_pos);
 }
 
 // Set shared by every ciphertext of a mixed batch, or -1.

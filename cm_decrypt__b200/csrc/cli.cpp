@@ -16,8 +16,9 @@ static int usage(const char *argv0)
 {
     fprintf(stderr,
             "Usage: %s <348864|460896|6688128|6960119|8192128> [KATNUM>0] [--sk PATH] [--ct PATH]\n"
-            "          [--out PATH] [--path auto|plain|fused] [--device N]\n",
-            argv0);
+            "          [--out PATH] [--path auto|plain|fused] [--device N] [--format text|binary]\n"
+            "       %s --to-text BINARY_PATH TEXT_PATH   (binary errorstream -> text)\n",
+            argv0, argv0);
     return CMD_E_ARG;
 }
 
@@ -25,6 +26,14 @@ int main(int argc, char **argv)
 {
     if (argc < 2)
         return usage(argv[0]);
+    if (!strcmp(argv[1], "--to-text")) {
+        if (argc != 4)
+            return usage(argv[0]);
+        const int rc = cmd_positions_to_errorstream(argv[2], argv[3]);
+        if (rc != CMD_OK)
+            fprintf(stderr, "convert: %s\n", cmd_last_error());
+        return rc;
+    }
     cmd_set set;
     if (cmd_set_from_name(argv[1], &set) != CMD_OK)
         return usage(argv[0]);
@@ -37,10 +46,16 @@ int main(int argc, char **argv)
     std::string out = "../../results/output/errorstream0_" + name + ".bin";
     cmd_path path = CMD_PATH_AUTO;
     int device = 0;
+    bool binary = false;
     for (int i = 2; i < argc; i++) {
         const std::string a = argv[i];
         auto val = [&]() -> const char * { return i + 1 < argc ? argv[++i] : nullptr; };
-        if (a == "--sk" || a == "--ct" || a == "--out" || a == "--path" || a == "--device") {
+        if (a == "--format") {
+            const char *v = val();
+            if (!v || (strcmp(v, "text") && strcmp(v, "binary")))
+                return usage(argv[0]);
+            binary = !strcmp(v, "binary");
+        } else if (a == "--sk" || a == "--ct" || a == "--out" || a == "--path" || a == "--device") {
             const char *v = val();
             if (!v)
                 return usage(argv[0]);
@@ -74,7 +89,8 @@ int main(int argc, char **argv)
         return rc;
     }
     double secs = 0;
-    rc = cmd_decrypt_files(eng, set, sk.c_str(), ct.c_str(), (size_t)katnum, out.c_str(), path, &secs);
+    rc = binary ? cmd_decrypt_files_binary(eng, set, sk.c_str(), ct.c_str(), (size_t)katnum, out.c_str(), &secs)
+                : cmd_decrypt_files(eng, set, sk.c_str(), ct.c_str(), (size_t)katnum, out.c_str(), path, &secs);
     if (rc != CMD_OK) {
         fprintf(stderr, "decrypt: %s\n", cmd_last_error());
     } else {
@@ -82,7 +98,7 @@ int main(int argc, char **argv)
         printf("ciphertexts processed : %ld\n", katnum);
         printf("device decrypt time   : %.6f s (host buffers, incl. transfers)\n", secs);
         printf("throughput            : %.2f cw/s\n", secs > 0 ? katnum / secs : 0.0);
-        printf("errorstream           : %s\n", out.c_str());
+        printf("errorstream           : %s%s\n", out.c_str(), binary ? " (binary positions)" : "");
     }
     cmd_engine_destroy(eng);
     return rc;

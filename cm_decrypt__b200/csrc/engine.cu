@@ -471,4 +471,52 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
     return CMD_OK;
 }
 
+int cmd_decrypt_positions_device(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count,
+                                 uint16_t *d_pos, void *stream)
+{
+    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_pos)))
+        return CMD_E_ARG;
+    if (count == 0)
+        return CMD_OK;
+    cudaSetDevice(eng->device);
+    std::lock_guard<std::mutex> lk(eng->mu);
+    return run_fused_single(eng, key, d_cts, count, nullptr, nullptr, stream ? (cudaStream_t)stream : eng->stream,
+                            d_pos);
+}
+
+int cmd_decrypt_positions(cmd_engine *eng, const cmd_key *key, const uint8_t *h_cts, size_t count, uint16_t *h_pos)
+{
+    if (!eng || !key || key->eng != eng || (count && (!h_cts || !h_pos)))
+        return CMD_E_ARG;
+    if (count == 0)
+        return CMD_OK;
+    cudaSetDevice(eng->device);
+    const SetInfo si = set_info(key->dev.set);
+    const size_t row = (size_t)si.t + 1;
+    std::lock_guard<std::mutex> lk(eng->mu);
+    const size_t chunk = std::min<size_t>(count, (size_t)1 << 20);
+    const size_t need = carve_size({chunk * si.ct, chunk * row * 2});
+    int rc = eng->io.reserve(eng, need);
+    if (rc)
+        return rc;
+    Carver cv{static_cast<uint8_t *>(eng->io.ptr)};
+    uint8_t *d_cts = cv.take<uint8_t>(chunk * si.ct);
+    uint16_t *d_pos = cv.take<uint16_t>(chunk * row);
+    cudaStream_t s = eng->stream;
+    for (size_t c0 = 0; c0 < count; c0 += chunk) {
+        const size_t n = std::min(chunk, count - c0);
+        cudaError_t e = cudaMemcpyAsync(d_cts, h_cts + c0 * si.ct, n * si.ct, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaMemcpyAsync(cts H2D)");
+        if ((rc = run_fused_single(eng, key, d_cts, n, nullptr, nullptr, s, d_pos)))
+            return rc;
+        e = cudaMemcpyAsync(h_pos + c0 * row, d_pos, n * row * 2, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "decrypt positions D2H");
+    }
+    return CMD_OK;
+}
+
 }  // extern "C"

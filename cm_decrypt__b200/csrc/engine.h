@@ -47,7 +47,7 @@ void budget_give(cmd_engine *eng, size_t bytes);
 int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
                uint32_t *d_err, uint16_t *d_weight, cudaStream_t s);
 int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                     uint16_t *d_weight, cudaStream_t s);
+                     uint16_t *d_weight, cudaStream_t s, uint16_t *d_pos = nullptr);
 size_t fused_smem(int set, int wpb);
 size_t smem_limit_bytes();
 int fused_blocks_per_sm(int single_set, int wpb, size_t smem);

@@ -91,10 +91,15 @@ __device__ __forceinline__ void fft_convert(uint32_t *cv, const uint16_t *__rest
 
 // One warp: error row (and weight) of locator q from the converted array cv
 // (bitsliced, cv[s * CVS + k]).  fa: this warp's FA_WORDS words of shared
-// memory.  erow: NW words.  Returns the weight (all lanes).
+// memory.  erow: NW words, or null.  prow: null, or t+1 u16 that receive the
+// weight, the flagged positions in ascending order and 0xFFFF in the unused
+// slots (the weight never exceeds t: the reversed locator's leading
+// coefficient is C[0], which the update never zeroes).  Returns the weight
+// (all lanes).
 template <int S, int CVS>
 __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t *fa, const uint32_t *__restrict__ tw,
-                                            const uint32_t *__restrict__ bctl, uint32_t *erow, int lane)
+                                            const uint32_t *__restrict__ bctl, uint32_t *erow, uint16_t *prow,
+                                            int lane)
 {
     using F = FftDims<S>;
     constexpr int M = F::M, D = F::D, NWD = F::NWD, R = F::R, NW = F::NW;
@@ -227,21 +232,52 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
             }
         }
     }
+    uint32_t v[R];
     int cnt = 0;
 #pragma unroll
     for (int j = 0; j < R; j++) {
         const int w = lane + 32 * j;
-        if (w < NW) {
-            const int left = F::N - 32 * w;
-            const uint32_t valid = left >= 32 ? FULL : ((1u << left) - 1u);
-            const uint32_t v = z[j] & valid;
-            erow[w] = v;
-            cnt += __popc(v);
-        }
+        const int left = F::N - 32 * w;
+        const uint32_t valid = left >= 32 ? FULL : (left > 0 ? ((1u << left) - 1u) : 0u);
+        v[j] = z[j] & valid;
+        if (erow && w < NW)
+            erow[w] = v[j];
+        cnt += __popc(v[j]);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
         cnt += __shfl_xor_sync(FULL, cnt, off);
+    if (prow) {
+        // Word w = lane + 32j: its positions start after those of every word
+        // with a smaller j, and of the lower lanes at the same j.  Every lane
+        // walks all 32 bits of its words (predicated stores, no branch on the
+        // error pattern).
+        int base = 0;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int c = __popc(v[j]);
+            int inc = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(FULL, inc, o);
+                inc += lane >= o ? y : 0;
+            }
+            int off = base + inc - c;
+            const int pos0 = 32 * (lane + 32 * j);
+#pragma unroll 8
+            for (int b = 0; b < 32; b++) {
+                const int bit = (int)((v[j] >> b) & 1u);
+                if (bit && off < F::T)
+                    prow[1 + off] = (uint16_t)(pos0 + b);
+                off += bit;
+            }
+            base += __shfl_sync(FULL, inc, 31);
+        }
+        for (int i = base + lane; i < F::T; i += 32)
+            prow[1 + i] = 0xFFFFu;
+        if (lane == 0)
+            prow[0] = (uint16_t)cnt;
+    }
     return cnt;
 }
 

@@ -315,8 +315,9 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     fft_convert<S, M, 32>(cv, pl.scalpow, lane, [] { __syncwarp(); });
     for (int q = 0; q < ntile; q++) {
         const uint64_t c = ct_index(rc, warp, q);
-        uint32_t *erow = a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride);
-        const int cnt = fft_root_one<S, M>(cv, q, fa, pl.tw, rc.key.bctl, erow, lane);
+        uint32_t *erow = a.err ? a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride) : nullptr;
+        uint16_t *prow = a.pos ? a.pos + c * (uint64_t)a.pos_stride : nullptr;
+        const int cnt = fft_root_one<S, M>(cv, q, fa, pl.tw, rc.key.bctl, erow, prow, lane);
         if (lane == 0 && a.weight)
             a.weight[c] = (uint16_t)cnt;
     }

@@ -98,6 +98,9 @@ struct FusedArgs {
     uint32_t *tile_counter;        // zeroed before the launch
     int single_set;                // >= 0: every round has this set
     uint32_t err_stride;           // words per error row when err_off is null
+    uint16_t *pos;                 // or null: per ciphertext t+1 u16, the weight
+                                   // then the error positions ascending, 0xFFFF after
+    uint32_t pos_stride;           // u16 per positions row
     FftPlanDev fft[NSETS];         // root-search plans, indexed by set
 };
 cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,

@@ -330,7 +330,7 @@ __device__ __forceinline__ void root_tile(const LatItem &it, const uint32_t *cv,
 {
     static_assert(FftDims<S>::FA_WORDS <= ROOT_FA_WORDS, "root array");
     const int lane = threadIdx.x & 31;
-    const int cnt = fft_root_one<S, 16>(cv, q, fa, pl.tw, it.bctl, err + it.err_off, lane);
+    const int cnt = fft_root_one<S, 16>(cv, q, fa, pl.tw, it.bctl, err + it.err_off, nullptr, lane);
     if (lane == 0 && weight)
         *weight = (uint16_t)cnt;
 }

@@ -182,6 +182,34 @@ int cmd_errorstream_format(cmd_set set, const uint8_t *h_err, size_t count,
 int cmd_errorstream_write(cmd_set set, const uint8_t *h_err, size_t count,
                           const char *path, int append);
 
+/* ---- error positions and the binary errorstream (no reference counterpart) */
+/* The decrypt result as error positions: row c of the output holds t+1 u16,
+ * the weight w, then the w flagged positions in ascending order (the numbers
+ * write_error_positions prints for that ciphertext), then 0xFFFF.  The
+ * weight never exceeds t (the reversed locator has degree exactly t).  Runs
+ * the fused kernel, which writes the rows directly: 2(t+1) bytes per
+ * ciphertext instead of n/8 (240 vs 870 bytes for 6960119).
+ * cmd_decrypt_positions takes host buffers (like cmd_decrypt_batch),
+ * cmd_decrypt_positions_device device buffers, asynchronous on `stream`. */
+int cmd_decrypt_positions(cmd_engine *eng, const cmd_key *key, const uint8_t *h_cts,
+                          size_t count, uint16_t *h_pos);
+int cmd_decrypt_positions_device(cmd_engine *eng, const cmd_key *key,
+                                 const uint8_t *d_cts, size_t count, uint16_t *d_pos,
+                                 void *stream);
+/* The errorstream text of positions rows: the same bytes cmd_errorstream_format
+ * gives for the equivalent error vectors. */
+int cmd_positions_format(cmd_set set, const uint16_t *h_pos, size_t count,
+                         char *out, size_t cap, size_t *out_len);
+/* Binary errorstream: a 24-byte header -- "CMDPOS01", the set id (u32 LE,
+ * e.g. 6960119), t (u32 LE), the row count (u64 LE) -- then the positions
+ * rows (t+1 u16 LE each).  Writing it is a copy of the rows; append != 0 adds
+ * rows to an existing file of the same set.  CMD_E_FILE on I/O errors or a
+ * foreign file. */
+int cmd_positions_write(cmd_set set, const uint16_t *h_pos, size_t count,
+                        const char *path, int append);
+/* Converts a binary errorstream into the reference's errorstream text. */
+int cmd_positions_to_errorstream(const char *binary_path, const char *text_path);
+
 /* ---- file contract ----------------------------------------------------- */
 /* Replaces `decrypt_<set> KATNUM` (decrypt.c:109-218): reads one sk
  * (sk_bytes) and katnum ciphertexts from the given files, decrypts on the GPU
@@ -192,6 +220,12 @@ int cmd_decrypt_files(cmd_engine *eng, cmd_set set, const char *sk_path,
                       const char *ct_path, size_t katnum,
                       const char *errorstream_path, cmd_path path,
                       double *out_seconds);
+/* As cmd_decrypt_files, writing the binary errorstream (positions rows, see
+ * cmd_positions_write) instead of the text; cmd_positions_to_errorstream
+ * turns it into the reference's text. */
+int cmd_decrypt_files_binary(cmd_engine *eng, cmd_set set, const char *sk_path,
+                             const char *ct_path, size_t katnum,
+                             const char *positions_path, double *out_seconds);
 
 /* ---- serving loop (no reference counterpart) ---------------------------- */
 /* Continuous batching of single-ciphertext decapsulation requests over many

@@ -201,6 +201,45 @@ def test_full_size_properties(engine, keys, path):
     assert (w == 119).all()
 
 
+@pytest.mark.parametrize("s", SETS)
+def test_positions_output(oracle_mod, engine, keys, s):
+    """cmd_decrypt_positions rows equal the positions of the packed error
+    vectors (oracle) for the kem fixtures, valid and malformed ciphertexts,
+    and their text is the reference errorstream."""
+    info = keys[s].info
+    kem = np.frombuffer(golden_ct(s), np.uint8).reshape(-1, info.ct_bytes)
+    pos = cmd.decrypt_positions(engine, keys[s], kem)
+    assert cmd.positions_text(s, pos) == golden_errorstream(s)
+    pk = cmd.PubKey(s, golden_sk(s))
+    cts, planted, valid = pk.ciphertexts(seed=31, count=333, malformed_permille=300)
+    ref = oracle_mod.Oracle(s).decrypt(golden_sk(s), cts, nthreads=8)
+    pos = cmd.decrypt_positions(engine, keys[s], cts)
+    assert np.array_equal(pos, cmd.positions_from_errors(s, ref))
+    assert (pos[valid == 1, 0] == info.t).all()
+    # device entry point, same rows
+    d_ct = dev(cts)
+    d_pos = torch.zeros((cts.shape[0], info.t + 1), dtype=torch.int16, device="cuda")
+    cmd.decrypt_positions_device(engine, keys[s], d_ct.data_ptr(), cts.shape[0], d_pos.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(d_pos.cpu().numpy().view(np.uint16), pos)
+
+
+def test_binary_errorstream_files_and_cli(engine, tmp_path):
+    s = 6960119
+    b = str(tmp_path / "es.pos")
+    cmd.decrypt_files_binary(engine, s, os.path.join(KEM, f"sk_{s}.bin"), os.path.join(KEM, f"ct_{s}.bin"), 5, b)
+    t = str(tmp_path / "es.txt")
+    r = subprocess.run([cmd.CLI_PATH, "--to-text", b, t], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert open(t, "rb").read() == golden_errorstream(s)
+    b2 = str(tmp_path / "cli.pos")
+    r = subprocess.run([cmd.CLI_PATH, str(s), "5", "--sk", os.path.join(KEM, f"sk_{s}.bin"), "--ct",
+                        os.path.join(KEM, f"ct_{s}.bin"), "--out", b2, "--format", "binary"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert open(b2, "rb").read() == open(b, "rb").read()
+
+
 def test_decrypt_files_and_cli(engine, tmp_path):
     s = 348864
     out = str(tmp_path / "es.bin")

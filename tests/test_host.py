@@ -116,3 +116,51 @@ def test_synth_key_rejects_bad_args():
     with pytest.raises(ValueError):
         cmd.synth_key(99, b"\0" * 10, 1)
     assert cmd.lib().cmd_synth_key(7, None, 1, None) == cmd.CMD_E_ARG
+
+
+def _sparse_errors(s, rows, seed):
+    """Error vectors of weight 0..t (the only weights a decode can produce)."""
+    info = cmd.set_info(s)
+    g = rng(seed)
+    err = np.zeros((rows, info.err_bytes), np.uint8)
+    for r in range(rows):
+        w = int(g.integers(0, info.t + 1)) if r > 1 else (0 if r == 0 else info.t)
+        for p in g.choice(info.n, w, replace=False):
+            err[r, p >> 3] |= np.uint8(1 << (p & 7))
+    return err
+
+
+@pytest.mark.parametrize("s", SETS)
+def test_positions_text_matches_errorstream(oracle_mod, s):
+    err = _sparse_errors(s, 9, s)
+    pos = cmd.positions_from_errors(s, err)
+    info = cmd.set_info(s)
+    assert pos.shape == (9, info.t + 1)
+    assert pos[0, 0] == 0 and (pos[0, 1:] == 0xFFFF).all()
+    assert pos[1, 0] == info.t and (np.diff(pos[1, 1:].astype(np.int64)) > 0).all()
+    assert cmd.positions_text(s, pos) == oracle_mod.Oracle(s).errorstream(err)
+
+
+def test_binary_errorstream_file_roundtrip(tmp_path, oracle_mod):
+    s = 6960119
+    err = _sparse_errors(s, 12, 5)
+    pos = cmd.positions_from_errors(s, err)
+    b = str(tmp_path / "es.pos")
+    cmd.write_positions(s, pos[:7], b)
+    cmd.write_positions(s, pos[7:], b, append=True)
+    raw = open(b, "rb").read()
+    assert raw[:8] == b"CMDPOS01"
+    assert int.from_bytes(raw[8:12], "little") == s and int.from_bytes(raw[16:24], "little") == 12
+    assert len(raw) == 24 + 12 * 120 * 2
+    t = str(tmp_path / "es.txt")
+    cmd.positions_to_errorstream(b, t)
+    assert open(t, "rb").read() == oracle_mod.Oracle(s).errorstream(err)
+    # a file of another set, or not a positions file at all, is refused
+    with pytest.raises(cmd.CmdError) as ei:
+        cmd.write_positions(348864, cmd.positions_from_errors(348864, _sparse_errors(348864, 1, 1)), b, append=True)
+    assert ei.value.code == cmd.CMD_E_FILE
+    junk = tmp_path / "junk.bin"
+    junk.write_bytes(b"\0" * 64)
+    with pytest.raises(cmd.CmdError) as ei:
+        cmd.positions_to_errorstream(str(junk), t)
+    assert ei.value.code == cmd.CMD_E_FILE
