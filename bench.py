@@ -497,6 +497,15 @@ def main() -> None:
         pos_s = float(t.item())
     pos_ok = bool(np.array_equal(h_pos[:512], cmd.positions_from_errors(SET, planted[:512])))
 
+    # KEM decapsulation on the same device-resident batches: decrypt, the
+    # re-encoding / weight / padding check and SHAKE256 session keys.
+    d_keys = torch.zeros((count, 32), dtype=torch.uint8, device="cuda")
+    d_acc = torch.zeros(count, dtype=torch.uint8, device="cuda")
+    cmd.prepare_decap(eng, key)
+    dec_ms = _time_stream(lambda: cmd.kem_decap_device(eng, key, d_cts[0].data_ptr(), count, d_keys.data_ptr(),
+                                                       d_acc.data_ptr(), sp), stream, max(1, args.steps // 2), 2)
+    dec_ok = bool(d_acc.cpu().numpy().all())
+
     value = world * count * args.steps / (ms * 1e-3)
     per_rank = count * args.steps / (ms * 1e-3)
     w = work_per_decap(SET)
@@ -527,6 +536,9 @@ def main() -> None:
         "e2e": {"value": world * count * args.steps / e2e_s, "unit": "decaps/s",
                 "h2d_bytes_per_step": count * info.ct_bytes,
                 "d2h_bytes_per_step": count * (info.err_bytes + 2)},
+        "kem_decap": {"value": world * count / (dec_ms * 1e-3), "unit": "decaps/s", "ms_per_batch": dec_ms,
+                      "call": "cmd_kem_decap_device (decrypt + re-encoding check + SHAKE256 keys), device buffers",
+                      "all_valid_accepted": dec_ok},
         "e2e_positions": {"value": world * count * args.steps / pos_s, "unit": "decaps/s",
                           "call": "cmd_decrypt_positions (error positions, binary errorstream rows)",
                           "h2d_bytes_per_step": count * info.ct_bytes,

@@ -117,6 +117,10 @@ def lib() -> ctypes.CDLL:
         "cmd_stage_root_images": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
         "cmd_errorstream_format": (_i32, [_i32, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz)]),
         "cmd_errorstream_write": (_i32, [_i32, _vp, _sz, ctypes.c_char_p, _i32]),
+        "cmd_key_prepare_decap": (_i32, [_vp, _vp]),
+        "cmd_kem_decap": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_kem_decap_device": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),
+        "cmd_pubkey_columns": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
         "cmd_decrypt_positions": (_i32, [_vp, _vp, _vp, _sz, _vp]),
         "cmd_decrypt_positions_device": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
         "cmd_positions_format": (_i32, [_i32, _vp, _sz, _vp, _sz, ctypes.POINTER(_sz)]),
@@ -447,6 +451,29 @@ def decrypt_files(engine: Engine, set_id: int, sk_path: str, ct_path: str, katnu
     return secs.value
 
 
+# ---- KEM decapsulation --------------------------------------------------------
+def prepare_decap(engine: Engine, key: Key) -> None:
+    """Derives the key's public key (host) and keeps it on the device."""
+    _check(lib().cmd_key_prepare_decap(engine.handle, key.handle), "cmd_key_prepare_decap")
+
+
+def kem_decap(engine: Engine, key: Key, cts: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Host buffers -> (keys uint8 [count, 32], accept uint8 [count])."""
+    info = key.info
+    c = np.ascontiguousarray(cts, np.uint8).reshape(-1, info.ct_bytes)
+    keys = np.zeros((c.shape[0], 32), np.uint8)
+    acc = np.zeros(c.shape[0], np.uint8)
+    _check(lib().cmd_kem_decap(engine.handle, key.handle, _ptr(c), c.shape[0], _ptr(keys), _ptr(acc)),
+           "cmd_kem_decap")
+    return keys, acc
+
+
+def kem_decap_device(engine: Engine, key: Key, d_cts: int, count: int, d_keys: int, d_accept: int = 0,
+                     stream: int = 0) -> None:
+    _check(lib().cmd_kem_decap_device(engine.handle, key.handle, d_cts, count, d_keys, d_accept or None,
+                                      stream or None), "cmd_kem_decap_device")
+
+
 # ---- error positions and the binary errorstream ------------------------------
 def decrypt_positions(engine: Engine, key: Key, cts: np.ndarray) -> np.ndarray:
     """Host buffers -> uint16 [count, t+1]: weight, positions ascending, 0xFFFF."""
@@ -541,6 +568,15 @@ class PubKey:
         _check(lib().cmd_synth_ciphertexts(self.handle, seed, count, malformed_permille, _ptr(cts), _ptr(err),
                                            _ptr(valid), nt), "cmd_synth_ciphertexts")
         return cts, err, valid
+
+    def columns(self) -> np.ndarray:
+        """The T block of [I | T]: uint64 [n - mt, words]; bit r of column i = T[r, i]."""
+        info = self.info
+        w = _sz()
+        _check(lib().cmd_pubkey_columns(self.handle, None, 0, ctypes.byref(w)), "cmd_pubkey_columns")
+        out = np.zeros((info.n - info.m * info.t, w.value), np.uint64)
+        _check(lib().cmd_pubkey_columns(self.handle, _ptr(out), out.size, ctypes.byref(w)), "cmd_pubkey_columns")
+        return out
 
 
 def cuda_available() -> bool:

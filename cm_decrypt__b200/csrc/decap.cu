@@ -1,0 +1,449 @@
+// KEM decapsulation around the decrypt path.  No counterpart in the
+// reference, which encapsulates only: kem/common/core/operations.c:15-34
+// computes C = [I | T] e and K = SHAKE256(1 || e || C) (32 bytes).  The
+// Classic McEliece decapsulation inverts that with implicit rejection:
+//
+//   e = decrypt(C)                       (the engine's fused kernel)
+//   accept = padding bits mt..8*ct-1 of C are zero  &&  wt(e) == t
+//            &&  C == [I | T] e          (e re-encodes to C)
+//   K = SHAKE256(b || v || C),  b = accept,  v = accept ? e : s
+//
+// with T the systematic public key (derived from the secret key on the host,
+// once per key) and s the random string stored at the end of the secret key.
+//
+// k_decap: 8 warps per CTA, lane = ciphertext, 256 ciphertexts per CTA.
+//  1. re-encoding: each lane keeps the mt-bit word vector acc = T * e[mt..n)
+//     in registers; the columns of T stream through shared memory in
+//     32-column chunks (cp.async double buffer shared by the CTA) and every
+//     column is masked by the lane's error bit -- every column for every
+//     ciphertext, so the work and the memory traffic do not depend on e;
+//  2. acc ^ e[0..mt) ^ C must vanish; padding and weight checks;
+//  3. SHAKE256 of the 1 + n/8 + ct byte preimage, one lane per ciphertext
+//     (Keccak-f[1600] as defined in FIPS 202; round constants and rotation
+//     offsets derived from the standard's definitions at compile time); the
+//     preimage's v bytes are selected with masks.
+#include <cstring>
+#include <vector>
+
+#include "engine.h"
+#include "fused_impl.cuh"
+
+namespace cmd {
+
+namespace {
+
+// ---- Keccak-f[1600] constants from their FIPS 202 definitions -----------
+// rc(t): output bit of the LFSR x^8 + x^6 + x^5 + x^4 + 1 (FIPS 202 alg. 5).
+constexpr bool rc_bit(int t)
+{
+    if (t % 255 == 0)
+        return true;
+    unsigned r = 1;  // R = 10000000 (bit 0 is the first position)
+    for (int i = 1; i <= t % 255; i++) {
+        unsigned r8 = r << 1;  // R = 0 || R
+        const unsigned b8 = (r8 >> 8) & 1u;
+        r8 ^= b8 | (b8 << 4) | (b8 << 5) | (b8 << 6);
+        r = r8 & 0xFFu;
+    }
+    return r & 1u;
+}
+struct KeccakConst {
+    uint64_t rc[24];
+    int rot[25];  // offset of lane x + 5y
+    constexpr KeccakConst() : rc(), rot()
+    {
+        for (int i = 0; i < 24; i++) {  // iota: RC[i], bit 2^j - 1 = rc(j + 7i)
+            uint64_t v = 0;
+            for (int j = 0; j <= 6; j++)
+                if (rc_bit(j + 7 * i))
+                    v |= 1ull << ((1 << j) - 1);
+            rc[i] = v;
+        }
+        rot[0] = 0;  // rho: walk (x, y) = (1, 0) -> (y, 2x + 3y)
+        int x = 1, y = 0;
+        for (int t = 0; t < 24; t++) {
+            rot[x + 5 * y] = ((t + 1) * (t + 2) / 2) % 64;
+            const int nx = y, ny = (2 * x + 3 * y) % 5;
+            x = nx;
+            y = ny;
+        }
+    }
+};
+constexpr KeccakConst KC{};
+static_assert(KC.rc[0] == 1 && KC.rot[1] == 1, "Keccak constants");
+__constant__ uint64_t kRC[24] = {KC.rc[0],  KC.rc[1],  KC.rc[2],  KC.rc[3],  KC.rc[4],  KC.rc[5],
+                                 KC.rc[6],  KC.rc[7],  KC.rc[8],  KC.rc[9],  KC.rc[10], KC.rc[11],
+                                 KC.rc[12], KC.rc[13], KC.rc[14], KC.rc[15], KC.rc[16], KC.rc[17],
+                                 KC.rc[18], KC.rc[19], KC.rc[20], KC.rc[21], KC.rc[22], KC.rc[23]};
+// rho offset of lane (x, y), folded to a constant in the unrolled round.
+__host__ __device__ constexpr int keccak_rot(int x0, int y0)
+{
+    if (x0 == 0 && y0 == 0)
+        return 0;
+    int x = 1, y = 0;
+    for (int t = 0; t < 24; t++) {
+        if (x == x0 && y == y0)
+            return ((t + 1) * (t + 2) / 2) % 64;
+        const int nx = y, ny = (2 * x + 3 * y) % 5;
+        x = nx;
+        y = ny;
+    }
+    return 0;
+}
+static_assert(keccak_rot(1, 0) == KC.rot[1] && keccak_rot(4, 4) == KC.rot[24], "Keccak rotations");
+
+__device__ __forceinline__ uint64_t rotl64(uint64_t v, int r) { return r ? (v << r) | (v >> (64 - r)) : v; }
+
+__device__ __forceinline__ void keccak_f(uint64_t *A)
+{
+#pragma unroll 1
+    for (int round = 0; round < 24; round++) {
+        uint64_t C[5], B[25];
+#pragma unroll
+        for (int x = 0; x < 5; x++)
+            C[x] = A[x] ^ A[x + 5] ^ A[x + 10] ^ A[x + 15] ^ A[x + 20];
+#pragma unroll
+        for (int x = 0; x < 5; x++) {
+            const uint64_t D = C[(x + 4) % 5] ^ rotl64(C[(x + 1) % 5], 1);
+#pragma unroll
+            for (int y = 0; y < 5; y++)
+                A[x + 5 * y] ^= D;
+        }
+        // rho and pi: B[y, 2x + 3y] = rotl(A[x, y], rot[x, y])
+#pragma unroll
+        for (int x = 0; x < 5; x++)
+#pragma unroll
+            for (int y = 0; y < 5; y++)
+                B[y + 5 * ((2 * x + 3 * y) % 5)] = rotl64(A[x + 5 * y], keccak_rot(x, y));
+        // chi
+#pragma unroll
+        for (int y = 0; y < 5; y++)
+#pragma unroll
+            for (int x = 0; x < 5; x++)
+                A[x + 5 * y] = B[x + 5 * y] ^ (~B[(x + 1) % 5 + 5 * y] & B[(x + 2) % 5 + 5 * y]);
+        A[0] ^= kRC[round];
+    }
+}
+
+constexpr int COLS = 32;  // public-key columns per staged chunk
+
+template <int S> struct DecapDims {
+    using P = Set<S>;
+    static constexpr int MT = P::M * P::T;
+    static constexpr int CW = (MT + 31) / 32;        // u32 words per column
+    static constexpr int CWP = (CW + 3) / 4 * 4;     // column stride (16-byte rows)
+    static constexpr int XC = P::N - MT;             // columns of T
+    static constexpr int NB = P::N / 8;              // bytes of e and of s
+    static constexpr int MSG = 1 + NB + P::CT;       // preimage bytes
+};
+
+}  // namespace
+
+struct DecapArgs {
+    const uint8_t *cts;
+    const uint32_t *err;       // error rows, nw words each
+    const uint16_t *weight;
+    const uint32_t *pkT;       // column c of T at pkT + c * CWP
+    const uint8_t *s;          // the secret key's n/8-byte string s
+    uint8_t *keys;             // 32 bytes per ciphertext
+    uint8_t *accept;           // or null: 1 byte per ciphertext
+    uint64_t count;
+};
+
+template <int S> __global__ void __launch_bounds__(256) k_decap(DecapArgs a)
+{
+    using P = Set<S>;
+    using Q = DecapDims<S>;
+    constexpr int CW = Q::CW, CWP = Q::CWP, XC = Q::XC, MT = Q::MT, NW = P::NW;
+    extern __shared__ __align__(16) uint32_t colbuf[];  // 2 x COLS x CWP words
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint64_t c = (uint64_t)blockIdx.x * 256 + tid;
+    const bool live = c < a.count;
+    const uint64_t cc = live ? c : 0;
+    const uint32_t *erow = a.err + cc * NW;
+
+    // ---- 1. acc = T * e[mt..n), every column masked by the error bit ------
+    uint32_t acc[CW];
+#pragma unroll
+    for (int w = 0; w < CW; w++)
+        acc[w] = 0;
+    constexpr int NCH = (XC + COLS - 1) / COLS;
+    constexpr int CHUNK_V = COLS * CWP / 4;
+    auto stage = [&](int ch) {
+        uint32_t *dst = colbuf + (ch & 1) * COLS * CWP;
+        const int cols = XC - ch * COLS < COLS ? XC - ch * COLS : COLS;
+        for (int v = tid; v < CHUNK_V; v += 256) {
+            if (v * 4 < cols * CWP)
+                cp_async16(dst + 4 * v, a.pkT + (size_t)ch * COLS * CWP + 4 * v);
+        }
+        cp_async_commit();
+    };
+    stage(0);
+    uint32_t ew = 0;
+#pragma unroll 1
+    for (int ch = 0; ch < NCH; ch++) {
+        if (ch + 1 < NCH) {
+            stage(ch + 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const uint32_t *buf = colbuf + (ch & 1) * COLS * CWP;
+        const int cols = XC - ch * COLS < COLS ? XC - ch * COLS : COLS;
+#pragma unroll 1
+        for (int j = 0; j < cols; j++) {
+            const int bit = MT + ch * COLS + j;
+            if (j == 0 || (bit & 31) == 0)
+                ew = live ? erow[bit >> 5] : 0u;
+            const uint32_t m = 0u - ((ew >> (bit & 31)) & 1u);
+            const uint4 *col = reinterpret_cast<const uint4 *>(buf + j * CWP);
+#pragma unroll
+            for (int v = 0; v < CWP / 4; v++) {
+                const uint4 x = col[v];
+                if (4 * v + 0 < CW) acc[4 * v + 0] ^= x.x & m;
+                if (4 * v + 1 < CW) acc[4 * v + 1] ^= x.y & m;
+                if (4 * v + 2 < CW) acc[4 * v + 2] ^= x.z & m;
+                if (4 * v + 3 < CW) acc[4 * v + 3] ^= x.w & m;
+            }
+        }
+        __syncthreads();
+    }
+    if (!live)
+        return;  // no block-wide barrier follows
+
+    // ---- 2. acceptance ------------------------------------------------------
+    const uint8_t *ct = a.cts + cc * P::CT;
+    uint32_t diff = 0;
+#pragma unroll
+    for (int w = 0; w < CW; w++) {
+        uint32_t cw = 0;
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            if (4 * w + b < P::CT)
+                cw |= (uint32_t)ct[4 * w + b] << (8 * b);
+        uint32_t d = acc[w] ^ erow[w] ^ cw;
+        if (32 * w + 32 > MT)
+            d &= (1u << (MT - 32 * w)) - 1u;  // bits mt.. are the padding check's
+        diff |= d;
+    }
+    uint32_t pad = 0;
+    for (int b = MT; b < 8 * P::CT; b++)
+        pad |= (ct[b >> 3] >> (b & 7)) & 1u;
+    const bool ok = diff == 0 && pad == 0 && a.weight[cc] == P::T;
+    const uint32_t okm = ok ? 0xFFu : 0u;
+    if (a.accept)
+        a.accept[cc] = ok ? 1 : 0;
+
+    // ---- 3. K = SHAKE256(b || v || C), 32 bytes ------------------------------
+    // preimage byte i: 0 -> b; 1..NB -> v; then C; then the pad10*1 padding
+    // with the SHAKE domain bits (0x1F ... 0x80) over whole 136-byte blocks.
+    constexpr int RATE = 136;
+    constexpr int NBLK = Q::MSG / RATE + 1;
+    const uint8_t *eb = reinterpret_cast<const uint8_t *>(erow);
+    auto msg = [&](int i) -> uint32_t {
+        if (i == 0)
+            return okm & 1u;
+        if (i <= Q::NB)
+            return (eb[i - 1] & okm) | (a.s[i - 1] & ~okm & 0xFFu);
+        if (i < Q::MSG)
+            return ct[i - 1 - Q::NB];
+        uint32_t v = i == Q::MSG ? 0x1Fu : 0u;
+        if (i == NBLK * RATE - 1)
+            v |= 0x80u;
+        return v;
+    };
+    uint64_t A[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++)
+        A[i] = 0;
+#pragma unroll 1
+    for (int blk = 0; blk < NBLK; blk++) {
+#pragma unroll
+        for (int l = 0; l < RATE / 8; l++) {  // static lane index: A stays in registers
+            uint64_t v = 0;
+#pragma unroll
+            for (int b = 0; b < 8; b++)
+                v |= (uint64_t)msg(blk * RATE + 8 * l + b) << (8 * b);
+            A[l] ^= v;
+        }
+        keccak_f(A);
+    }
+    uint64_t *out = reinterpret_cast<uint64_t *>(a.keys + cc * 32);
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        out[i] = A[i];
+    (void)lane;
+}
+
+size_t decap_pk_words(int set)
+{
+    return dispatch_set(set, [&]<int S>() -> size_t { return (size_t)DecapDims<S>::XC * DecapDims<S>::CWP; });
+}
+
+// Column-major copy of the public key's T block for k_decap (host side).
+int decap_pk_columns(int set, const uint8_t *sk, std::vector<uint32_t> &out)
+{
+    cmd_pubkey *pk = nullptr;
+    int rc = cmd_synth_pubkey((cmd_set)set, sk, &pk);
+    if (rc)
+        return rc;
+    std::vector<uint64_t> cols;
+    size_t xw = 0;
+    rc = cmd_pubkey_columns(pk, nullptr, 0, &xw);
+    const SetInfo si = set_info(set);
+    const int mt = si.m * si.t, xc = si.n - mt;
+    cols.resize((size_t)xc * xw);
+    if (rc == CMD_OK)
+        rc = cmd_pubkey_columns(pk, cols.data(), cols.size(), &xw);
+    cmd_synth_pubkey_free(pk);
+    if (rc)
+        return rc;
+    dispatch_set(set, [&]<int S>() {
+        using Q = DecapDims<S>;
+        out.assign((size_t)Q::XC * Q::CWP, 0);
+        for (int cidx = 0; cidx < Q::XC; cidx++)
+            for (int w = 0; w < Q::CW; w++) {
+                const uint64_t v = cols[(size_t)cidx * xw + (w >> 1)];
+                out[(size_t)cidx * Q::CWP + w] = (uint32_t)(v >> (32 * (w & 1)));
+            }
+        return 0;
+    });
+    return CMD_OK;
+}
+
+cudaError_t launch_decap(int set, const uint8_t *d_cts, const uint32_t *d_err, const uint16_t *d_w,
+                         const uint32_t *d_pk, const uint8_t *d_s, uint8_t *d_keys, uint8_t *d_accept, size_t count,
+                         cudaStream_t s, LaunchCounter lc)
+{
+    if (count == 0)
+        return cudaSuccess;
+    DecapArgs a{d_cts, d_err, d_w, d_pk, d_s, d_keys, d_accept, count};
+    return dispatch_set(set, [&]<int S>() -> cudaError_t {
+        const size_t smem = 2 * (size_t)COLS * DecapDims<S>::CWP * 4;
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(k_decap<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess)
+                return e;
+            attr = true;
+        }
+        k_decap<S><<<(unsigned)((count + 255) / 256), 256, smem, s>>>(a);
+        lc.bump();
+        return cudaGetLastError();
+    });
+}
+
+}  // namespace cmd
+
+using namespace cmd;
+
+extern "C" {
+
+int cmd_key_prepare_decap(cmd_engine *eng, cmd_key *key)
+{
+    if (!eng || !key || key->eng != eng)
+        return CMD_E_ARG;
+    if (key->pk)
+        return CMD_OK;
+    const int set = key->dev.set;
+    const SetInfo si = set_info(set);
+    std::vector<uint8_t> sk(si.sk);
+    cudaSetDevice(eng->device);
+    cudaError_t e = cudaMemcpy(sk.data(), key->dev.sk, si.sk, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "secret key D2H");
+    std::vector<uint32_t> cols;
+    int rc = decap_pk_columns(set, sk.data(), cols);
+    if (rc) {
+        set_last_error("the secret key's public key has no systematic form");
+        return rc;
+    }
+    const size_t bytes = cols.size() * 4;
+    if (!budget_take(eng, bytes)) {
+        set_last_error("public key does not fit the engine HBM budget");
+        return CMD_E_BUDGET;
+    }
+    void *p = nullptr;
+    if ((e = cudaMalloc(&p, bytes)) != cudaSuccess || (e = cudaMemcpy(p, cols.data(), bytes, cudaMemcpyHostToDevice)) !=
+                                                          cudaSuccess) {
+        if (p)
+            cudaFree(p);
+        budget_give(eng, bytes);
+        return cuda_fail(e, "public key upload");
+    }
+    key->pk = static_cast<uint32_t *>(p);
+    key->pk_bytes = bytes;
+    return CMD_OK;
+}
+
+int cmd_kem_decap_device(cmd_engine *eng, cmd_key *key, const uint8_t *d_cts, size_t count, uint8_t *d_keys,
+                         uint8_t *d_accept, void *stream)
+{
+    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_keys)))
+        return CMD_E_ARG;
+    if (count == 0)
+        return CMD_OK;
+    int rc = cmd_key_prepare_decap(eng, key);
+    if (rc)
+        return rc;
+    const SetInfo si = set_info(key->dev.set);
+    cudaSetDevice(eng->device);
+    std::lock_guard<std::mutex> lk(eng->mu);
+    cudaStream_t s = stream ? (cudaStream_t)stream : eng->stream;
+    const size_t words = count * si.nw;
+    if ((rc = eng->scratch.reserve(eng, words * 4 + count * 2 + 256)))
+        return rc;
+    uint32_t *d_err = static_cast<uint32_t *>(eng->scratch.ptr);
+    uint16_t *d_w = reinterpret_cast<uint16_t *>(d_err + words);
+    if ((rc = run_fused_single(eng, key, d_cts, count, d_err, d_w, s)))
+        return rc;
+    const uint8_t *d_s = key->dev.sk + 40 + 2 * si.t + si.cond;
+    cudaError_t e = launch_decap(key->dev.set, d_cts, d_err, d_w, key->pk, d_s, d_keys, d_accept, count, s,
+                                 LaunchCounter{&eng->launches});
+    return e == cudaSuccess ? CMD_OK : cuda_fail(e, "decapsulation kernel");
+}
+
+int cmd_kem_decap(cmd_engine *eng, cmd_key *key, const uint8_t *h_cts, size_t count, uint8_t *h_keys,
+                  uint8_t *h_accept)
+{
+    if (!eng || !key || key->eng != eng || (count && (!h_cts || !h_keys)))
+        return CMD_E_ARG;
+    if (count == 0)
+        return CMD_OK;
+    int rc = cmd_key_prepare_decap(eng, key);
+    if (rc)
+        return rc;
+    const SetInfo si = set_info(key->dev.set);
+    cudaSetDevice(eng->device);
+    const size_t chunk = std::min<size_t>(count, (size_t)1 << 20);
+    uint8_t *d_cts = nullptr, *d_keys = nullptr, *d_acc = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(eng->mu);
+        if ((rc = eng->io.reserve(eng, chunk * (si.ct + 32 + 1) + 1024)))
+            return rc;
+        uint8_t *base = static_cast<uint8_t *>(eng->io.ptr);
+        d_cts = base;
+        d_keys = base + (chunk * si.ct + 255) / 256 * 256;
+        d_acc = d_keys + chunk * 32;
+    }
+    cudaStream_t s = eng->stream;
+    for (size_t c0 = 0; c0 < count; c0 += chunk) {
+        const size_t n = std::min(chunk, count - c0);
+        cudaError_t e = cudaMemcpyAsync(d_cts, h_cts + c0 * si.ct, n * si.ct, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cudaMemcpyAsync(cts H2D)");
+        if ((rc = cmd_kem_decap_device(eng, key, d_cts, n, d_keys, d_acc, s)))
+            return rc;
+        e = cudaMemcpyAsync(h_keys + c0 * 32, d_keys, n * 32, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && h_accept)
+            e = cudaMemcpyAsync(h_accept + c0, d_acc, n, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "decapsulation D2H");
+    }
+    return CMD_OK;
+}
+
+}  // extern "C"

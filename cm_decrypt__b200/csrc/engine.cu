@@ -275,6 +275,10 @@ void cmd_key_free(cmd_key *key)
     cudaStreamSynchronize(key->eng->stream);
     cudaFree(key->block);
     budget_give(key->eng, key->bytes);
+    if (key->pk) {
+        cudaFree(key->pk);
+        budget_give(key->eng, key->pk_bytes);
+    }
     delete key;
 }
 

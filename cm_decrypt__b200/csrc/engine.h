@@ -96,4 +96,6 @@ struct cmd_key {
     cmd::KeyDev dev;
     void *block = nullptr;
     size_t bytes = 0;
+    uint32_t *pk = nullptr;  // decapsulation: T block of the public key, column-major
+    size_t pk_bytes = 0;
 };

@@ -256,6 +256,19 @@ int cmd_synth_pubkey(cmd_set set, const uint8_t *h_sk, cmd_pubkey **out)
 
 void cmd_synth_pubkey_free(cmd_pubkey *pk) { delete pk; }
 
+int cmd_pubkey_columns(const cmd_pubkey *pk, uint64_t *out, size_t cap_words, size_t *words_per_col)
+{
+    if (!pk || !words_per_col)
+        return CMD_E_ARG;
+    *words_per_col = (size_t)pk->xwords;
+    if (!out)
+        return CMD_OK;
+    if (cap_words < pk->xcols.size())
+        return CMD_E_ARG;
+    memcpy(out, pk->xcols.data(), pk->xcols.size() * sizeof(uint64_t));
+    return CMD_OK;
+}
+
 int cmd_synth_ciphertexts(const cmd_pubkey *pk, uint64_t seed, size_t count, uint32_t malformed_permille,
                           uint8_t *h_cts_out, uint8_t *h_err_out, uint8_t *h_valid_out, int nthreads)
 {

@@ -210,6 +210,25 @@ int cmd_positions_write(cmd_set set, const uint16_t *h_pos, size_t count,
 /* Converts a binary errorstream into the reference's errorstream text. */
 int cmd_positions_to_errorstream(const char *binary_path, const char *text_path);
 
+/* ---- KEM decapsulation (no counterpart in the reference) --------------- */
+/* The reference encapsulates only (kem/common/core/operations.c:15-34:
+ * C = [I | T] e, K = SHAKE256(1 || e || C), 32 bytes).  Decapsulation with
+ * implicit rejection: e = the decrypt of C (as cmd_decrypt_*); accept iff the
+ * padding bits of C above mt are zero, wt(e) == t and C == [I | T] e; then
+ * K = SHAKE256(b || v || C) with b = accept and v = e, or v = the secret
+ * key's n/8-byte string s when rejected.  The re-encoding check reads every
+ * column of T for every ciphertext, and v is selected with masks, so the
+ * work does not depend on e.  The first call for a key derives T from the
+ * secret key on the host (Gaussian elimination, ~0.3 s for 6960119) and
+ * keeps it on the device, charged to the engine's budget (1.1 MB for
+ * 6960119); cmd_key_prepare_decap does that step ahead of time.
+ * keys: 32 bytes per ciphertext; accept (may be NULL): 1 byte each. */
+int cmd_key_prepare_decap(cmd_engine *eng, cmd_key *key);
+int cmd_kem_decap(cmd_engine *eng, cmd_key *key, const uint8_t *h_cts, size_t count,
+                  uint8_t *h_keys, uint8_t *h_accept);
+int cmd_kem_decap_device(cmd_engine *eng, cmd_key *key, const uint8_t *d_cts, size_t count,
+                         uint8_t *d_keys, uint8_t *d_accept, void *stream);
+
 /* ---- file contract ----------------------------------------------------- */
 /* Replaces `decrypt_<set> KATNUM` (decrypt.c:109-218): reads one sk
  * (sk_bytes) and katnum ciphertexts from the given files, decrypts on the GPU
@@ -332,6 +351,11 @@ int cmd_synth_key(cmd_set set, const uint8_t *h_base_sk, uint64_t seed,
 typedef struct cmd_pubkey cmd_pubkey;
 int cmd_synth_pubkey(cmd_set set, const uint8_t *h_sk, cmd_pubkey **out);
 void cmd_synth_pubkey_free(cmd_pubkey *pk);
+/* The T block of the systematic public key [I | T]: column i (i < n - mt)
+ * in words_per_col u64 (bit r = row r, r < mt) at out + i * words_per_col.
+ * out == NULL only reports words_per_col. */
+int cmd_pubkey_columns(const cmd_pubkey *pk, uint64_t *out, size_t cap_words,
+                       size_t *words_per_col);
 /* count ciphertexts: ciphertext i is valid (an error vector of weight exactly
  * t, positions uniform over [0,n), seeded by (seed, i)) unless
  * i is drawn malformed with probability malformed_permille/1000, in which case

@@ -350,3 +350,64 @@ long o_errorstream_format(const o_params *p, const uint8_t *err_bytes,
     }
     return (long)pos;
 }
+
+/* KEM decapsulation check.  No counterpart in the reference (it encapsulates
+ * only: kem/common/core/operations.c:15-34 hashes K = SHAKE256(1 || e || C));
+ * this is the Classic McEliece decapsulation's acceptance test, stated with
+ * the reference's own syndrome: accept[c] = 1 iff the padding bits mt..sb-1
+ * of ciphertext c are zero, e_c has weight exactly t, and the 2t syndromes
+ * of e_c over all n support points (sum over set bits i of L_i^j / g(L_i)^2)
+ * equal the syndromes of the ciphertext (o_synd), i.e. the received word
+ * plus e_c is a codeword.  The session key is then SHAKE256(b || v || C),
+ * v = e (b = 1) or the sk's random string s (b = 0). */
+int o_decap_accept(const o_params *p, const uint8_t *sk, const uint8_t *cts,
+                   const uint8_t *errs, size_t count, uint8_t *accept)
+{
+    const int m = p->m, t = p->t, t2 = 2 * p->t, mt = m * t;
+    uint16_t g[130];
+    uint16_t *L = (uint16_t *)malloc((size_t)p->n * sizeof(uint16_t));
+    uint16_t *tab = (uint16_t *)malloc((size_t)p->sb * t2 * sizeof(uint16_t));
+    uint16_t *ginv2 = (uint16_t *)malloc((size_t)p->n * sizeof(uint16_t));
+    int rc = 0;
+    if (!L || !tab || !ginv2 || o_key_expand(p, sk, g, L, tab) != 0) {
+        rc = -1;
+        goto out;
+    }
+    for (int i = 0; i < p->n; i++) {
+        uint16_t v = o_eval(m, t, g, L[i]);
+        ginv2[i] = o_gf_inv(m, o_gf_mul(m, v, v));
+    }
+    for (size_t c = 0; c < count; c++) {
+        const uint8_t *ct = cts + c * (size_t)p->ct_bytes;
+        const uint8_t *e = errs + c * (size_t)(p->n / 8);
+        int ok = 1;
+        for (int b = mt; b < p->sb; b++)
+            if ((ct[b >> 3] >> (b & 7)) & 1u)
+                ok = 0;
+        uint16_t s[256], se[256];
+        o_synd(p, tab, ct, s);
+        memset(se, 0, sizeof se);
+        int w = 0;
+        for (int i = 0; i < p->n; i++) {
+            if (!((e[i >> 3] >> (i & 7)) & 1u))
+                continue;
+            w++;
+            uint16_t x = ginv2[i];
+            for (int j = 0; j < t2; j++) {
+                se[j] ^= x;
+                x = o_gf_mul(m, x, L[i]);
+            }
+        }
+        if (w != t)
+            ok = 0;
+        for (int j = 0; j < t2; j++)
+            if (s[j] != se[j])
+                ok = 0;
+        accept[c] = (uint8_t)ok;
+    }
+out:
+    free(L);
+    free(tab);
+    free(ginv2);
+    return rc;
+}

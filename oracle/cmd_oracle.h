@@ -65,6 +65,12 @@ int o_decrypt_batch(const o_params *p, const uint8_t *sk, const uint8_t *cts,
 
 /* Errorstream text (decrypt.c:55-66): " %d" per set bit, then '\n'.
  * Returns the number of bytes written, or -1 if cap is too small. */
+/* KEM decapsulation acceptance test (no counterpart in the reference; see the
+ * definition): accept[c] = padding zero && wt(e_c) == t && the 2t syndromes
+ * of e_c over all n support points equal those of ciphertext c. */
+int o_decap_accept(const o_params *p, const uint8_t *sk, const uint8_t *cts,
+                   const uint8_t *errs, size_t count, uint8_t *accept);
+
 long o_errorstream_format(const o_params *p, const uint8_t *err_bytes,
                           size_t count, char *out, size_t cap);
 

@@ -129,6 +129,28 @@ class Oracle:
             raise RuntimeError("oracle decrypt failed")
         return err
 
+    def decap(self, sk: bytes, cts: np.ndarray, nthreads: int = 1) -> tuple[np.ndarray, np.ndarray]:
+        """Classic McEliece decapsulation around the reference's decrypt (no
+        counterpart in the reference, which encapsulates only:
+        kem/common/core/operations.c:15-34, K = SHAKE256(1 || e || C)).
+        Returns (keys uint8 [count, 32], accept uint8 [count]): K =
+        SHAKE256(b || v || C), b = accept, v = e or the sk's string s."""
+        import hashlib
+        cts = np.ascontiguousarray(cts, np.uint8).reshape(-1, self.ct_bytes)
+        err = self.decrypt(sk, cts, nthreads)
+        skb = np.frombuffer(bytes(sk), np.uint8).copy()
+        acc = np.zeros(cts.shape[0], np.uint8)
+        if self.lib.o_decap_accept(ctypes.byref(self.p), _ptr(skb, _u8p), _ptr(cts, _u8p), _ptr(err, _u8p),
+                                   ctypes.c_size_t(cts.shape[0]), _ptr(acc, _u8p)):
+            raise RuntimeError("oracle decap failed")
+        s_off = 40 + 2 * self.t + (1 << (self.m - 4)) * (2 * self.m - 1)
+        s = bytes(sk)[s_off: s_off + self.n // 8]
+        keys = np.zeros((cts.shape[0], 32), np.uint8)
+        for c in range(cts.shape[0]):
+            pre = (b"\x01" + err[c].tobytes()) if acc[c] else (b"\x00" + s)
+            keys[c] = np.frombuffer(hashlib.shake_256(pre + cts[c].tobytes()).digest(32), np.uint8)
+        return keys, acc
+
     def errorstream(self, err: np.ndarray) -> bytes:
         err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n // 8)
         cap = err.shape[0] * (1 + 6 * self.n // 8 * 8) + 16

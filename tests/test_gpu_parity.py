@@ -224,6 +224,42 @@ def test_positions_output(oracle_mod, engine, keys, s):
     assert np.array_equal(d_pos.cpu().numpy().view(np.uint16), pos)
 
 
+@pytest.mark.parametrize("s", SETS)
+def test_kem_decap(oracle_mod, engine, keys, s):
+    """Decapsulation keys and accept flags equal the oracle's for valid and
+    malformed ciphertexts, the reference's kem/ ciphertexts and (6960119)
+    valid ciphertexts with a padding bit set; accepted keys are the reference
+    encapsulation's SHAKE256(1 || e || C)."""
+    import hashlib
+    info = keys[s].info
+    sk = golden_sk(s)
+    cts, planted, valid = cmd.PubKey(s, sk).ciphertexts(seed=77, count=300, malformed_permille=200)
+    kem = np.frombuffer(golden_ct(s), np.uint8).reshape(-1, info.ct_bytes)
+    allc = np.concatenate([cts, kem])
+    if 8 * info.ct_bytes > info.m * info.t:
+        padded = cts[valid == 1][:5].copy()
+        padded[:, -1] |= 0x80
+        allc = np.concatenate([allc, padded])
+    k, a = cmd.kem_decap(engine, keys[s], allc)
+    rk, ra = oracle_mod.Oracle(s).decap(sk, allc, nthreads=8)
+    assert np.array_equal(a, ra)
+    assert np.array_equal(k, rk)
+    assert a[: cts.shape[0]].sum() == valid.sum()
+    # kem/ draws error positions from m-bit values without rejecting those >= n
+    # (kem/common/core/encrypt.c:147-190): below weight t, so rejected, except
+    # for 8192128 where n = 2^m and the weight is always t
+    k0 = cts.shape[0]
+    assert (a[k0: k0 + kem.shape[0]] == (1 if info.n == 1 << info.m else 0)).all()
+    assert not a[k0 + kem.shape[0]:].any()   # padding bit set
+    for c in np.nonzero(valid)[0][:40]:
+        assert k[c].tobytes() == hashlib.shake_256(b"\x01" + planted[c].tobytes() + cts[c].tobytes()).digest(32)
+    d_ct = dev(allc)
+    d_k = torch.zeros((allc.shape[0], 32), dtype=torch.uint8, device="cuda")
+    cmd.kem_decap_device(engine, keys[s], d_ct.data_ptr(), allc.shape[0], d_k.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(d_k.cpu().numpy(), k)
+
+
 def test_binary_errorstream_files_and_cli(engine, tmp_path):
     s = 6960119
     b = str(tmp_path / "es.pos")

@@ -164,3 +164,41 @@ def test_binary_errorstream_file_roundtrip(tmp_path, oracle_mod):
     with pytest.raises(cmd.CmdError) as ei:
         cmd.positions_to_errorstream(str(junk), t)
     assert ei.value.code == cmd.CMD_E_FILE
+
+
+@pytest.mark.parametrize("s", [348864, 6960119])
+def test_pubkey_columns_reencode(s):
+    """C = [I | T] e for valid synthetic ciphertexts, with T read back through
+    cmd_pubkey_columns (the block the decapsulation kernel checks against)."""
+    info = cmd.set_info(s)
+    mt = info.m * info.t
+    pk = cmd.PubKey(s, golden_sk(s))
+    T = pk.columns()
+    assert T.shape[0] == info.n - mt
+    cts, err, valid = pk.ciphertexts(seed=8, count=6, malformed_permille=0)
+    Tb = np.unpackbits(T.view(np.uint8), axis=1, bitorder="little")[:, :mt]   # [n-mt, mt]
+    for c in range(6):
+        e = np.unpackbits(err[c], bitorder="little")
+        ct = np.unpackbits(cts[c], bitorder="little")[:mt]
+        enc = (e[:mt] + Tb[e[mt:].astype(bool)].sum(axis=0)) & 1
+        assert np.array_equal(enc, ct)
+
+
+@pytest.mark.parametrize("s", [348864, 6960119])
+def test_oracle_decap_matches_encapsulation(oracle_mod, s):
+    """The oracle's decapsulation returns the reference encapsulation's key
+    K = SHAKE256(1 || e || C) (kem/common/core/operations.c:15-34) for valid
+    ciphertexts and rejects malformed ones and the reference's own kem/
+    ciphertexts (their error vectors have weight below t)."""
+    import hashlib
+    o = oracle_mod.Oracle(s)
+    sk = golden_sk(s)
+    cts, planted, valid = cmd.PubKey(s, sk).ciphertexts(seed=12, count=24, malformed_permille=300)
+    keys, acc = o.decap(sk, cts)
+    assert np.array_equal(acc, valid)
+    for c in range(cts.shape[0]):
+        if valid[c]:
+            assert keys[c].tobytes() == hashlib.shake_256(b"\x01" + planted[c].tobytes() + cts[c].tobytes()).digest(32)
+    from conftest import golden_ct
+    _, acc2 = o.decap(sk, np.frombuffer(golden_ct(s), np.uint8).reshape(-1, o.ct_bytes))
+    assert not acc2.any()
