@@ -35,7 +35,7 @@ void HostScratch::release()
     cap = 0;
 }
 
-static int ensure_counter(cmd_engine *eng)
+int ensure_counter(cmd_engine *eng)
 {
     if (eng->tile_counter)
         return CMD_OK;
@@ -72,12 +72,13 @@ static uint32_t round_size(cmd_engine *eng, int set, int wpb, size_t count, bool
 }
 
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos)
+                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced)
 {
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
     const int wpb = eng->fcfg[set].wpb;
-    const uint32_t round = round_size(eng, set, wpb, count, eng->fcfg[set].balanced);
+    const uint32_t round =
+        round_size(eng, set, wpb, count, balanced < 0 ? eng->fcfg[set].balanced : balanced != 0);
     const uint64_t rounds = (count + round - 1) / round;
     if (rounds > 0xFFFFFFFFull)
         return CMD_E_ARG;
@@ -120,7 +121,7 @@ int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
     int rc = ensure_counter(eng);
     if (rc)
         return rc;
-    return run_fused_counter(eng, key, d_cts, count, d_err, d_weight, s, eng->tile_counter, d_pos);
+    return run_fused_counter(eng, key, d_cts, count, d_err, d_weight, s, eng->tile_counter, d_pos, -1);
 }
 
 // Set shared by every ciphertext of a mixed batch, or -1.

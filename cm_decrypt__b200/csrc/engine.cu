@@ -192,6 +192,11 @@ void cmd_engine_destroy(cmd_engine *eng)
     eng->fused.release(eng);
     eng->host_scratch.release();
     release_fft_plans(eng);
+    for (int i = 0; i < BATCH_STREAMS; i++)
+        if (eng->piece_stream[i]) {
+            cudaStreamSynchronize(eng->piece_stream[i]);
+            cudaStreamDestroy(eng->piece_stream[i]);
+        }
     if (eng->tile_counter)
         cudaFree(eng->tile_counter);
     cudaStreamDestroy(eng->stream);
@@ -455,8 +460,57 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
     uint32_t *d_err = cv.take<uint32_t>(chunk * si.nw);
     uint16_t *d_w = cv.take<uint16_t>(chunk);
     cudaStream_t s = eng->stream;
+    // Large fused batches go as BATCH_STREAMS pieces on their own streams
+    // (each with its own work counter, full rounds): one piece's copies run
+    // while the others compute, and the pieces' kernels share the SMs.
+    const bool pieces = path != CMD_PATH_PLAIN && chunk >= (size_t)BATCH_STREAMS * 8192;
+    if (pieces) {
+        if ((rc = ensure_counter(eng)))
+            return rc;
+        for (int i = 0; i < BATCH_STREAMS; i++)
+            if (!eng->piece_stream[i]) {
+                cudaError_t e = cudaStreamCreateWithFlags(&eng->piece_stream[i], cudaStreamNonBlocking);
+                if (e != cudaSuccess)
+                    return cuda_fail(e, "cudaStreamCreate(piece)");
+            }
+    }
     for (size_t c0 = 0; c0 < count; c0 += chunk) {
         const size_t n = std::min(chunk, count - c0);
+        if (pieces) {
+            // pieces of a multiple of 256 ciphertexts: whole rounds, and every
+            // piece's ciphertexts start 16-byte aligned
+            const size_t per = (n + BATCH_STREAMS * 256 - 1) / (BATCH_STREAMS * 256) * 256;
+            cudaError_t e = cudaSuccess;
+            for (int i = 0; i < BATCH_STREAMS && e == cudaSuccess && rc == CMD_OK; i++) {
+                const size_t p0 = (size_t)i * per;
+                if (p0 >= n)
+                    break;
+                const size_t pn = std::min(per, n - p0);
+                cudaStream_t ps = eng->piece_stream[i];
+                e = cudaMemcpyAsync(d_cts + p0 * si.ct, h_cts + (c0 + p0) * si.ct, pn * si.ct, cudaMemcpyHostToDevice,
+                                    ps);
+                if (e != cudaSuccess)
+                    break;
+                rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, d_err + p0 * si.nw, d_w + p0, ps,
+                                       eng->tile_counter + 1 + i, nullptr, 0);
+                if (rc)
+                    break;
+                e = cudaMemcpy2DAsync(h_err + (c0 + p0) * (si.n / 8), si.n / 8, d_err + p0 * si.nw, (size_t)si.nw * 4,
+                                      si.n / 8, pn, cudaMemcpyDeviceToHost, ps);
+                if (e == cudaSuccess && h_weight)
+                    e = cudaMemcpyAsync(h_weight + c0 + p0, d_w + p0, pn * 2, cudaMemcpyDeviceToHost, ps);
+            }
+            for (int i = 0; i < BATCH_STREAMS; i++) {
+                const cudaError_t e2 = cudaStreamSynchronize(eng->piece_stream[i]);
+                if (e == cudaSuccess)
+                    e = e2;
+            }
+            if (rc)
+                return rc;
+            if (e != cudaSuccess)
+                return cuda_fail(e, "decrypt batch pieces");
+            continue;
+        }
         cudaError_t e = cudaMemcpyAsync(d_cts, h_cts + c0 * si.ct, n * si.ct, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess)
             return cuda_fail(e, "cudaMemcpyAsync(cts H2D)");
@@ -507,8 +561,50 @@ int cmd_decrypt_positions(cmd_engine *eng, const cmd_key *key, const uint8_t *h_
     uint8_t *d_cts = cv.take<uint8_t>(chunk * si.ct);
     uint16_t *d_pos = cv.take<uint16_t>(chunk * row);
     cudaStream_t s = eng->stream;
+    const bool pieces = chunk >= (size_t)BATCH_STREAMS * 8192;
+    if (pieces) {
+        if ((rc = ensure_counter(eng)))
+            return rc;
+        for (int i = 0; i < BATCH_STREAMS; i++)
+            if (!eng->piece_stream[i]) {
+                cudaError_t e = cudaStreamCreateWithFlags(&eng->piece_stream[i], cudaStreamNonBlocking);
+                if (e != cudaSuccess)
+                    return cuda_fail(e, "cudaStreamCreate(piece)");
+            }
+    }
     for (size_t c0 = 0; c0 < count; c0 += chunk) {
         const size_t n = std::min(chunk, count - c0);
+        if (pieces) {  // as in cmd_decrypt_batch
+            const size_t per = (n + BATCH_STREAMS * 256 - 1) / (BATCH_STREAMS * 256) * 256;
+            cudaError_t e = cudaSuccess;
+            for (int i = 0; i < BATCH_STREAMS && e == cudaSuccess && rc == CMD_OK; i++) {
+                const size_t p0 = (size_t)i * per;
+                if (p0 >= n)
+                    break;
+                const size_t pn = std::min(per, n - p0);
+                cudaStream_t ps = eng->piece_stream[i];
+                e = cudaMemcpyAsync(d_cts + p0 * si.ct, h_cts + (c0 + p0) * si.ct, pn * si.ct, cudaMemcpyHostToDevice,
+                                    ps);
+                if (e != cudaSuccess)
+                    break;
+                rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, nullptr, nullptr, ps,
+                                       eng->tile_counter + 1 + i, d_pos + p0 * row, 0);
+                if (rc)
+                    break;
+                e = cudaMemcpyAsync(h_pos + (c0 + p0) * row, d_pos + p0 * row, pn * row * 2, cudaMemcpyDeviceToHost,
+                                    ps);
+            }
+            for (int i = 0; i < BATCH_STREAMS; i++) {
+                const cudaError_t e2 = cudaStreamSynchronize(eng->piece_stream[i]);
+                if (e == cudaSuccess)
+                    e = e2;
+            }
+            if (rc)
+                return rc;
+            if (e != cudaSuccess)
+                return cuda_fail(e, "decrypt positions pieces");
+            continue;
+        }
         cudaError_t e = cudaMemcpyAsync(d_cts, h_cts + c0 * si.ct, n * si.ct, cudaMemcpyHostToDevice, s);
         if (e != cudaSuccess)
             return cuda_fail(e, "cudaMemcpyAsync(cts H2D)");

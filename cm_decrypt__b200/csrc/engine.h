@@ -48,6 +48,12 @@ int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t
                uint32_t *d_err, uint16_t *d_weight, cudaStream_t s);
 int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                      uint16_t *d_weight, cudaStream_t s, uint16_t *d_pos = nullptr);
+// Explicit work counter and round schedule (balanced: -1 = the tuned choice,
+// 0 = full rounds, 1 = equal shares).
+int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced);
+int ensure_counter(cmd_engine *eng);  // eng->tile_counter: 64 u32 work counters
+constexpr int BATCH_STREAMS = 8;      // pieces of a host-buffer batch in flight
 size_t fused_smem(int set, int wpb);
 size_t smem_limit_bytes();
 int fused_blocks_per_sm(int single_set, int wpb, size_t smem);
@@ -75,6 +81,7 @@ struct cmd_engine {
     cmd::Scratch fused;            // fused-kernel work lists
     cmd::HostScratch host_scratch; // pinned staging
     uint32_t *tile_counter = nullptr;
+    cudaStream_t piece_stream[cmd::BATCH_STREAMS] = {};  // host-buffer batches, created on first use
     std::atomic<uint64_t> launches{0};
     cmd::FusedConfig fcfg[cmd::NSETS];
     cmd::FusedConfig fcfg_mixed;

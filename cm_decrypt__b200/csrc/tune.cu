@@ -24,8 +24,6 @@
 
 namespace cmd {
 
-int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos);
 size_t plain_scratch_bytes(int set, size_t count);
 cudaError_t fused_prepare(cmd_engine *eng, int set);
 
@@ -201,7 +199,7 @@ int cmd_tune(cmd_engine *eng, const cmd_key *key, size_t sample_count, int force
             bool ok = true;
             for (int rep = 0; rep < 4 && ok; rep++) {
                 cudaEventRecord(e0, s);
-                ok = run_fused_counter(eng, key, d_cts, sample_count, d_err, nullptr, s, eng->tile_counter, nullptr) == 0;
+                ok = run_fused_counter(eng, key, d_cts, sample_count, d_err, nullptr, s, eng->tile_counter, nullptr, -1) == 0;
                 cudaEventRecord(e1, s);
                 if (cudaEventSynchronize(e1) != cudaSuccess)
                     ok = false;
@@ -274,7 +272,7 @@ int cmd_graph_capture(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
         if (path == CMD_PATH_PLAIN)
             rc = run_device(eng, key, path, d_cts, count, d_err, d_weight, cs);
         else
-            rc = run_fused_counter(eng, key, d_cts, count, d_err, d_weight, cs, g->counter, nullptr);
+            rc = run_fused_counter(eng, key, d_cts, count, d_err, d_weight, cs, g->counter, nullptr, -1);
         cudaGraph_t graph = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(cs, &graph);
         if (rc == CMD_OK && e2 != cudaSuccess)

@@ -201,6 +201,28 @@ def test_full_size_properties(engine, keys, path):
     assert (w == 119).all()
 
 
+def test_host_batch_in_pieces(oracle_mod, engine, keys):
+    """A ragged host-buffer batch large enough to be split over the engine's
+    piece streams (four concurrent fused launches with their own counters)
+    equals the one-launch device path row for row."""
+    s = 460896
+    pk = cmd.PubKey(s, golden_sk(s))
+    count = 4 * 8192 * 3 + 17
+    cts, planted, valid = pk.ciphertexts(seed=5, count=count, malformed_permille=100)
+    err, w = cmd.decrypt(engine, keys[s], cts, path="fused")
+    assert np.array_equal(err[valid == 1], planted[valid == 1])
+    info = keys[s].info
+    d_ct = dev(cts)
+    d_err = torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda")
+    d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+    cmd.decrypt_device(engine, keys[s], d_ct.data_ptr(), count, d_err.data_ptr(), d_w.data_ptr(), 0, "fused")
+    torch.cuda.synchronize()
+    assert np.array_equal(words_to_bytes(d_err, info.n), err)
+    assert np.array_equal(d_w.cpu().numpy().view(np.uint16), w)
+    bad = np.nonzero(valid == 0)[0][:64]
+    assert np.array_equal(err[bad], oracle_mod.Oracle(s).decrypt(golden_sk(s), cts[bad], nthreads=8))
+
+
 @pytest.mark.parametrize("s", SETS)
 def test_positions_output(oracle_mod, engine, keys, s):
     """cmd_decrypt_positions rows equal the positions of the packed error
