@@ -142,7 +142,7 @@ SERVE_SETS = (348864, 460896, 6688128, 6960119, 8192128)
 SERVE_WEIGHTS = (30, 15, 20, 20, 15)
 
 
-SERVER_CONFIG = {"max_batch": 8192, "slots": 6, "max_wait_us": 150, "fused_threshold": 0}
+SERVER_CONFIG = {"max_batch": 8192, "slots": 8, "max_wait_us": 150, "fused_threshold": 0}
 
 
 def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: int = 16384,
@@ -566,7 +566,7 @@ def main() -> None:
         g_.close()
     if world == 1 and not args.no_serve:
         fused_rate = value
-        rates = sorted({1e4, 1e5, 5e5, 1e6, min(2e6, 0.5 * fused_rate), min(2e6, 0.7 * fused_rate), 2e6})
+        rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, round(0.5 * fused_rate, -5)})
         line["serving"] = serving_leg(cmd, eng, args.serve_keys, rates, args.serve_seconds)
         line["serving"]["fused_batch_decaps_per_s"] = fused_rate
         best = line["serving"]["max_decaps_per_s_p99_under_1ms"]

@@ -26,6 +26,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <iterator>
 #include <mutex>
 #include <random>
 #include <thread>
@@ -73,7 +74,7 @@ struct Slot {
     std::vector<uint32_t> slot_of;      // request i -> result row (item slot)
     size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
-    std::vector<Request> reqs;
+    std::deque<Request> reqs;  // swapped in from the queue (O(1) when a batch takes it all)
     std::vector<uint32_t> pinned;  // key ids pinned by this batch
     bool fused = false;
 };
@@ -204,7 +205,7 @@ int cmd_server::launch(Slot &sl)
         for (uint32_t k : ready)
             keys[k].pins++;
         if (ready.size() < kid.size()) {
-            std::vector<Request> keep, defer;
+            std::deque<Request> keep, defer;
             for (const Request &r : sl.reqs)
                 (std::find(ready.begin(), ready.end(), r.key_id) != ready.end() ? keep : defer).push_back(r);
             pending.insert(pending.begin(), defer.begin(), defer.end());
@@ -361,8 +362,13 @@ void cmd_server::dispatch_loop()
         free_slots.pop_front();
         Slot &sl = slots[si];
         const size_t take = std::min<size_t>(pending.size(), cfg.max_batch);
-        sl.reqs.assign(pending.begin(), pending.begin() + take);
-        pending.erase(pending.begin(), pending.begin() + take);
+        sl.reqs.clear();
+        if (take == pending.size()) {
+            sl.reqs.swap(pending);  // the common case: no copy under the lock
+        } else {
+            sl.reqs.assign(std::make_move_iterator(pending.begin()), std::make_move_iterator(pending.begin() + take));
+            pending.erase(pending.begin(), pending.begin() + take);
+        }
         lk.unlock();
         int rc = launch(sl);
         lk.lock();
@@ -412,10 +418,33 @@ void cmd_server::complete_loop()
         cv_complete.wait(lk, [&] { return !inflight.empty() || dispatch_exited; });
         if (inflight.empty())
             break;
-        const int si = inflight.front();
+        // Whichever batch in flight finishes first: batches of different
+        // sizes complete out of order, and a small one must not wait behind
+        // a large one.  With one batch in flight, block on its event.
+        int si = -1;
+        cudaError_t e = cudaSuccess;
+        while (si < 0) {
+            std::vector<int> snap(inflight.begin(), inflight.end());
+            lk.unlock();
+            if (snap.size() == 1) {
+                si = snap[0];
+                e = cudaEventSynchronize(slots[si].done);
+            } else {
+                for (int x : snap) {
+                    const cudaError_t q = cudaEventQuery(slots[x].done);
+                    if (q != cudaErrorNotReady) {
+                        si = x;
+                        e = q;
+                        break;
+                    }
+                }
+                if (si < 0)
+                    std::this_thread::yield();
+            }
+            lk.lock();
+        }
         lk.unlock();
         Slot &sl = slots[si];
-        const cudaError_t e = cudaEventSynchronize(sl.done);
         const uint64_t t = now_ns();
         float gpu_ms = 0;
         if (e == cudaSuccess)
@@ -451,7 +480,7 @@ void cmd_server::complete_loop()
             keys[k].pins--;
         sl.pinned.clear();
         sl.reqs.clear();
-        inflight.pop_front();
+        inflight.erase(std::find(inflight.begin(), inflight.end(), si));
         free_slots.push_back(si);
         completions_gen++;
         cv_dispatch.notify_one();
@@ -582,6 +611,7 @@ int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uin
     r.key_id = key_id;
     r.tag = tag;
     r.err_out = h_err_out;
+    bool wake = false;
     {
         std::lock_guard<std::mutex> lk(srv->mu);
         if (key_id >= srv->keys.size())
@@ -599,8 +629,13 @@ int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uin
         if (srv->submitted++ == 0)
             srv->t_first = r.t_arrive;
         srv->pending.push_back(r);
+        // The dispatcher waits for a first request or for a full batch: only
+        // those two transitions need a wake-up (not every submission).
+        const size_t np = srv->pending.size();
+        wake = np == 1 || np == srv->cfg.max_batch;
     }
-    srv->cv_dispatch.notify_one();
+    if (wake)
+        srv->cv_dispatch.notify_one();
     return CMD_OK;
 }
 
