@@ -206,6 +206,28 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
     return out
 
 
+def rank_seed(rank: int) -> int:
+    """Seed of a replica's workload: every rank decrypts its own batch."""
+    return 1000 + rank
+
+
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's figure: a multi-GPU step takes as long as its slowest
+    replica (NCCL on the GPUs; any backend the process group runs)."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job throughput: the units all replicas processed / the slowest time."""
+    return world * units_per_rank / seconds
+
+
 def _time_stream(fn, stream, reps: int, warmup: int) -> float:
     """ms per call of fn(), CUDA events on `stream` after `warmup` untimed calls."""
     import torch
@@ -372,7 +394,7 @@ def main() -> None:
     key = cmd.Key(eng, SET, sk)
     info = key.info
     pk = cmd.PubKey(SET, sk)
-    cts, planted, valid = pk.ciphertexts(seed=1000 + rank, count=count)
+    cts, planted, valid = pk.ciphertexts(seed=rank_seed(rank), count=count)
 
     # Rotating device buffer sets, together larger than 2x L2, so no step
     # reads inputs or writes outputs the previous step left in L2.
@@ -432,16 +454,13 @@ def main() -> None:
         launches = eng.launch_count() - l0
         for b in range(min(nbuf, steps)):
             check(b)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, world)
         return ms, launches, clk.summary()
 
     if args.kernel_only:
         ms, launches, _ = timed("fused", args.steps, args.warmup)
         if rank == 0:
-            print(json.dumps({"kernel_only": True, "decaps_per_s": world * count * args.steps / (ms * 1e-3),
+            print(json.dumps({"kernel_only": True, "decaps_per_s": job_rate(world, count * args.steps, ms * 1e-3),
                               "ms_per_step": ms / args.steps, "gpu_launches": launches}), flush=True)
         return
     int_peak = eng.int_peak()
@@ -468,11 +487,7 @@ def main() -> None:
         cmd.decrypt_into(eng, key, h_cts, h_err, h_w, path="fused")
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
 
     # The same through cmd_decrypt_positions (binary wire format: t+1 u16 per
     # ciphertext come back instead of n/8 bytes).
@@ -490,11 +505,7 @@ def main() -> None:
     for _ in range(args.steps):
         pos_call()
     torch.cuda.synchronize()
-    pos_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([pos_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        pos_s = float(t.item())
+    pos_s = max_over_ranks(time.perf_counter() - t0, world)
     pos_ok = bool(np.array_equal(h_pos[:512], cmd.positions_from_errors(SET, planted[:512])))
 
     # KEM decapsulation on the same device-resident batches: decrypt, the
@@ -504,9 +515,10 @@ def main() -> None:
     cmd.prepare_decap(eng, key)
     dec_ms = _time_stream(lambda: cmd.kem_decap_device(eng, key, d_cts[0].data_ptr(), count, d_keys.data_ptr(),
                                                        d_acc.data_ptr(), sp), stream, max(1, args.steps // 2), 2)
+    dec_ms = max_over_ranks(dec_ms, world)
     dec_ok = bool(d_acc.cpu().numpy().all())
 
-    value = world * count * args.steps / (ms * 1e-3)
+    value = job_rate(world, count * args.steps, ms * 1e-3)
     per_rank = count * args.steps / (ms * 1e-3)
     w = work_per_decap(SET)
     achieved = per_rank * w["total"]
@@ -530,16 +542,16 @@ def main() -> None:
                    "l2": f"rotating {nbuf} resident buffer sets ({nbuf * per_set / 2**20:.0f} MiB > 2x L2)"},
         "gpu_launches": launches,
         "plain": None if ms_plain is None else {
-            "value": world * count * min(args.steps, 3) / (ms_plain * 1e-3),
+            "value": job_rate(world, count * min(args.steps, 3), ms_plain * 1e-3),
             "ms_per_step": ms_plain / max(1, min(args.steps, 3)),
             "fused_speedup": (ms_plain / max(1, min(args.steps, 3))) / (ms / args.steps)},
-        "e2e": {"value": world * count * args.steps / e2e_s, "unit": "decaps/s",
+        "e2e": {"value": job_rate(world, count * args.steps, e2e_s), "unit": "decaps/s",
                 "h2d_bytes_per_step": count * info.ct_bytes,
                 "d2h_bytes_per_step": count * (info.err_bytes + 2)},
-        "kem_decap": {"value": world * count / (dec_ms * 1e-3), "unit": "decaps/s", "ms_per_batch": dec_ms,
+        "kem_decap": {"value": job_rate(world, count, dec_ms * 1e-3), "unit": "decaps/s", "ms_per_batch": dec_ms,
                       "call": "cmd_kem_decap_device (decrypt + re-encoding check + SHAKE256 keys), device buffers",
                       "all_valid_accepted": dec_ok},
-        "e2e_positions": {"value": world * count * args.steps / pos_s, "unit": "decaps/s",
+        "e2e_positions": {"value": job_rate(world, count * args.steps, pos_s), "unit": "decaps/s",
                           "call": "cmd_decrypt_positions (error positions, binary errorstream rows)",
                           "h2d_bytes_per_step": count * info.ct_bytes,
                           "d2h_bytes_per_step": count * (info.t + 1) * 2, "results_match_planted": pos_ok},
