@@ -320,14 +320,8 @@ cudaError_t launch_decap(int set, const uint8_t *d_cts, const uint32_t *d_err, c
         return cudaSuccess;
     DecapArgs a{d_cts, d_err, d_w, d_pk, d_s, d_keys, d_accept, count};
     return dispatch_set(set, [&]<int S>() -> cudaError_t {
-        const size_t smem = 2 * (size_t)COLS * DecapDims<S>::CWP * 4;
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(k_decap<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess)
-                return e;
-            attr = true;
-        }
+        const size_t smem = 2 * (size_t)COLS * DecapDims<S>::CWP * 4;  // <= 13.3 KB: no opt-in needed
+        static_assert(2 * COLS * DecapDims<S>::CWP * 4 <= 48 * 1024, "decap staging");
         k_decap<S><<<(unsigned)((count + 255) / 256), 256, smem, s>>>(a);
         lc.bump();
         return cudaGetLastError();

@@ -372,7 +372,10 @@ size_t smem_limit_bytes();
 // so the attribute is set to what a launch needs, not to the device limit).
 template <int SETMASK, int WPB> cudaError_t ensure_smem_attr(size_t smem)
 {
-    static size_t set_to = 0;
+    static size_t given[64] = {};  // per device: the attribute is a per-device setting
+    int dev = 0;
+    cudaGetDevice(&dev);
+    size_t &set_to = given[dev & 63];
     if (smem <= set_to)
         return cudaSuccess;
     cudaError_t e =

@@ -377,16 +377,20 @@ cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t
 {
     if (ntiles == 0)
         return cudaSuccess;
-    static size_t attr = 0;
+    // the opt-in is per device: remember what each device has been given
+    static size_t attr[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    size_t &set_to = attr[dev & 63];
     const size_t smem = tile_smem_bytes();
     const size_t root_smem = ROOT_WARPS * ROOT_FA_WORDS * 4;
-    if (attr < smem) {
+    if (set_to < smem) {
         cudaError_t e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)root_smem);
         if (e != cudaSuccess)
             return e;
-        attr = smem;
+        set_to = smem;
     }
     const LatItem *items = static_cast<const LatItem *>(d_items);
     uint32_t *d_loc_bs = d_scratch;
