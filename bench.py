@@ -200,7 +200,9 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
                                   "refused": st["refused"], "results_match_planted": ok,
                                   "gpu_batch_p50_ms": st["gpu_p50_us"] / 1e3,
                                   "gpu_batch_p99_ms": st["gpu_p99_us"] / 1e3,
-                                  "wait_p50_ms": st["wait_p50_us"] / 1e3, "wait_p99_ms": st["wait_p99_us"] / 1e3})
+                                  "wait_p50_ms": st["wait_p50_us"] / 1e3, "wait_p99_ms": st["wait_p99_us"] / 1e3,
+                                  "dispatch_busy": st["dispatch_busy"], "complete_busy": st["complete_busy"],
+                                  "mean_inflight": st["mean_inflight"]})
     under = [p for p in out["points"] if p["p99_ms"] < 1.0]
     out["max_decaps_per_s_p99_under_1ms"] = max((p["decaps_per_s"] for p in under), default=None)
     return out

@@ -73,7 +73,8 @@ class ServerStats(ctypes.Structure):
                 ("submitted", "completed", "refused", "batches", "fused_batches", "resident_keys")] + \
                [(n, ctypes.c_double) for n in
                 ("mean_batch", "p50_us", "p99_us", "max_us", "mean_us", "decaps_per_s", "offered_per_s",
-                 "gpu_p50_us", "gpu_p99_us", "wait_p50_us", "wait_p99_us")]
+                 "gpu_p50_us", "gpu_p99_us", "wait_p50_us", "wait_p99_us", "dispatch_busy", "complete_busy",
+                 "mean_inflight")]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}

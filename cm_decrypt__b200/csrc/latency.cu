@@ -64,15 +64,18 @@ __device__ __forceinline__ void tile_synd(const LatItem &it, const uint8_t *cts,
     const bool live = 4 * lane < TWP;
     const uint4 *tab = reinterpret_cast<const uint4 *>(it.tab) + lane;
     uint4 acc = make_uint4(0, 0, 0, 0);
+    // Rows whose ciphertext bit is clear are skipped (the bit is the same for
+    // the whole warp, so the branch does not diverge): about half the table
+    // is read.  The ciphertext is public, so which rows are read reveals
+    // nothing about the key or the error vector.
 #pragma unroll 8
     for (int b = b0 + warp; b < b1; b += 8) {
-        const uint32_t m = 0u - ((ct[b >> 3] >> (b & 7)) & 1u);
-        if (live) {
+        if (live && ((ct[b >> 3] >> (b & 7)) & 1u)) {
             const uint4 x = __ldg(tab + (size_t)b * (TWP / 4));
-            acc.x ^= x.x & m;
-            acc.y ^= x.y & m;
-            acc.z ^= x.z & m;
-            acc.w ^= x.w & m;
+            acc.x ^= x.x;
+            acc.y ^= x.y;
+            acc.z ^= x.z;
+            acc.w ^= x.w;
         }
     }
     if (live)
@@ -117,7 +120,9 @@ template <int S> struct TileSmem {
 };
 
 // Threads of k_tile_bm: two roles of up to five warps each (t+1 <= 129
-// coefficients per role).
+// coefficients per role).  The kernel is bounded to 96 registers a thread
+// so that two tiles share an SM: one tile keeps an SM's ALUs about half busy
+// (its steps are a chain of dependent multiplies and barriers).
 constexpr int TILE_THREADS = 320;
 
 template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32_t *synp, uint32_t *loc_bs,
@@ -304,7 +309,7 @@ template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32
     }
 }
 
-__global__ void __launch_bounds__(TILE_THREADS) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
+__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
                                                  uint32_t *__restrict__ loc_bs, FftPlans plans)
 {
     extern __shared__ __align__(16) uint8_t smem_tile[];
@@ -388,6 +393,15 @@ cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t
         cudaError_t e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)root_smem);
+        // One shared-memory split for all three kernels, so that CTAs of
+        // concurrent batches' kernels can share an SM without it draining to
+        // change its split (two k_tile_bm or two k_root_tile CTAs per SM).
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_synd, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         if (e != cudaSuccess)
             return e;
         set_to = smem;

@@ -16,21 +16,29 @@
 //  * Small batches run the latency kernels of latency.cu (any mix of keys and
 //    sets in three launches, a short pass per ciphertext); batches of
 //    fused_threshold or more run the fused kernel (highest throughput).
-//  * A completer thread waits for slots in dispatch order, copies each
-//    result to its request's buffer and records arrival-to-completion
-//    latency for the p50/p99 statistics.
+//  * A completer thread polls the batches in flight without the queue lock,
+//    takes whichever finishes first, copies each result to its request's
+//    buffer (large batches split across a few copy threads) and records
+//    arrival-to-completion latency for the p50/p99 statistics.
+//  * Host work per request is O(1): the queue is a vector whose buffers
+//    circulate between the queue and the slots (no allocation per request),
+//    keys get a batch-local index by generation stamp, and requests are
+//    grouped by set and key with a counting sort.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <functional>
 #include <iterator>
+#include <memory>
 #include <mutex>
 #include <random>
+#include <shared_mutex>
 #include <thread>
-#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -49,10 +57,50 @@ static uint64_t now_ns()
 
 struct Request {
     uint32_t key_id;
+    int32_t set;  // the key's set, fixed when the request is queued
     uint64_t tag;
     uint8_t *err_out;
     uint64_t t_arrive;
     uint8_t ct[CT_STRIDE];
+};
+
+// FIFO of requests in a vector with a head index.  Whole-queue takes swap
+// buffers with the taking slot, so buffers circulate and steady-state
+// submission allocates nothing.
+struct RequestQueue {
+    std::vector<Request> v;
+    size_t head = 0;
+    size_t size() const { return v.size() - head; }
+    bool empty() const { return head == v.size(); }
+    const Request &front() const { return v[head]; }
+    void push_back(const Request &r) { v.push_back(r); }
+    // Moves the oldest `take` requests into out (whose old contents are dropped).
+    void take_front(size_t take, std::vector<Request> &out)
+    {
+        out.clear();
+        if (head == 0 && take == v.size()) {
+            out.swap(v);
+            return;
+        }
+        out.assign(v.begin() + head, v.begin() + head + take);
+        head += take;
+        if (head == v.size()) {
+            v.clear();
+            head = 0;
+        }
+    }
+    // Puts requests back at the front, oldest first.
+    template <class It>
+    void push_front(It b, It e)
+    {
+        const size_t n = (size_t)std::distance(b, e);
+        if (head >= n) {
+            head -= n;
+            std::copy(b, e, v.begin() + head);
+        } else {
+            v.insert(v.begin() + head, b, e);
+        }
+    }
 };
 
 struct KeyEntry {
@@ -61,6 +109,83 @@ struct KeyEntry {
     cmd_key *key = nullptr;
     uint64_t last_use = 0;
     int pins = 0;
+    uint64_t batch_gen = 0;  // dispatcher only: generation of the batch that last indexed this key
+    uint32_t batch_idx = 0;  // index within that batch's key table
+};
+
+// A few threads that split one batch's result copies with the completer.
+class CopyPool {
+public:
+    explicit CopyPool(int helpers)
+    {
+        for (int i = 0; i < helpers; i++)
+            th_.emplace_back([this] { loop(); });
+    }
+    ~CopyPool()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto &t : th_)
+            t.join();
+    }
+    // Runs fn(c) for every c in [0, chunks) on the helpers and the calling
+    // thread; returns when all chunks are done.
+    void run(size_t chunks, const std::function<void(size_t)> &fn)
+    {
+        if (chunks <= 1 || th_.empty()) {
+            for (size_t c = 0; c < chunks; c++)
+                fn(c);
+            return;
+        }
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &fn;
+            chunks_ = chunks;
+            next_.store(0);
+            active_ = th_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_done_.wait(lk, [&] { return active_ == 0; });
+        job_ = nullptr;
+    }
+
+private:
+    void work()
+    {
+        size_t c;
+        while ((c = next_.fetch_add(1)) < chunks_)
+            (*job_)(c);
+    }
+    void loop()
+    {
+        uint64_t seen = 0;
+        std::unique_lock<std::mutex> lk(mu_);
+        while (true) {
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_)
+                return;
+            seen = gen_;
+            lk.unlock();
+            work();
+            lk.lock();
+            if (--active_ == 0)
+                cv_done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_, cv_done_;
+    const std::function<void(size_t)> *job_ = nullptr;
+    size_t chunks_ = 0, active_ = 0;
+    std::atomic<size_t> next_{0};
+    uint64_t gen_ = 0;
+    bool stop_ = false;
 };
 
 struct Slot {
@@ -74,9 +199,12 @@ struct Slot {
     std::vector<uint32_t> slot_of;      // request i -> result row (item slot)
     size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
-    std::deque<Request> reqs;  // swapped in from the queue (O(1) when a batch takes it all)
+    std::vector<Request> reqs;  // taken from the queue (a buffer swap when a batch takes it all)
     std::vector<uint32_t> pinned;  // key ids pinned by this batch
     bool fused = false;
+    // completer scratch, reused batch to batch
+    std::vector<uint32_t> lats, waits;
+    std::vector<cmd_completion> comps;
 };
 
 }  // namespace cmd
@@ -87,23 +215,31 @@ struct cmd_server {
     cmd_engine *eng = nullptr;
     cmd_server_config cfg{};
     size_t in_bytes = 0, device_bytes = 0;
+    // Lock order: keys_mu before mu.  keys_mu guards the key table's shape
+    // (add_key appends under both locks); the dispatcher reads entries under
+    // a shared hold, the completer and submitters under mu.
+    std::shared_mutex keys_mu;
     std::mutex mu;
     std::condition_variable cv_dispatch, cv_complete, cv_poll;
-    std::deque<Request> pending;
+    RequestQueue pending;
     std::deque<KeyEntry> keys;   // deque: entries keep their address as keys are added
     std::vector<Slot> slots;
-    std::deque<int> free_slots, inflight;
+    std::deque<int> free_slots;
+    std::atomic<uint32_t> inflight{0};  // bit s: slot s has a batch on the GPU (set under mu)
     std::deque<cmd_completion> completions;
     std::thread dispatcher, completer;
+    std::unique_ptr<CopyPool> copiers;
     bool stop = false;
     bool dispatch_exited = false;
     int status = CMD_OK;
+    uint64_t batch_gen = 0;  // dispatcher only
     // statistics
     std::vector<uint32_t> lat_ns;
     std::vector<uint32_t> gpu_ns;   // per batch
     std::vector<uint32_t> wait_ns;  // per request: arrival -> launch
     uint64_t submitted = 0, completed = 0, refused = 0, batches = 0, fused_batches = 0, batched_cts = 0;
     uint64_t t_first = 0, t_last = 0;
+    uint64_t dispatch_ns = 0, complete_ns = 0, inflight_sum = 0;  // host time in launch / result handling
     uint64_t tick = 0;
     uint64_t completions_gen = 0;  // bumped each time a batch completes
 
@@ -173,8 +309,12 @@ int cmd_server::ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys)
         }
         if (victim < 0)
             return held ? CMD_E_BUSY : CMD_E_BUDGET;  // BUSY: retry once a batch completes
-        cmd_key_free(keys[victim].key);
-        keys[victim].key = nullptr;
+        cmd_key *gone = keys[victim].key;
+        {
+            std::lock_guard<std::mutex> lk(mu);  // stats read residency under mu
+            keys[victim].key = nullptr;
+        }
+        cmd_key_free(gone);
     }
 }
 
@@ -184,12 +324,15 @@ int cmd_server::launch(Slot &sl)
     // them at once, the requests of the keys that did not fit go back to the
     // front of the queue for the next batch (only a batch whose first key
     // cannot be made resident fails).
+    std::shared_lock<std::shared_mutex> key_hold(keys_mu);
     std::vector<uint32_t> kid;
-    {
-        std::unordered_map<uint32_t, int> seen;
-        for (const Request &r : sl.reqs)
-            if (seen.emplace(r.key_id, 1).second)
-                kid.push_back(r.key_id);
+    uint64_t gen = ++batch_gen;
+    for (const Request &r : sl.reqs) {
+        KeyEntry &ke = keys[r.key_id];
+        if (ke.batch_gen != gen) {
+            ke.batch_gen = gen;
+            kid.push_back(r.key_id);
+        }
     }
     std::vector<uint32_t> ready;
     for (uint32_t k : kid) {
@@ -205,23 +348,28 @@ int cmd_server::launch(Slot &sl)
         for (uint32_t k : ready)
             keys[k].pins++;
         if (ready.size() < kid.size()) {
-            std::deque<Request> keep, defer;
+            gen = ++batch_gen;  // re-stamp: only the ready keys stay in this batch
+            for (uint32_t k : ready)
+                keys[k].batch_gen = gen;
+            std::vector<Request> keep, defer;
             for (const Request &r : sl.reqs)
-                (std::find(ready.begin(), ready.end(), r.key_id) != ready.end() ? keep : defer).push_back(r);
-            pending.insert(pending.begin(), defer.begin(), defer.end());
+                (keys[r.key_id].batch_gen == gen ? keep : defer).push_back(r);
+            pending.push_front(defer.begin(), defer.end());
             sl.reqs.swap(keep);
         }
     }
     sl.pinned = ready;
+    // Key table in set order, so that grouping requests by key index also
+    // groups them by set.
     kid = ready;
+    std::stable_sort(kid.begin(), kid.end(), [&](uint32_t a, uint32_t b) { return keys[a].set < keys[b].set; });
+    for (size_t k = 0; k < kid.size(); k++)
+        keys[kid[k]].batch_idx = (uint32_t)k;
     const size_t B = sl.reqs.size();
     InLayout lay(B, B);
-    std::unordered_map<uint32_t, uint32_t> local;
-    for (size_t k = 0; k < kid.size(); k++)
-        local.emplace(kid[k], (uint32_t)k);
     uint32_t *key_idx = reinterpret_cast<uint32_t *>(sl.h_in + lay.key_idx);
     for (size_t i = 0; i < B; i++) {
-        key_idx[i] = local[sl.reqs[i].key_id];
+        key_idx[i] = keys[sl.reqs[i].key_id].batch_idx;
         memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
     }
     FusedKeyRef *krefs = reinterpret_cast<FusedKeyRef *>(sl.h_in + lay.keys);
@@ -243,15 +391,16 @@ int cmd_server::launch(Slot &sl)
         // Tile path: requests grouped by set into tiles of up to 32 (any keys
         // within a tile); item slot 32*t + q is request q of tile t.
         LatItem *items = reinterpret_cast<LatItem *>(sl.h_in + lay.items);
-        std::vector<uint32_t> by_set(B);
+        // by set, then by key (counting sort on the set-ordered key index):
+        // requests of one key sit side by side, so their syndrome CTAs read
+        // the same table rows close together in time
+        std::vector<uint32_t> by_set(B), start(kid.size() + 1, 0);
         for (size_t i = 0; i < B; i++)
-            by_set[i] = (uint32_t)i;
-        // by set, then by key: requests of one key sit side by side, so their
-        // syndrome CTAs read the same table rows close together in time
-        std::stable_sort(by_set.begin(), by_set.end(), [&](uint32_t a, uint32_t b) {
-            const int sa = kset[key_idx[a]], sb = kset[key_idx[b]];
-            return sa != sb ? sa < sb : key_idx[a] < key_idx[b];
-        });
+            start[key_idx[i] + 1]++;
+        for (size_t k = 0; k < kid.size(); k++)
+            start[k + 1] += start[k];
+        for (size_t i = 0; i < B; i++)
+            by_set[start[key_idx[i]]++] = (uint32_t)i;
         uint32_t ntiles = 0;
         size_t i = 0;
         while (i < B) {
@@ -347,12 +496,12 @@ void cmd_server::dispatch_loop()
             continue;
         // Continuous batching: with batches already on the GPU, give the
         // oldest waiting request up to max_wait_us to collect batch-mates.
-        if (!inflight.empty() && pending.size() < cfg.max_batch && !stop) {
+        if (inflight.load() && pending.size() < cfg.max_batch && !stop) {
             const uint64_t deadline = pending.front().t_arrive + (uint64_t)cfg.max_wait_us * 1000;
             const uint64_t t = now_ns();
             if (t < deadline) {
                 cv_dispatch.wait_for(lk, std::chrono::nanoseconds(deadline - t), [&] {
-                    return stop || pending.size() >= cfg.max_batch || inflight.empty();
+                    return stop || pending.size() >= cfg.max_batch || !inflight.load();
                 });
                 if (pending.empty() || free_slots.empty())
                     continue;
@@ -361,25 +510,21 @@ void cmd_server::dispatch_loop()
         const int si = free_slots.front();
         free_slots.pop_front();
         Slot &sl = slots[si];
-        const size_t take = std::min<size_t>(pending.size(), cfg.max_batch);
-        sl.reqs.clear();
-        if (take == pending.size()) {
-            sl.reqs.swap(pending);  // the common case: no copy under the lock
-        } else {
-            sl.reqs.assign(std::make_move_iterator(pending.begin()), std::make_move_iterator(pending.begin() + take));
-            pending.erase(pending.begin(), pending.begin() + take);
-        }
+        pending.take_front(std::min<size_t>(pending.size(), cfg.max_batch), sl.reqs);
         lk.unlock();
+        const uint64_t t0 = now_ns();
         int rc = launch(sl);
+        const uint64_t t1 = now_ns();
         lk.lock();
+        dispatch_ns += t1 - t0;
         if (rc == CMD_E_BUSY) {
             // Every key that could be evicted is in use by a batch in flight:
             // requeue the batch and wait for a completion before retrying.
-            pending.insert(pending.begin(), sl.reqs.begin(), sl.reqs.end());
+            pending.push_front(sl.reqs.begin(), sl.reqs.end());
             sl.reqs.clear();
             free_slots.push_front(si);
             const uint64_t gen = completions_gen;
-            cv_dispatch.wait(lk, [&] { return stop || completions_gen != gen || inflight.empty(); });
+            cv_dispatch.wait(lk, [&] { return stop || completions_gen != gen || !inflight.load(); });
             continue;
         }
         if (rc != CMD_OK) {
@@ -403,7 +548,8 @@ void cmd_server::dispatch_loop()
         batches++;
         fused_batches += sl.fused ? 1 : 0;
         batched_cts += sl.reqs.size();
-        inflight.push_back(si);
+        inflight.fetch_or(1u << si);
+        inflight_sum += __builtin_popcount(inflight.load());
         cv_complete.notify_one();
     }
     dispatch_exited = true;
@@ -413,74 +559,87 @@ void cmd_server::dispatch_loop()
 void cmd_server::complete_loop()
 {
     cudaSetDevice(eng->device);
-    std::unique_lock<std::mutex> lk(mu);
     while (true) {
-        cv_complete.wait(lk, [&] { return !inflight.empty() || dispatch_exited; });
-        if (inflight.empty())
-            break;
+        uint32_t mask = inflight.load();
+        if (!mask) {
+            std::unique_lock<std::mutex> lk(mu);
+            cv_complete.wait(lk, [&] { return inflight.load() != 0 || dispatch_exited; });
+            if (!inflight.load())
+                break;  // the dispatcher has exited and every batch is done
+            continue;
+        }
         // Whichever batch in flight finishes first: batches of different
         // sizes complete out of order, and a small one must not wait behind
-        // a large one.  With one batch in flight, block on its event.
+        // a large one.  With one batch in flight, block on its event.  The
+        // in-flight set is read without the queue lock, so polling does not
+        // slow submitters down.
         int si = -1;
         cudaError_t e = cudaSuccess;
-        while (si < 0) {
-            std::vector<int> snap(inflight.begin(), inflight.end());
-            lk.unlock();
-            if (snap.size() == 1) {
-                si = snap[0];
-                e = cudaEventSynchronize(slots[si].done);
-            } else {
-                for (int x : snap) {
-                    const cudaError_t q = cudaEventQuery(slots[x].done);
-                    if (q != cudaErrorNotReady) {
-                        si = x;
-                        e = q;
-                        break;
-                    }
+        if (__builtin_popcount(mask) == 1) {
+            si = __builtin_ctz(mask);
+            e = cudaEventSynchronize(slots[si].done);
+        } else {
+            for (uint32_t m = mask; m; m &= m - 1) {
+                const int x = __builtin_ctz(m);
+                const cudaError_t q = cudaEventQuery(slots[x].done);
+                if (q != cudaErrorNotReady) {
+                    si = x;
+                    e = q;
+                    break;
                 }
-                if (si < 0)
-                    std::this_thread::yield();
             }
-            lk.lock();
+            if (si < 0) {
+                std::this_thread::yield();
+                continue;
+            }
         }
-        lk.unlock();
         Slot &sl = slots[si];
         const uint64_t t = now_ns();
         float gpu_ms = 0;
         if (e == cudaSuccess)
             cudaEventElapsedTime(&gpu_ms, sl.start, sl.done);
-        std::vector<uint32_t> lats, waits;
-        lats.reserve(sl.reqs.size());
-        waits.reserve(sl.reqs.size());
-        std::vector<cmd_completion> done;
-        for (size_t i = 0; i < sl.reqs.size(); i++) {
-            const Request &r = sl.reqs[i];
-            const SetInfo info = set_info(keys[r.key_id].set);
-            if (e == cudaSuccess && r.err_out)
-                memcpy(r.err_out, sl.h_err + (size_t)sl.slot_of[i] * ERR_STRIDE, info.n / 8);
-            const uint64_t lat = t - r.t_arrive;
-            lats.push_back((uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu));
-            waits.push_back((uint32_t)std::min<uint64_t>(sl.t_launch - r.t_arrive, 0xFFFFFFFFu));
-            if (cfg.record_completions)
-                done.push_back(
-                    cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[sl.slot_of[i]], 0, lat});
-        }
-        lk.lock();
+        const size_t B = sl.reqs.size();
+        sl.lats.resize(B);
+        sl.waits.resize(B);
+        if (cfg.record_completions)
+            sl.comps.resize(B);
+        // Results to the requests' buffers, in chunks across the copy threads
+        // for large batches.
+        constexpr size_t CHUNK = 256;
+        const size_t chunks = (B + CHUNK - 1) / CHUNK;
+        copiers->run(chunks, [&](size_t c) {
+            const size_t end = std::min(B, (c + 1) * CHUNK);
+            for (size_t i = c * CHUNK; i < end; i++) {
+                const Request &r = sl.reqs[i];
+                if (e == cudaSuccess && r.err_out)
+                    memcpy(r.err_out, sl.h_err + (size_t)sl.slot_of[i] * ERR_STRIDE, set_info(r.set).n / 8);
+                const uint64_t lat = t - r.t_arrive;
+                sl.lats[i] = (uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu);
+                sl.waits[i] = (uint32_t)std::min<uint64_t>(sl.t_launch - r.t_arrive, 0xFFFFFFFFu);
+                if (cfg.record_completions)
+                    sl.comps[i] =
+                        cmd_completion{r.tag, e == cudaSuccess ? CMD_OK : CMD_E_CUDA, sl.h_w[sl.slot_of[i]], 0, lat};
+            }
+        });
+        const uint64_t t_done = now_ns();
+        std::lock_guard<std::mutex> lk(mu);
         if (e != cudaSuccess && status == CMD_OK) {
             status = CMD_E_CUDA;
             set_last_error(std::string("server batch: ") + cudaGetErrorString(e));
         }
-        completions.insert(completions.end(), done.begin(), done.end());
-        lat_ns.insert(lat_ns.end(), lats.begin(), lats.end());
-        wait_ns.insert(wait_ns.end(), waits.begin(), waits.end());
+        if (cfg.record_completions)
+            completions.insert(completions.end(), sl.comps.begin(), sl.comps.end());
+        lat_ns.insert(lat_ns.end(), sl.lats.begin(), sl.lats.end());
+        wait_ns.insert(wait_ns.end(), sl.waits.begin(), sl.waits.end());
         gpu_ns.push_back((uint32_t)(gpu_ms * 1e6f));
-        completed += sl.reqs.size();
+        completed += B;
         t_last = t;
+        complete_ns += t_done - t;
         for (uint32_t k : sl.pinned)
             keys[k].pins--;
         sl.pinned.clear();
         sl.reqs.clear();
-        inflight.erase(std::find(inflight.begin(), inflight.end(), si));
+        inflight.fetch_and(~(1u << si));
         free_slots.push_back(si);
         completions_gen++;
         cv_dispatch.notify_one();
@@ -544,6 +703,10 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
     for (int i = 0; i < (int)cfg->slots; i++)
         srv->free_slots.push_back(i);
     srv->dispatcher = std::thread([srv] { srv->dispatch_loop(); });
+    // up to three copy helpers beside the completer, leaving cores to the
+    // submitters and the dispatcher
+    const unsigned hc = std::thread::hardware_concurrency();
+    srv->copiers.reset(new CopyPool((int)std::min(3u, hc > 4 ? (hc - 4) / 2 : 0u)));
     srv->completer = std::thread([srv] { srv->complete_loop(); });
     *out = srv;
     return CMD_OK;
@@ -594,6 +757,7 @@ int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t
 {
     if (!srv || !h_sk || !key_id || !valid_set(set) || sk_len != (size_t)set_info(set).sk)
         return CMD_E_ARG;
+    std::unique_lock<std::shared_mutex> key_hold(srv->keys_mu);
     std::lock_guard<std::mutex> lk(srv->mu);
     KeyEntry ke;
     ke.set = set;
@@ -622,7 +786,8 @@ int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uin
             srv->refused++;
             return CMD_E_BUSY;
         }
-        const int ctb = set_info(srv->keys[key_id].set).ct;
+        r.set = srv->keys[key_id].set;
+        const int ctb = set_info(r.set).ct;
         memcpy(r.ct, h_ct, ctb);
         memset(r.ct + ctb, 0, CT_STRIDE - ctb);
         r.t_arrive = now_ns();
@@ -709,8 +874,13 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
             sum += x;
         st->mean_us = sum / v.size() / 1e3;
     }
-    if (srv->t_last > srv->t_first)
-        st->decaps_per_s = srv->completed / ((srv->t_last - srv->t_first) * 1e-9);
+    if (srv->t_last > srv->t_first) {
+        const double span = (double)(srv->t_last - srv->t_first);
+        st->decaps_per_s = srv->completed / (span * 1e-9);
+        st->dispatch_busy = srv->dispatch_ns / span;
+        st->complete_busy = srv->complete_ns / span;
+    }
+    st->mean_inflight = srv->batches ? (double)srv->inflight_sum / srv->batches : 0;
     if (reset) {
         srv->lat_ns.clear();
         srv->gpu_ns.clear();
@@ -719,6 +889,7 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
         srv->completed = 0;
         srv->refused = srv->batches = srv->fused_batches = srv->batched_cts = 0;
         srv->t_first = srv->t_last = 0;
+        srv->dispatch_ns = srv->complete_ns = srv->inflight_sum = 0;
     }
     return CMD_OK;
 }

@@ -283,6 +283,9 @@ typedef struct {
     double gpu_p50_us, gpu_p99_us; /* per batch: device time from the input copy
                                       to the end of the result copy          */
     double wait_p50_us, wait_p99_us; /* per request: arrival -> batch launch  */
+    double dispatch_busy;  /* host time forming and launching batches / interval */
+    double complete_busy;  /* host time delivering results / interval          */
+    double mean_inflight;  /* batches on the GPU when a batch is launched (incl.) */
 } cmd_server_stats;
 
 int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server **out);
