@@ -120,6 +120,8 @@ def lib() -> ctypes.CDLL:
         "cmd_errorstream_write": (_i32, [_i32, _vp, _sz, ctypes.c_char_p, _i32]),
         "cmd_key_prepare_decap": (_i32, [_vp, _vp]),
         "cmd_kem_decap": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_kem_keypair": (_i32, [_vp, _i32, _vp, _vp, _vp, _vp]),
+        "cmd_kem_keypair_batch": (_i32, [_vp, _i32, _vp, _sz, _vp, _vp, _vp, ctypes.c_uint32]),
         "cmd_kem_decap_device": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),
         "cmd_pubkey_columns": (_i32, [_vp, _vp, _sz, ctypes.POINTER(_sz)]),
         "cmd_decrypt_positions": (_i32, [_vp, _vp, _vp, _sz, _vp]),
@@ -453,6 +455,43 @@ def decrypt_files(engine: Engine, set_id: int, sk_path: str, ct_path: str, katnu
 
 
 # ---- KEM decapsulation --------------------------------------------------------
+def pk_bytes(set_id: int) -> int:
+    """Public-key bytes: mt rows of (n - mt + 7)/8 bytes (pk_gen.c:145-146)."""
+    info = set_info(set_id)
+    mt = info.m * info.t
+    return mt * ((info.n - mt + 7) // 8)
+
+
+def kem_keypair(engine: Engine, set_id: int, seed: bytes) -> tuple[bytes, bytes, int]:
+    """crypto_kem_keypair with randombytes() yielding `seed` (32 bytes), on
+    the GPU.  Returns (pk, sk, attempts)."""
+    seed = bytes(seed)
+    if len(seed) != 32:
+        raise ValueError("seed must be 32 bytes")
+    info = set_info(set_id)
+    pk = np.zeros(pk_bytes(set_id), np.uint8)
+    sk = np.zeros(info.sk_bytes, np.uint8)
+    att = ctypes.c_uint32()
+    sb = np.frombuffer(seed, np.uint8).copy()
+    _check(lib().cmd_kem_keypair(engine.handle, set_index(set_id), _ptr(sb), _ptr(pk), _ptr(sk), ctypes.byref(att)),
+           "cmd_kem_keypair")
+    return pk.tobytes(), sk.tobytes(), att.value
+
+
+def kem_keypair_batch(engine: Engine, set_id: int, seeds: np.ndarray,
+                      max_attempts: int = 0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Key pairs for a batch of 32-byte seeds: (pk uint8 [count, pk_bytes],
+    sk uint8 [count, sk_bytes], attempts uint32 [count])."""
+    sd = np.ascontiguousarray(seeds, np.uint8).reshape(-1, 32)
+    info = set_info(set_id)
+    pk = np.zeros((sd.shape[0], pk_bytes(set_id)), np.uint8)
+    sk = np.zeros((sd.shape[0], info.sk_bytes), np.uint8)
+    att = np.zeros(sd.shape[0], np.uint32)
+    _check(lib().cmd_kem_keypair_batch(engine.handle, set_index(set_id), _ptr(sd), sd.shape[0], _ptr(pk), _ptr(sk),
+                                       _ptr(att), max_attempts), "cmd_kem_keypair_batch")
+    return pk, sk, att
+
+
 def prepare_decap(engine: Engine, key: Key) -> None:
     """Derives the key's public key (host) and keeps it on the device."""
     _check(lib().cmd_key_prepare_decap(engine.handle, key.handle), "cmd_key_prepare_decap")

@@ -1,0 +1,1017 @@
+// On-device Classic McEliece key generation: crypto_kem_keypair of the
+// reference's kem/ tree (kem/common/core/operations.c:36-107) for a batch of
+// seeds, every stage on the GPU.  One attempt per pending key and round:
+//
+//  1. k_kg_expand     SHAKE256(64 || seed) -> r = s | perm | f | next seed
+//                     (one thread per key; Keccak-f[1600] in registers)
+//  2. k_kg_genpoly    minimal polynomial g of f in GF((2^m)^t): the powers
+//                     f^0..f^t, then Gauss-Jordan over GF(2^m) (sk_gen.c:24-85)
+//  3. k_kg_support    pi = indices ordered by their random words (bitonic
+//                     sort of (word << 31 | index) in shared memory, rejected
+//                     on equal words), L = bitrev(pi), 1/g(L), and the mt x n
+//                     parity-check matrix, 32 columns per warp by ballots
+//                     (pk_gen.c:52-113)
+//  4. elimination     blocked Gauss-Jordan on the first mt columns, 32 pivot
+//                     columns per panel: k_ge_panel finds the pivot rows and
+//                     the 32 x 32 transform on the panel words alone,
+//                     k_ge_pivots forms the reduced pivot rows, k_ge_apply
+//                     clears the panel columns of every other row.  The
+//                     result is the unique reduced form [I | T] that
+//                     pk_gen.c:115-143 reaches (rejected when a pivot is
+//                     missing, i.e. the left block is singular)
+//  5. k_kg_controlbits Benes control bits of pi by the cycle-labelling
+//                     recursion (controlbits.c:22-170), all sub-networks of a
+//                     level at once over segmented bitonic sorts, then checked
+//                     by running the network (controlbits.c:180-220)
+//  6. k_kg_output     pk rows (bytes mt/8 .. of each reduced row,
+//                     pk_gen.c:145-146) and sk = seed | pivots | g | control
+//                     bits | s (operations.c:60-100)
+//
+// A rejected attempt continues with the next seed from r, exactly as the
+// reference's loop does, so a seed yields the reference's key pair.
+//
+// Not constant-time: the GF(2^m) arithmetic uses log/antilog tables in shared
+// memory and the elimination reads the pivot rows it selects, so kernel timing
+// depends on secret values.  The sorts and the control-bit recursion have
+// data-independent access patterns.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "engine.h"
+#include "keccak.cuh"
+
+namespace cmd {
+namespace {
+
+constexpr int KG_MAX_Q = 1 << 13;
+constexpr int PANEL = 32;
+
+enum KgStatus : int { KG_OK = 0, KG_GENPOLY = 1, KG_PERM = 2, KG_SINGULAR = 3, KG_CBITS = 4 };
+
+// Runtime sizes of one set's key generation and the per-key workspace.
+struct KgDims {
+    int set, m, n, t, q, mt, rlen, rw, pk_row, cond, sk;
+    size_t off_r, off_irr, off_pi, off_cond, off_panel, off_pv, off_mv, off_mat, stride;
+};
+
+struct PanelInfo {
+    int status;         // KgStatus of this key's attempt
+    int npiv, nmove;    // pivots in the current panel; rows moved out of its window
+    int pad;
+    uint32_t src[PANEL];   // pivot b comes from (pre-panel) row src[b]
+    uint32_t T[PANEL];     // pivot b = XOR over bits j of T[b] of row src[j]
+    uint32_t from[PANEL];  // non-pivot rows inside the window ...
+    uint32_t to[PANEL];    // ... and the vacated pivot rows they move to
+};
+
+KgDims kg_dims(int set)
+{
+    const SetInfo si = set_info(set);
+    KgDims d;
+    d.set = set;
+    d.m = si.m;
+    d.n = si.n;
+    d.t = si.t;
+    d.q = 1 << si.m;
+    d.mt = si.m * si.t;
+    d.rlen = si.n / 8 + 4 * d.q + 2 * si.t + 32;
+    d.rw = ((si.n + 31) / 32 + 3) / 4 * 4;  // row words, 16-byte rows
+    d.pk_row = (si.n - d.mt + 7) / 8;
+    d.cond = si.cond;
+    d.sk = si.sk;
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    size_t o = 0;
+    d.off_r = o;
+    o = al(o + d.rlen);
+    d.off_irr = o;
+    o = al(o + 2 * (size_t)d.t);
+    d.off_pi = o;
+    o = al(o + 2 * (size_t)d.q);
+    d.off_cond = o;
+    o = al(o + d.cond);
+    d.off_panel = o;
+    o = al(o + sizeof(PanelInfo));
+    d.off_pv = o;
+    o = al(o + (size_t)PANEL * d.rw * 4);
+    d.off_mv = o;
+    o = al(o + (size_t)PANEL * d.rw * 4);
+    d.off_mat = o;
+    o = al(o + (size_t)d.mt * d.rw * 4);
+    d.stride = o;
+    return d;
+}
+
+// ---- GF(2^m) by log/antilog tables (built on the host) --------------------
+struct GfTables {
+    uint16_t lg[KG_MAX_Q];  // lg[0] unused
+    uint16_t ex[KG_MAX_Q];  // ex[i] = gen^i, i < 2^m - 1
+};
+
+__device__ __forceinline__ uint16_t gmul(const uint16_t *lg, const uint16_t *ex, int q1, uint32_t a, uint32_t b)
+{
+    if (!a || !b)
+        return 0;
+    int s = lg[a] + lg[b];
+    s = s >= q1 ? s - q1 : s;
+    return ex[s];
+}
+__device__ __forceinline__ uint16_t ginv(const uint16_t *lg, const uint16_t *ex, int q1, uint32_t a)
+{
+    return a ? ex[lg[a] ? q1 - lg[a] : 0] : 0;
+}
+__device__ __forceinline__ uint32_t bitrev_m(uint32_t v, int m) { return __brev(v) >> (32 - m); }
+
+// Copies both tables to shared memory.
+__device__ void load_tables(const GfTables *g, uint16_t *lg, uint16_t *ex, int q)
+{
+    const uint32_t *s1 = reinterpret_cast<const uint32_t *>(g->lg), *s2 = reinterpret_cast<const uint32_t *>(g->ex);
+    uint32_t *d1 = reinterpret_cast<uint32_t *>(lg), *d2 = reinterpret_cast<uint32_t *>(ex);
+    for (int i = threadIdx.x; i < q / 2; i += blockDim.x) {
+        d1[i] = s1[i];
+        d2[i] = s2[i];
+    }
+}
+
+// ---- 1. seed expansion ----------------------------------------------------
+__global__ void k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work, KgDims d, int K)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= K)
+        return;
+    const uint8_t *sd = seeds + (size_t)k * 32;
+    uint8_t *r = work + (size_t)k * d.stride + d.off_r;
+    reinterpret_cast<PanelInfo *>(work + (size_t)k * d.stride + d.off_panel)->status = KG_OK;
+    // absorb 64 || seed (33 bytes) in one block with the SHAKE padding
+    uint64_t A[25];
+#pragma unroll
+    for (int i = 0; i < 25; i++)
+        A[i] = 0;
+    uint8_t blk[40];
+    blk[0] = 64;
+    for (int i = 0; i < 32; i++)
+        blk[1 + i] = sd[i];
+    blk[33] = 0x1F;
+    for (int i = 34; i < 40; i++)
+        blk[i] = 0;
+#pragma unroll
+    for (int l = 0; l < 5; l++) {
+        uint64_t v = 0;
+#pragma unroll
+        for (int b = 0; b < 8; b++)
+            v |= (uint64_t)blk[8 * l + b] << (8 * b);
+        A[l] = v;
+    }
+    A[16] ^= 0x8000000000000000ull;  // last byte of the 136-byte block
+    constexpr int RATE = 136;
+#pragma unroll 1
+    for (int off = 0; off < d.rlen; off += RATE) {
+        keccak_f(A);
+        const int len = min(RATE, d.rlen - off);
+#pragma unroll
+        for (int l = 0; l < RATE / 8; l++) {
+            const uint64_t v = A[l];
+            if (8 * l + 8 <= len) {
+#pragma unroll
+                for (int b = 0; b < 8; b++)
+                    r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
+            } else if (8 * l < len) {
+                for (int b = 0; b < len - 8 * l; b++)
+                    r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
+            }
+        }
+    }
+}
+
+// ---- 2. Goppa polynomial --------------------------------------------------
+// Terms of F(y) = y^t + sum c_u y^off_u defining GF((2^m)^t)
+// (kem/variant_<set>/gf.c GF_mul).
+struct ExtPoly {
+    int nt, off[4];
+    uint16_t c[4];
+};
+__host__ __device__ inline ExtPoly ext_poly(int set)
+{
+    switch (set) {
+    case S348864: return {3, {3, 1, 0, 0}, {1, 1, 2, 0}};        // y^64 + y^3 + y + z
+    case S460896: return {4, {10, 9, 6, 0}, {1, 1, 1, 1}};       // y^96 + y^10 + y^9 + y^6 + 1
+    case S6960119: return {2, {8, 0, 0, 0}, {1, 1, 0, 0}};       // y^119 + y^8 + 1
+    default: return {4, {7, 2, 1, 0}, {1, 1, 1, 1}};             // y^128 + y^7 + y^2 + y + 1
+    }
+}
+
+constexpr int GP_THREADS = 256;
+
+// Shared memory: tables, the t x (t+1) system (row = coordinate, column =
+// power), the current power, the product, the column of multipliers.
+size_t genpoly_smem(const KgDims &d)
+{
+    return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 3 * 256 * 2 + 256 * 2 + 64;
+}
+
+__global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__ work, const GfTables *__restrict__ tabs,
+                                                           KgDims d)
+{
+    extern __shared__ __align__(16) uint8_t sm_gp[];
+    uint16_t *lg = reinterpret_cast<uint16_t *>(sm_gp);
+    uint16_t *ex = lg + KG_MAX_Q;
+    uint16_t *A = ex + KG_MAX_Q;                 // [t][t+1]
+    uint16_t *pw = A + (size_t)d.t * (d.t + 1);  // 256
+    uint16_t *pr = pw + 256;                     // product, 2t - 1 <= 255
+    uint16_t *v1 = pr + 256;                     // first fold, t + 10
+    uint16_t *col = v1 + 256;                    // multipliers
+    __shared__ int s_piv;
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
+    const int tid = threadIdx.x, t = d.t, q1 = d.q - 1, W = t + 1;
+    load_tables(tabs, lg, ex, d.q);
+    const uint8_t *fr = wk + d.off_r + d.rlen - 32 - 2 * t;
+    if (tid < t) {
+        col[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);  // f (col is free until the elimination)
+        pw[tid] = tid == 0 ? 1 : 0;
+    }
+    __syncthreads();
+    const ExtPoly F = ext_poly(d.set);
+    int offmax = 0;
+    for (int u = 0; u < F.nt; u++)
+        offmax = max(offmax, F.off[u]);
+    // powers f^0 .. f^t into the columns of A
+    for (int c = 0; c <= t; c++) {
+        if (tid < t)
+            A[tid * W + c] = pw[tid];
+        if (c == t)
+            break;
+        // pr = pw * f (degree <= 2t - 2)
+        if (tid < 2 * t - 1) {
+            uint16_t acc = 0;
+            const int lo = max(0, tid - t + 1), hi = min(tid, t - 1);
+            for (int i = lo; i <= hi; i++)
+                acc ^= gmul(lg, ex, q1, pw[i], col[tid - i]);
+            pr[tid] = acc;
+        }
+        __syncthreads();
+        // fold y^(t+i) = sum_u c_u y^(i+off_u): twice, the second for the at
+        // most offmax coefficients the first pushes to degree >= t
+        if (tid < t + offmax) {
+            uint16_t acc = tid < t ? pr[tid] : 0;
+            for (int u = 0; u < F.nt; u++) {
+                const int i = tid - F.off[u];
+                if (i >= 0 && i <= t - 2)
+                    acc ^= F.c[u] == 1 ? pr[t + i] : gmul(lg, ex, q1, pr[t + i], F.c[u]);
+            }
+            v1[tid] = acc;
+        }
+        __syncthreads();
+        if (tid < t) {
+            uint16_t acc = v1[tid];
+            for (int u = 0; u < F.nt; u++) {
+                const int i = tid - F.off[u];
+                if (i >= 0 && i < offmax)
+                    acc ^= F.c[u] == 1 ? v1[t + i] : gmul(lg, ex, q1, v1[t + i], F.c[u]);
+            }
+            pw[tid] = acc;
+        }
+        __syncthreads();
+    }
+    __syncthreads();
+    // Gauss-Jordan: sum_{j<t} g_j f^j = f^t
+    for (int c = 0; c < t; c++) {
+        if (tid == 0)
+            s_piv = t;
+        __syncthreads();
+        for (int r = c + tid; r < t; r += GP_THREADS)
+            if (A[r * W + c])
+                atomicMin(&s_piv, r);
+        __syncthreads();
+        const int piv = s_piv;
+        if (piv >= t) {
+            if (tid == 0)
+                pinfo->status = KG_GENPOLY;
+            return;
+        }
+        if (piv != c)
+            for (int x = c + tid; x <= t; x += GP_THREADS) {
+                const uint16_t a = A[piv * W + x];
+                A[piv * W + x] = A[c * W + x];
+                A[c * W + x] = a;
+            }
+        __syncthreads();
+        const uint16_t inv = ginv(lg, ex, q1, A[c * W + c]);
+        __syncthreads();
+        for (int x = c + tid; x <= t; x += GP_THREADS)
+            A[c * W + x] = gmul(lg, ex, q1, A[c * W + x], inv);
+        for (int r = tid; r < t; r += GP_THREADS)
+            col[r] = r == c ? 0 : A[r * W + c];
+        __syncthreads();
+        const int width = t + 1 - c;
+        for (int e = tid; e < t * width; e += GP_THREADS) {
+            const int r = e / width, x = c + e % width;
+            const uint16_t k = col[r];
+            if (k)
+                A[r * W + x] ^= gmul(lg, ex, q1, A[c * W + x], k);
+        }
+        __syncthreads();
+    }
+    uint16_t *irr = reinterpret_cast<uint16_t *>(wk + d.off_irr);
+    if (tid < t)
+        irr[tid] = A[tid * W + t];
+}
+
+// ---- bitonic sorts in shared memory ----------------------------------------
+// Ascending sort of each aligned segment of 2^seg_log elements of x[0, n)
+// (n a power of two): the compare-exchange pattern depends on indices only.
+template <class T>
+__device__ void seg_sort(T *x, int n, int seg_log)
+{
+    const int seg = 1 << seg_log;
+    for (int k = 2; k <= seg; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            __syncthreads();
+            for (int p = threadIdx.x; p < n / 2; p += blockDim.x) {
+                const int i = 2 * p - (p & (j - 1)), l = i + j;
+                const bool asc = k == seg || !(i & k);
+                const T a = x[i], b = x[l];
+                const T lo = a < b ? a : b, hi = a < b ? b : a;
+                x[i] = asc ? lo : hi;
+                x[l] = asc ? hi : lo;
+            }
+        }
+    }
+    __syncthreads();
+}
+
+// ---- 3. support, 1/g(L) and the parity-check matrix ------------------------
+constexpr int SUP_THREADS = 1024;
+
+size_t support_smem(const KgDims &d) { return sizeof(GfTables) + (size_t)d.q * 8 + 256 * 2 + 16; }
+
+__global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict__ work, const GfTables *__restrict__ tabs,
+                                                            KgDims d)
+{
+    extern __shared__ __align__(16) uint8_t sm_sup[];
+    uint64_t *buf = reinterpret_cast<uint64_t *>(sm_sup);
+    uint16_t *lg = reinterpret_cast<uint16_t *>(buf + d.q);
+    uint16_t *ex = lg + KG_MAX_Q;
+    uint16_t *g = ex + KG_MAX_Q;
+    __shared__ int s_dup;
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
+    if (pinfo->status != KG_OK)
+        return;
+    const int tid = threadIdx.x, q = d.q, q1 = q - 1, t = d.t, m = d.m, n = d.n;
+    load_tables(tabs, lg, ex, q);
+    const uint8_t *pm = wk + d.off_r + d.n / 8;  // the 2^m random words
+    for (int i = tid; i < q; i += SUP_THREADS) {
+        const uint32_t w = pm[4 * i] | (pm[4 * i + 1] << 8) | (pm[4 * i + 2] << 16) | ((uint32_t)pm[4 * i + 3] << 24);
+        buf[i] = ((uint64_t)w << 31) | (uint64_t)i;
+    }
+    const uint16_t *irr = reinterpret_cast<const uint16_t *>(wk + d.off_irr);
+    for (int i = tid; i <= t; i += SUP_THREADS)
+        g[i] = i < t ? irr[i] : 1;
+    if (tid == 0)
+        s_dup = 0;
+    seg_sort(buf, q, m);
+    for (int i = 1 + tid; i < q; i += SUP_THREADS)
+        if ((buf[i - 1] >> 31) == (buf[i] >> 31))
+            s_dup = 1;
+    __syncthreads();
+    if (s_dup) {
+        if (tid == 0)
+            pinfo->status = KG_PERM;
+        return;
+    }
+    int16_t *pi = reinterpret_cast<int16_t *>(wk + d.off_pi);
+    for (int i = tid; i < q; i += SUP_THREADS)
+        pi[i] = (int16_t)(buf[i] & (uint64_t)q1);
+    // Row j*m + k, column i: bit k of L_i^j / g(L_i); warp w owns 32-column
+    // groups w, w + 32, ...; lane k < m stores row j*m + k of its group.
+    uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
+    const int warp = tid >> 5, lane = tid & 31, groups = (n + 31) / 32;
+    for (int grp = warp; grp < groups; grp += SUP_THREADS / 32) {
+        const int i = 32 * grp + lane;
+        uint32_t L = 0, v = 0;
+        if (i < n) {
+            L = bitrev_m((uint32_t)(buf[i] & (uint64_t)q1), m);
+            uint32_t e = g[t];
+            for (int j = t - 1; j >= 0; j--)
+                e = gmul(lg, ex, q1, e, L) ^ g[j];
+            v = ginv(lg, ex, q1, e);
+        }
+        for (int j = 0; j < t; j++) {
+            uint32_t mine = 0;
+#pragma unroll
+            for (int k = 0; k < 13; k++) {
+                if (k < m) {
+                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (v >> k) & 1u);
+                    if (lane == k)
+                        mine = bal;
+                }
+            }
+            if (lane < m)
+                mat[(size_t)(j * m + lane) * d.rw + grp] = mine;
+            v = gmul(lg, ex, q1, v, L);
+        }
+    }
+    for (int e = tid; e < d.mt * (d.rw - groups); e += SUP_THREADS) {
+        const int r = e / (d.rw - groups), w = groups + e % (d.rw - groups);
+        mat[(size_t)r * d.rw + w] = 0;
+    }
+}
+
+// ---- 4. elimination ---------------------------------------------------------
+constexpr int PANEL_THREADS = 1024;
+constexpr int MAX_MT = 13 * 128;
+
+// Pivot rows and transform of panel p (columns 32p .. 32p + npiv - 1) from
+// the panel words of rows >= 32p: Gauss-Jordan on those words, tracking for
+// every row which selected rows it has absorbed.
+__global__ void __launch_bounds__(PANEL_THREADS) k_ge_panel(uint8_t *__restrict__ work, KgDims d, int p)
+{
+    __shared__ uint32_t P[MAX_MT], tag[MAX_MT];
+    __shared__ uint8_t sel[MAX_MT];
+    __shared__ int s_piv;
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    PanelInfo *pi = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
+    if (pi->status != KG_OK)
+        return;
+    const uint32_t *mat = reinterpret_cast<const uint32_t *>(wk + d.off_mat);
+    const int tid = threadIdx.x, c0 = PANEL * p, rows = d.mt - c0, npiv = min(PANEL, d.mt - c0);
+    for (int r = tid; r < rows; r += PANEL_THREADS) {
+        P[r] = mat[(size_t)(c0 + r) * d.rw + p];
+        tag[r] = 0;
+        sel[r] = 0;
+    }
+    for (int b = 0; b < npiv; b++) {
+        if (tid == 0)
+            s_piv = rows;
+        __syncthreads();
+        for (int r = tid; r < rows; r += PANEL_THREADS)
+            if (!sel[r] && ((P[r] >> b) & 1u))
+                atomicMin(&s_piv, r);
+        __syncthreads();
+        const int sr = s_piv;
+        if (sr >= rows) {
+            if (tid == 0)
+                pi->status = KG_SINGULAR;
+            return;
+        }
+        if (tid == 0) {
+            sel[sr] = 1;
+            tag[sr] |= 1u << b;
+            pi->src[b] = (uint32_t)(c0 + sr);
+        }
+        __syncthreads();
+        const uint32_t ps = P[sr], ts = tag[sr];
+        __syncthreads();
+        for (int r = tid; r < rows; r += PANEL_THREADS)
+            if (r != sr && ((P[r] >> b) & 1u)) {
+                P[r] ^= ps;
+                tag[r] ^= ts;
+            }
+        __syncthreads();
+    }
+    if (tid < npiv)
+        pi->T[tid] = tag[pi->src[tid] - c0];
+    if (tid == 0) {
+        // rows of the window [c0, c0 + npiv) that are not pivots move to the
+        // pivot rows outside it (both lists ascending)
+        int na = 0, nb = 0;
+        for (int r = 0; r < npiv; r++)
+            if (!sel[r])
+                pi->from[na++] = (uint32_t)(c0 + r);
+        for (int b = 0; b < npiv; b++)
+            if ((int)pi->src[b] >= c0 + npiv)
+                pi->to[nb++] = pi->src[b];
+        // pivot rows are found in row order only per column: sort `to`
+        for (int x = 1; x < nb; x++)
+            for (int y = x; y > 0 && pi->to[y - 1] > pi->to[y]; y--) {
+                const uint32_t tmp = pi->to[y];
+                pi->to[y] = pi->to[y - 1];
+                pi->to[y - 1] = tmp;
+            }
+        pi->npiv = npiv;
+        pi->nmove = na;
+    }
+}
+
+// Reduced pivot rows PV[b] and copies MV[i] of the rows that move, words p..
+__global__ void k_ge_pivots(uint8_t *__restrict__ work, KgDims d, int p)
+{
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    const PanelInfo *pi = reinterpret_cast<const PanelInfo *>(wk + d.off_panel);
+    if (pi->status != KG_OK)
+        return;
+    const uint32_t *mat = reinterpret_cast<const uint32_t *>(wk + d.off_mat);
+    uint32_t *pv = reinterpret_cast<uint32_t *>(wk + d.off_pv), *mv = reinterpret_cast<uint32_t *>(wk + d.off_mv);
+    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p;
+    const int items = (npiv + nmove) * width;
+    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < items; e += gridDim.y * blockDim.x) {
+        const int row = e / width, w = p + e % width;
+        if (row < npiv) {
+            uint32_t acc = 0, T = pi->T[row];
+            while (T) {
+                const int j = __ffs(T) - 1;
+                T &= T - 1;
+                acc ^= mat[(size_t)pi->src[j] * d.rw + w];
+            }
+            pv[row * d.rw + w] = acc;
+        } else {
+            const int i = row - npiv;
+            mv[i * d.rw + w] = mat[(size_t)pi->from[i] * d.rw + w];
+        }
+    }
+}
+
+constexpr int APPLY_THREADS = 256;
+
+// Every row slot of the matrix, words p..: window slots take the pivot rows,
+// the others their (possibly moved) row with the panel columns cleared.
+__global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p)
+{
+    extern __shared__ __align__(16) uint32_t s_pv[];  // npiv x width
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    const PanelInfo *pi = reinterpret_cast<const PanelInfo *>(wk + d.off_panel);
+    if (pi->status != KG_OK)
+        return;
+    uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
+    const uint32_t *pv = reinterpret_cast<const uint32_t *>(wk + d.off_pv);
+    const uint32_t *mv = reinterpret_cast<const uint32_t *>(wk + d.off_mv);
+    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p, c0 = PANEL * p;
+    const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
+    for (int e = threadIdx.x; e < npiv * width; e += APPLY_THREADS)
+        s_pv[e] = pv[(e / width) * d.rw + p + e % width];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t to_l = lane < nmove ? pi->to[lane] : 0xFFFFFFFFu;
+    for (int slot = blockIdx.y * (APPLY_THREADS / 32) + warp; slot < d.mt; slot += gridDim.y * (APPLY_THREADS / 32)) {
+        uint32_t *dst = mat + (size_t)slot * d.rw + p;
+        if (slot >= c0 && slot < c0 + npiv) {
+            const uint32_t *src = s_pv + (slot - c0) * width;
+            for (int w = lane; w < width; w += 32)
+                dst[w] = src[w];
+            continue;
+        }
+        const uint32_t hit = __ballot_sync(0xFFFFFFFFu, to_l == (uint32_t)slot);
+        const uint32_t *src = hit ? mv + (__ffs(hit) - 1) * d.rw + p : dst;
+        // the row's panel word, read before any lane overwrites word 0
+        const uint32_t pw = __shfl_sync(0xFFFFFFFFu, lane == 0 ? src[0] : 0u, 0) & pmask;
+        for (int w = lane; w < width; w += 32) {
+            uint32_t acc = src[w], bits = pw;
+            while (bits) {
+                const int b = __ffs(bits) - 1;
+                bits &= bits - 1;
+                acc ^= s_pv[b * width + w];
+            }
+            dst[w] = acc;
+        }
+    }
+}
+
+// ---- 5. control bits ----------------------------------------------------------
+constexpr int CB_THREADS = 1024;
+constexpr int CB_PER = KG_MAX_Q / CB_THREADS;  // elements per thread (m = 13)
+
+size_t cbits_smem(const KgDims &d) { return (size_t)d.q * 4 + (size_t)d.q * 2 + (size_t)(d.cond + 3) / 4 * 4; }
+
+__device__ __forceinline__ uint32_t rev_bits(uint32_t s, int nb) { return nb ? __brev(s) >> (32 - nb) : 0; }
+
+// Control bit `gb` is bit gb % 8 of byte gb / 8 (controlbits.c:17-18).
+__device__ __forceinline__ void put_bit(uint32_t *bits, long gb, uint32_t v)
+{
+    if (v)
+        atomicOr(&bits[gb >> 5], 1u << (gb & 31));
+}
+
+__global__ void __launch_bounds__(CB_THREADS) k_kg_controlbits(uint8_t *__restrict__ work, KgDims d)
+{
+    extern __shared__ __align__(16) uint8_t sm_cb[];
+    int32_t *A = reinterpret_cast<int32_t *>(sm_cb);       // sort buffer, q entries
+    int16_t *X = reinterpret_cast<int16_t *>(A + d.q);     // exchange buffer
+    uint32_t *bits = reinterpret_cast<uint32_t *>(X + d.q);
+    __shared__ int s_bad;
+    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
+    PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
+    if (pinfo->status != KG_OK)
+        return;
+    const int tid = threadIdx.x, m = d.m, n = d.q, per = n / CB_THREADS;
+    const int16_t *pig = reinterpret_cast<const int16_t *>(wk + d.off_pi);
+    for (int i = tid; i < (d.cond + 3) / 4; i += CB_THREADS)
+        bits[i] = 0;
+    if (tid == 0)
+        s_bad = 0;
+    int P[CB_PER];
+#pragma unroll
+    for (int e = 0; e < CB_PER; e++)
+        if (e < per)
+            P[e] = pig[tid + CB_THREADS * e];
+    // element x = tid + CB_THREADS * e; local index lx = x mod ns
+    for (int lev = 0; lev < m - 1; lev++) {
+        const int w = m - lev, ns = n >> lev, half = n / 2;
+        int c[CB_PER], pp[CB_PER], tmp[CB_PER];
+        // (a) pibar(y) = pi(pi^-1(y ^ 1) ^ 1): sort (pi(x)^1, pi(x^1))
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per)
+                X[tid + CB_THREADS * e] = (int16_t)P[e];
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e;
+                A[x] = ((P[e] ^ 1) << 16) | X[x ^ 1];
+            }
+        seg_sort(A, n, w);
+        // c = min(x, pibar(x)); pp = pibar^2 via pibar^-1
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), pb = A[x] & 0xFFFF;
+                c[e] = min(lx, pb);
+                tmp[e] = pb;
+                A[x] = (pb << 16) | lx;
+            }
+        seg_sort(A, n, w);
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e;
+                A[x] = ((A[x] & 0xFFFF) << 16) | tmp[e];  // (pibar^-1(x), pibar(x))
+            }
+        seg_sort(A, n, w);
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per)
+                pp[e] = A[tid + CB_THREADS * e] & 0xFFFF;
+        // w - 2 times: c <- min(c, c o pp), pp <- pp o pp
+        for (int it = 1; it < w - 1; it++) {
+#pragma unroll
+            for (int e = 0; e < CB_PER; e++)
+                if (e < per) {
+                    const int x = tid + CB_THREADS * e;
+                    A[x] = (pp[e] << 16) | (x & (ns - 1));
+                }
+            seg_sort(A, n, w);
+#pragma unroll
+            for (int e = 0; e < CB_PER; e++)
+                if (e < per) {
+                    const int x = tid + CB_THREADS * e;
+                    tmp[e] = A[x] & 0xFFFF;  // pp^-1(x)
+                    A[x] = (tmp[e] << 16) | c[e];
+                }
+            seg_sort(A, n, w);
+#pragma unroll
+            for (int e = 0; e < CB_PER; e++)
+                if (e < per)
+                    c[e] = min(c[e], A[tid + CB_THREADS * e] & 0xFFFF);
+            if (it < w - 2) {
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < CB_PER; e++)
+                    if (e < per)
+                        A[tid + CB_THREADS * e] = (tmp[e] << 16) | pp[e];
+                seg_sort(A, n, w);
+#pragma unroll
+                for (int e = 0; e < CB_PER; e++)
+                    if (e < per)
+                        pp[e] = A[tid + CB_THREADS * e] & 0xFFFF;
+            }
+        }
+        // first layer: pair j of a segment swaps when c(2j) is odd
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per)
+                X[tid + CB_THREADS * e] = (int16_t)c[e];
+        __syncthreads();
+        int F[CB_PER];
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), s = x / ns;
+                const int f = X[x & ~1] & 1;
+                F[e] = lx ^ f;
+                if (!(lx & 1))
+                    put_bit(bits, (long)lev * half + rev_bits(s, lev) + (long)(lx >> 1) * (1 << lev), f);
+                A[x] = (P[e] << 16) | lx;  // for pi^-1
+            }
+        seg_sort(A, n, w);
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e;
+                A[x] = ((A[x] & 0xFFFF) << 16) | F[e];  // (pi^-1(x), F(x))
+            }
+        seg_sort(A, n, w);
+        // last layer: pair k swaps when F(pi(2k)) is odd; M(L(x)) = F(pi(x))
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e;
+                tmp[e] = A[x] & 0xFFFF;  // F(pi(x))
+                X[x] = (int16_t)tmp[e];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), s = x / ns;
+                const int l = X[x & ~1] & 1;
+                if (!(lx & 1))
+                    put_bit(bits,
+                            (long)lev * half + rev_bits(s, lev) + (long)(2 * w - 2) * half + (long)(lx >> 1) * (1 << lev),
+                            l);
+                tmp[e] = ((lx ^ l) << 16) | tmp[e];
+            }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per)
+                A[tid + CB_THREADS * e] = tmp[e];
+        seg_sort(A, n, w);
+        // halves of M become the two inner problems: q0(j) = M(2j)/2 in the
+        // first half of the segment, q1(j) = M(2j+1)/2 in the second
+#pragma unroll
+        for (int e = 0; e < CB_PER; e++)
+            if (e < per) {
+                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), base = x - lx, h = ns / 2;
+                const int src = lx < h ? base + 2 * lx : base + 2 * (lx - h) + 1;
+                P[e] = (A[src] & 0xFFFF) >> 1;
+            }
+    }
+    // w = 1: the pair swaps when pi(0) = 1
+#pragma unroll
+    for (int e = 0; e < CB_PER; e++)
+        if (e < per) {
+            const int x = tid + CB_THREADS * e;
+            if (!(x & 1))
+                put_bit(bits, (long)(m - 1) * (n / 2) + rev_bits(x >> 1, m - 1), P[e] & 1);
+        }
+    __syncthreads();
+    // check: layers 0..m-1 then m-2..0 (stride 2^s) applied to the identity
+    // must give pi (controlbits.c:193-212)
+    for (int i = tid; i < n; i += CB_THREADS)
+        X[i] = (int16_t)i;
+    for (int layer = 0; layer < 2 * m - 1; layer++) {
+        const int sh = layer < m ? layer : 2 * m - 2 - layer;
+        __syncthreads();
+        for (int k = tid; k < n / 2; k += CB_THREADS) {
+            const long gb = (long)layer * (n / 2) + k;
+            const int blk = k >> sh, j = k & ((1 << sh) - 1);
+            const int a = blk * (2 << sh) + j, b = a + (1 << sh);
+            if ((bits[gb >> 5] >> (gb & 31)) & 1u) {
+                const int16_t u = X[a];
+                X[a] = X[b];
+                X[b] = u;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += CB_THREADS)
+        if (X[i] != pig[i])
+            s_bad = 1;
+    __syncthreads();
+    uint8_t *cond = wk + d.off_cond;
+    const uint8_t *bb = reinterpret_cast<const uint8_t *>(bits);
+    for (int i = tid; i < d.cond; i += CB_THREADS)
+        cond[i] = bb[i];
+    if (tid == 0 && s_bad)
+        pinfo->status = KG_CBITS;
+}
+
+// ---- 6. outputs ---------------------------------------------------------------
+// sk = seed | 0xFFFFFFFF as 8 little-endian bytes | g (2t) | control bits | s
+// (operations.c:60-100); pk row r = bytes mt/8 .. of reduced row r.
+__global__ void k_kg_output(const uint8_t *__restrict__ work, const uint8_t *__restrict__ seeds, const int *__restrict__ idx,
+                            uint8_t *__restrict__ pk, uint8_t *__restrict__ sk, KgDims d)
+{
+    const int k = blockIdx.x;
+    const uint8_t *wk = work + (size_t)k * d.stride;
+    if (reinterpret_cast<const PanelInfo *>(wk + d.off_panel)->status != KG_OK)
+        return;
+    const int out = idx[k];
+    uint8_t *skp = sk + (size_t)out * d.sk;
+    const int off_irr = 40, off_cond = 40 + 2 * d.t, off_s = off_cond + d.cond;
+    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < d.sk; i += gridDim.y * blockDim.x) {
+        uint8_t v;
+        if (i < 32)
+            v = seeds[(size_t)k * 32 + i];
+        else if (i < 40)
+            v = i < 36 ? 0xFF : 0;
+        else if (i < off_cond)
+            v = wk[d.off_irr + (i - off_irr)];
+        else if (i < off_s)
+            v = wk[d.off_cond + (i - off_cond)];
+        else
+            v = wk[d.off_r + (i - off_s)];
+        skp[i] = v;
+    }
+    const uint8_t *mat = wk + d.off_mat;
+    uint8_t *pkp = pk + (size_t)out * d.mt * d.pk_row;
+    const size_t total = (size_t)d.mt * d.pk_row;
+    for (size_t e = (size_t)blockIdx.y * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.y * blockDim.x) {
+        const int r = (int)(e / d.pk_row), b = (int)(e % d.pk_row);
+        pkp[e] = mat[(size_t)r * d.rw * 4 + d.mt / 8 + b];
+    }
+}
+
+// Log/antilog tables of GF(2^m) for the smallest generator.
+void host_tables(int m, GfTables &T)
+{
+    const uint32_t poly = m == 12 ? 0x1009u : 0x201Bu, q = 1u << m;
+    auto mul = [&](uint32_t a, uint32_t b) {
+        uint32_t r = 0;
+        for (int i = 0; i < m; i++)
+            if ((b >> i) & 1u)
+                r ^= a << i;
+        for (int k = 2 * m - 2; k >= m; k--)
+            if ((r >> k) & 1u)
+                r ^= poly << (k - m);
+        return r;
+    };
+    memset(&T, 0, sizeof T);
+    for (uint32_t gen = 2; gen < q; gen++) {
+        uint32_t x = 1, i = 0;
+        bool ok = true;
+        for (i = 0; i < q - 1; i++) {
+            if (x == 1 && i > 0) {
+                ok = false;
+                break;
+            }
+            T.ex[i] = (uint16_t)x;
+            T.lg[x] = (uint16_t)i;
+            x = mul(x, gen);
+        }
+        if (ok && x == 1)
+            return;
+    }
+}
+
+const GfTables &tables_for(int m)
+{
+    static GfTables t12, t13;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        host_tables(12, t12);
+        host_tables(13, t13);
+    });
+    return m == 12 ? t12 : t13;
+}
+
+int set_smem_attr(const void *fn, size_t bytes)
+{
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return e == cudaSuccess ? CMD_OK : cuda_fail(e, "keygen smem attribute");
+}
+
+}  // namespace
+}  // namespace cmd
+
+using namespace cmd;
+
+extern "C" {
+
+int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, size_t count, uint8_t *h_pk,
+                          uint8_t *h_sk, uint32_t *h_attempts, uint32_t max_attempts)
+{
+    if (!eng || !valid_set(set) || !h_seeds || !h_pk || !h_sk || count == 0 || count > 4096)
+        return CMD_E_ARG;
+    if (max_attempts == 0)
+        max_attempts = 1000;
+    std::lock_guard<std::mutex> lk(eng->mu);
+    cudaSetDevice(eng->device);
+    const KgDims d = kg_dims(set);
+    const size_t pk_bytes = (size_t)d.mt * d.pk_row;
+    // workspace for up to `chunk` keys at once, within the budget
+    size_t chunk = std::min<size_t>(count, 256);
+    const size_t fixed = sizeof(GfTables) + 256;
+    auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 4 + pk_bytes + d.sk); };
+    while (chunk > 1 && !budget_take(eng, need(chunk)))
+        chunk /= 2;
+    if (chunk == 1 && !budget_take(eng, need(1))) {
+        set_last_error("key generation workspace exceeds the engine HBM budget");
+        return CMD_E_BUDGET;
+    }
+    const size_t bytes = need(chunk);
+    uint8_t *mem = nullptr;
+    cudaError_t e = cudaMalloc(&mem, bytes);
+    if (e != cudaSuccess) {
+        budget_give(eng, bytes);
+        return cuda_fail(e, "keygen workspace");
+    }
+    uint8_t *d_work = mem;
+    uint8_t *d_seed = d_work + chunk * d.stride;
+    int *d_idx = reinterpret_cast<int *>(d_seed + chunk * 32);
+    uint8_t *d_pk = reinterpret_cast<uint8_t *>(d_idx + chunk);
+    uint8_t *d_sk = d_pk + chunk * pk_bytes;
+    GfTables *d_tab = reinterpret_cast<GfTables *>(d_sk + chunk * d.sk);
+    d_tab = reinterpret_cast<GfTables *>((reinterpret_cast<uintptr_t>(d_tab) + 255) / 256 * 256);
+    cudaStream_t s = eng->stream;
+    LaunchCounter lc{&eng->launches};
+    int rc = CMD_OK;
+    const size_t smem_gp = genpoly_smem(d), smem_sup = support_smem(d), smem_cb = cbits_smem(d);
+    const size_t smem_apply = (size_t)PANEL * d.rw * 4;
+    if ((rc = set_smem_attr((const void *)k_kg_genpoly, smem_gp)) || (rc = set_smem_attr((const void *)k_kg_support, smem_sup)) ||
+        (rc = set_smem_attr((const void *)k_kg_controlbits, smem_cb)) ||
+        (rc = set_smem_attr((const void *)k_ge_apply, smem_apply))) {
+        cudaFree(mem);
+        budget_give(eng, bytes);
+        return rc;
+    }
+    e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
+    // keys still to finish: their output index and current seed
+    std::vector<int> pend(count);
+    std::vector<uint8_t> seeds(h_seeds, h_seeds + 32 * count);
+    for (size_t i = 0; i < count; i++) {
+        pend[i] = (int)i;
+        if (h_attempts)
+            h_attempts[i] = 0;
+    }
+    std::vector<int> status;
+    std::vector<uint8_t> nxt;
+    std::vector<uint8_t> cur_seed;
+    for (uint32_t round = 0; round < max_attempts && !pend.empty() && e == cudaSuccess; round++) {
+        std::vector<int> still;
+        for (size_t base = 0; base < pend.size() && e == cudaSuccess; base += chunk) {
+            const int K = (int)std::min(chunk, pend.size() - base);
+            cur_seed.resize((size_t)K * 32);
+            std::vector<int> idx(K);
+            for (int k = 0; k < K; k++) {
+                idx[k] = k;
+                memcpy(&cur_seed[(size_t)k * 32], &seeds[(size_t)pend[base + k] * 32], 32);
+            }
+            if ((e = cudaMemcpyAsync(d_seed, cur_seed.data(), (size_t)K * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(d_idx, idx.data(), (size_t)K * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                break;
+            k_kg_expand<<<(K + 31) / 32, 32, 0, s>>>(d_seed, d_work, d, K);
+            k_kg_genpoly<<<K, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
+            k_kg_support<<<K, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
+            const int npanels = (d.mt + PANEL - 1) / PANEL;
+            const int gy = std::max(1, std::min(64, 2 * eng->num_sms / K));
+            for (int p = 0; p < npanels; p++) {
+                k_ge_panel<<<K, PANEL_THREADS, 0, s>>>(d_work, d, p);
+                k_ge_pivots<<<dim3(K, 8), 256, 0, s>>>(d_work, d, p);
+                k_ge_apply<<<dim3(K, gy), APPLY_THREADS, (size_t)PANEL * (d.rw - p) * 4, s>>>(d_work, d, p);
+            }
+            k_kg_controlbits<<<K, CB_THREADS, smem_cb, s>>>(d_work, d);
+            k_kg_output<<<dim3(K, 16), 256, 0, s>>>(d_work, d_seed, d_idx, d_pk, d_sk, d);
+            lc.bump(5 + 3 * (uint64_t)npanels);
+            if ((e = cudaGetLastError()) != cudaSuccess)
+                break;
+            // statuses and next seeds
+            status.resize(K);
+            nxt.resize((size_t)K * 32);
+            for (int k = 0; k < K && e == cudaSuccess; k++) {
+                e = cudaMemcpyAsync(&status[k], d_work + (size_t)k * d.stride + d.off_panel, 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(&nxt[(size_t)k * 32], d_work + (size_t)k * d.stride + d.off_r + d.rlen - 32, 32,
+                                        cudaMemcpyDeviceToHost, s);
+            }
+            if (e == cudaSuccess)
+                e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess)
+                break;
+            for (int k = 0; k < K; k++) {
+                const int out = pend[base + k];
+                if (h_attempts)
+                    h_attempts[out]++;
+                if (status[k] == KG_OK) {
+                    if ((e = cudaMemcpy(h_pk + (size_t)out * pk_bytes, d_pk + (size_t)k * pk_bytes, pk_bytes,
+                                        cudaMemcpyDeviceToHost)) != cudaSuccess ||
+                        (e = cudaMemcpy(h_sk + (size_t)out * d.sk, d_sk + (size_t)k * d.sk, d.sk, cudaMemcpyDeviceToHost)) !=
+                            cudaSuccess)
+                        break;
+                } else if (status[k] == KG_CBITS) {
+                    rc = CMD_E_KEYGEN;
+                    set_last_error("key generation: control bits do not reproduce the permutation");
+                } else {
+                    memcpy(&seeds[(size_t)out * 32], &nxt[(size_t)k * 32], 32);
+                    still.push_back(out);
+                }
+            }
+        }
+        pend.swap(still);
+    }
+    cudaFree(mem);
+    budget_give(eng, bytes);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "key generation");
+    if (rc)
+        return rc;
+    if (!pend.empty()) {
+        set_last_error("key generation: attempt limit reached");
+        return CMD_E_KEYGEN;
+    }
+    return CMD_OK;
+}
+
+int cmd_kem_keypair(cmd_engine *eng, cmd_set set, const uint8_t *h_seed, uint8_t *h_pk, uint8_t *h_sk,
+                    uint32_t *attempts)
+{
+    return cmd_kem_keypair_batch(eng, set, h_seed, 1, h_pk, h_sk, attempts, 0);
+}
+
+}  // extern "C"

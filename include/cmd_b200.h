@@ -36,6 +36,7 @@ extern "C" {
 #define CMD_E_BUSY        -8  /* serving queue full                           */
 #define CMD_E_TIMEOUT     -9  /* a bounded wait gave up                       */
 #define CMD_E_NODEVICE   -10  /* no CUDA device / kernels not loadable        */
+#define CMD_E_KEYGEN     -11  /* key generation: attempt limit or self-check   */
 
 /* ---- parameter sets (CPU/param/param<set>/include/common.h) ----------- */
 typedef enum {
@@ -311,6 +312,23 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *out, int reset);
 int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *cts, size_t ct_stride,
                        uint8_t *err_pool, size_t err_stride, size_t pool, double rate_per_s,
                        double seconds, uint64_t seed, cmd_server_stats *out);
+
+/* ---- key generation (kem/common/core/operations.c:36-107) -------------- */
+/* crypto_kem_keypair with randombytes() yielding the caller's 32-byte seed:
+ * pk receives mt rows of (n - mt + 7)/8 bytes (pk_gen.c:145-146), sk the
+ * reference's secret-key layout (seed | pivots | g | control bits | s).  A
+ * rejected attempt continues with the next seed of the expansion, as the
+ * reference's loop does, so a seed yields the reference's key pair; the
+ * secret key's first 32 bytes are the seed of the accepted attempt.
+ * *attempts (may be NULL) receives the attempts taken.  Every stage runs on
+ * the GPU (not constant-time; see keygen.cu).  CMD_E_KEYGEN if the attempt
+ * limit is reached or the control bits fail their self-check. */
+int cmd_kem_keypair(cmd_engine *eng, cmd_set set, const uint8_t *h_seed, uint8_t *h_pk,
+                    uint8_t *h_sk, uint32_t *attempts);
+/* count (1..4096) seeds of 32 bytes: key pairs in pk/sk rows of the sizes
+ * above; attempts[i] per key (may be NULL); max_attempts 0 = 1000. */
+int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, size_t count,
+                          uint8_t *h_pk, uint8_t *h_sk, uint32_t *attempts, uint32_t max_attempts);
 
 /* ---- fused-kernel tuning and graph replay (no reference counterpart) --- */
 /* Picks the fused kernel's launch configuration for key's set on this GPU

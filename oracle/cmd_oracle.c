@@ -411,3 +411,268 @@ out:
     free(ginv2);
     return rc;
 }
+
+/* ---- key generation ---------------------------------------------------- */
+
+/* Reduction terms of the degree-t field polynomial F(y) defining GF((2^m)^t)
+ * (kem/variant_<set>/gf.c GF_mul): y^t = sum of coef * y^off.
+ *   348864: y^64 = y^3 + y + z      (z = the field element 2)
+ *   460896: y^96 = y^10 + y^9 + y^6 + 1
+ *   6688128, 8192128: y^128 = y^7 + y^2 + y + 1
+ *   6960119: y^119 = y^8 + 1 */
+static int ext_terms(int set_id, int *off, uint16_t *coef)
+{
+    switch (set_id) {
+    case 348864: off[0] = 3; off[1] = 1; off[2] = 0; coef[0] = 1; coef[1] = 1; coef[2] = 2; return 3;
+    case 460896: off[0] = 10; off[1] = 9; off[2] = 6; off[3] = 0; break;
+    case 6960119: off[0] = 8; off[1] = 0; coef[0] = coef[1] = 1; return 2;
+    default: off[0] = 7; off[1] = 2; off[2] = 1; off[3] = 0; break;
+    }
+    coef[0] = coef[1] = coef[2] = coef[3] = 1;
+    return 4;
+}
+
+/* out = a * b in GF((2^m)^t): schoolbook product, then y^k (k >= t) folded
+ * down from the top with the terms of F. */
+static void ext_mul(const o_params *p, uint16_t *out, const uint16_t *a, const uint16_t *b)
+{
+    const int t = p->t, m = p->m;
+    uint16_t prod[2 * 128];
+    int off[4];
+    uint16_t coef[4];
+    const int nt = ext_terms(p->set_id, off, coef);
+    memset(prod, 0, sizeof prod);
+    for (int i = 0; i < t; i++)
+        for (int j = 0; j < t; j++)
+            prod[i + j] ^= o_gf_mul(m, a[i], b[j]);
+    for (int k = 2 * t - 2; k >= t; k--)
+        for (int u = 0; u < nt; u++)
+            prod[k - t + off[u]] ^= coef[u] == 1 ? prod[k] : o_gf_mul(m, prod[k], coef[u]);
+    memcpy(out, prod, (size_t)t * sizeof(uint16_t));
+}
+
+/* The minimal polynomial y^t + sum_{j<t} g_j y^j of f satisfies
+ * f^t = sum_j g_j f^j: solve that t x t system over GF(2^m) (columns f^j) by
+ * Gauss-Jordan elimination.  A singular system means f lies in a proper
+ * subfield (degree below t): the reference rejects the draw (sk_gen.c:60-63). */
+int o_kg_genpoly(const o_params *p, const uint16_t *f, uint16_t *irr)
+{
+    const int t = p->t, m = p->m;
+    /* a[r][c]: row r = coordinate, column c = power f^c; column t = f^t */
+    uint16_t *a = (uint16_t *)calloc((size_t)t * (t + 1), sizeof(uint16_t));
+    uint16_t *pw = (uint16_t *)calloc((size_t)t, sizeof(uint16_t));
+    uint16_t *nx = (uint16_t *)calloc((size_t)t, sizeof(uint16_t));
+    if (!a || !pw || !nx) {
+        free(a), free(pw), free(nx);
+        return -2;
+    }
+#define A_(r, c) a[(size_t)(r) * (t + 1) + (c)]
+    pw[0] = 1;
+    for (int c = 0; c <= t; c++) {
+        for (int r = 0; r < t; r++)
+            A_(r, c) = pw[r];
+        if (c < t) {
+            ext_mul(p, nx, pw, f);
+            memcpy(pw, nx, (size_t)t * sizeof(uint16_t));
+        }
+    }
+    int rc = 0;
+    for (int col = 0; col < t && rc == 0; col++) {
+        int piv = -1;
+        for (int r = col; r < t; r++)
+            if (A_(r, col)) {
+                piv = r;
+                break;
+            }
+        if (piv < 0) {
+            rc = -1;
+            break;
+        }
+        if (piv != col)
+            for (int c = 0; c <= t; c++) {
+                uint16_t x = A_(piv, c);
+                A_(piv, c) = A_(col, c);
+                A_(col, c) = x;
+            }
+        const uint16_t inv = o_gf_inv(m, A_(col, col));
+        for (int c = col; c <= t; c++)
+            A_(col, c) = o_gf_mul(m, A_(col, c), inv);
+        for (int r = 0; r < t; r++) {
+            const uint16_t k = A_(r, col);
+            if (r == col || !k)
+                continue;
+            for (int c = col; c <= t; c++)
+                A_(r, c) ^= o_gf_mul(m, A_(col, c), k);
+        }
+    }
+    if (rc == 0)
+        for (int r = 0; r < t; r++)
+            irr[r] = A_(r, t);
+#undef A_
+    free(a), free(pw), free(nx);
+    return rc;
+}
+
+static int cmp_u64(const void *x, const void *y)
+{
+    const uint64_t a = *(const uint64_t *)x, b = *(const uint64_t *)y;
+    return a < b ? -1 : a > b;
+}
+
+/* Support and parity-check matrix as in pk_gen.c:52-113: pi lists the
+ * indices 0..2^m-1 ordered by their random word (rejected if two words are
+ * equal), L_i = bitrev(pi_i), and row j*m + k, column i holds bit k of
+ * L_i^j / g(L_i).  Gauss-Jordan elimination on the first mt columns must find
+ * every pivot (else rejected); the reduced matrix is [I | T] whatever order
+ * the eliminations take, and the public key is each row's bytes from byte
+ * mt/8 on (pk_gen.c:145-146), so for mt not a multiple of 8 the first byte of
+ * a row also carries the last mt mod 8 identity columns. */
+int o_kg_pk_gen(const o_params *p, const uint16_t *irr, const uint32_t *perm, uint8_t *pk, int16_t *pi)
+{
+    const int m = p->m, n = p->n, t = p->t, mt = m * t, q = 1 << m;
+    const int row_words = (n + 63) / 64, nbytes = n / 8, pk_row = (n - mt + 7) / 8;
+    uint64_t *buf = (uint64_t *)malloc((size_t)q * sizeof(uint64_t));
+    uint64_t *mat = (uint64_t *)calloc((size_t)mt * row_words, sizeof(uint64_t));
+    uint16_t *g = (uint16_t *)malloc((size_t)(t + 1) * sizeof(uint16_t));
+    uint16_t *L = (uint16_t *)malloc((size_t)n * sizeof(uint16_t));
+    uint16_t *v = (uint16_t *)malloc((size_t)n * sizeof(uint16_t));
+    int rc = 0;
+    if (!buf || !mat || !g || !L || !v) {
+        rc = -2;
+        goto out;
+    }
+    for (int i = 0; i < q; i++)
+        buf[i] = ((uint64_t)perm[i] << 31) | (uint64_t)i;
+    qsort(buf, (size_t)q, sizeof(uint64_t), cmp_u64);
+    for (int i = 1; i < q; i++)
+        if ((buf[i - 1] >> 31) == (buf[i] >> 31)) {
+            rc = -1;
+            goto out;
+        }
+    for (int i = 0; i < q; i++)
+        pi[i] = (int16_t)(buf[i] & (uint64_t)(q - 1));
+    for (int i = 0; i < n; i++)
+        L[i] = o_bitrev(m, (uint16_t)pi[i]);
+    memcpy(g, irr, (size_t)t * sizeof(uint16_t));
+    g[t] = 1;
+    for (int i = 0; i < n; i++)
+        v[i] = o_gf_inv(m, o_eval(m, t, g, L[i]));
+    for (int j = 0; j < t; j++) {
+        for (int i = 0; i < n; i++) {
+            for (int k = 0; k < m; k++)
+                if ((v[i] >> k) & 1u)
+                    mat[(size_t)(j * m + k) * row_words + i / 64] |= 1ull << (i % 64);
+            v[i] = o_gf_mul(m, v[i], L[i]);
+        }
+    }
+    for (int c = 0; c < mt; c++) {
+        const int w = c / 64;
+        const uint64_t bit = 1ull << (c % 64);
+        int piv = -1;
+        for (int r = c; r < mt; r++)
+            if (mat[(size_t)r * row_words + w] & bit) {
+                piv = r;
+                break;
+            }
+        if (piv < 0) {
+            rc = -1;
+            goto out;
+        }
+        uint64_t *pr = mat + (size_t)piv * row_words, *cr = mat + (size_t)c * row_words;
+        if (piv != c)
+            for (int x = 0; x < row_words; x++) {
+                const uint64_t tmp = pr[x];
+                pr[x] = cr[x];
+                cr[x] = tmp;
+            }
+        for (int r = 0; r < mt; r++) {
+            uint64_t *rr = mat + (size_t)r * row_words;
+            if (r != c && (rr[w] & bit))
+                for (int x = w; x < row_words; x++)
+                    rr[x] ^= cr[x];
+        }
+    }
+    for (int r = 0; r < mt; r++) {
+        const uint64_t *rr = mat + (size_t)r * row_words;
+        for (int b = 0; b < pk_row; b++) {
+            const int byte = mt / 8 + b;
+            pk[(size_t)r * pk_row + b] = byte < nbytes ? (uint8_t)(rr[byte / 8] >> (8 * (byte % 8))) : 0;
+        }
+    }
+out:
+    free(buf), free(mat), free(g), free(L), free(v);
+    return rc;
+}
+
+/* Benes control bits by the cycle-labelling recursion of Nassimi and Sahni
+ * in the formulation of Bernstein, "Verified fast formulas for control bits
+ * for permutation networks" (2020), which controlbits.c:22-170 implements
+ * with constant-time sorts; here every sort is the permutation algebra it
+ * performs (inverses, compositions, gathers).  For pi on n = 2^w points:
+ *   pibar(y) = pi(pi^-1(y ^ 1) ^ 1);  c(x) = min(x, pibar(x)); p = pibar^2;
+ *   w-2 times: c <- min(c, c o p), p <- p o p;
+ *   first-layer bit j = c(2j) & 1 (F swaps pair j when set);
+ *   last-layer bit k = F(pi(2k)) & 1 (L swaps pair k when set);
+ *   M = F o pi o L; the two halves q0(j) = M(2j)/2, q1(j) = M(2j+1)/2 recurse
+ *   as the inner networks, interleaved at stride 2 step. */
+static void cb_rec(uint8_t *out, long pos, long step, const int16_t *pi, int w, long n, int32_t *ws)
+{
+    if (w == 1) {
+        out[pos >> 3] ^= (uint8_t)((pi[0] & 1) << (pos & 7));
+        return;
+    }
+    int32_t *inv = ws, *pb = ws + n, *c = ws + 2 * n, *pp = ws + 3 * n, *tmp = ws + 4 * n, *F = ws + 5 * n;
+    int16_t *q = (int16_t *)(ws + 6 * n);
+    int32_t *rest = ws + 7 * n;
+    for (long x = 0; x < n; x++)
+        inv[pi[x]] = (int32_t)x;
+    for (long y = 0; y < n; y++)
+        pb[y] = pi[inv[y ^ 1] ^ 1];
+    for (long x = 0; x < n; x++) {
+        c[x] = x < pb[x] ? (int32_t)x : pb[x];
+        pp[x] = pb[pb[x]];
+    }
+    for (int i = 1; i < w - 1; i++) {
+        for (long x = 0; x < n; x++) {
+            const int32_t cp = c[pp[x]];
+            tmp[x] = cp < c[x] ? cp : c[x];
+        }
+        memcpy(c, tmp, (size_t)n * sizeof(int32_t));
+        for (long x = 0; x < n; x++)
+            tmp[x] = pp[pp[x]];
+        memcpy(pp, tmp, (size_t)n * sizeof(int32_t));
+    }
+    for (long j = 0; j < n / 2; j++) {
+        const int32_t fj = c[2 * j] & 1;
+        out[(pos + j * step) >> 3] ^= (uint8_t)(fj << ((pos + j * step) & 7));
+        F[2 * j] = (int32_t)(2 * j) + fj;
+        F[2 * j + 1] = F[2 * j] ^ 1;
+    }
+    const long last = pos + (2 * w - 2) * step * (n / 2);
+    for (long k = 0; k < n / 2; k++) {
+        const int32_t a0 = F[pi[2 * k]], a1 = F[pi[2 * k + 1]];
+        const int32_t lk = a0 & 1;
+        out[(last + k * step) >> 3] ^= (uint8_t)(lk << ((last + k * step) & 7));
+        /* M(L(y)) = F(pi(y)); L swaps the pair when lk is set */
+        tmp[2 * k + lk] = a0;
+        tmp[(2 * k + lk) ^ 1] = a1;
+    }
+    for (long j = 0; j < n / 2; j++) {
+        q[j] = (int16_t)(tmp[2 * j] >> 1);
+        q[j + n / 2] = (int16_t)(tmp[2 * j + 1] >> 1);
+    }
+    cb_rec(out, pos + (n / 2) * step, step * 2, q, w - 1, n / 2, rest);
+    cb_rec(out, pos + (n / 2) * step + step, step * 2, q + n / 2, w - 1, n / 2, rest);
+}
+
+void o_kg_controlbits(int m, const int16_t *pi, uint8_t *out)
+{
+    const long n = 1L << m;
+    memset(out, 0, (size_t)((2 * m - 1) * n / 2 + 7) / 8);
+    /* each level takes 6.5 n int32 of workspace (q: n int16) */
+    int32_t *ws = (int32_t *)malloc((size_t)(8 * n) * sizeof(int32_t) * 2);
+    if (!ws)
+        return;
+    cb_rec(out, 0, 1, pi, m, n, ws);
+    free(ws);
+}

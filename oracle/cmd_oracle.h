@@ -74,6 +74,21 @@ int o_decap_accept(const o_params *p, const uint8_t *sk, const uint8_t *cts,
 long o_errorstream_format(const o_params *p, const uint8_t *err_bytes,
                           size_t count, char *out, size_t cap);
 
+/* Key generation stages of crypto_kem_keypair (kem/common/core/operations.c:
+ * 36-107); the seed expansion around them is restated in oracle.py.
+ *  o_kg_genpoly: minimal polynomial of f in GF((2^m)^t) (sk_gen.c:24-85 with
+ *    kem/variant_<set>/gf.c GF_mul); irr gets its t low coefficients; -1 if
+ *    the degree is below t.
+ *  o_kg_pk_gen: public key (mt rows of (n-mt+7)/8 bytes) and support
+ *    permutation pi (2^m entries) from the Goppa polynomial (t coefficients)
+ *    and 2^m random words (pk_gen.c:29-149); -1 when the draw is rejected.
+ *  o_kg_controlbits: Benes control bits of pi, (2m-1) 2^(m-4) bytes
+ *    (controlbits.c:22-220). */
+int o_kg_genpoly(const o_params *p, const uint16_t *f, uint16_t *irr);
+int o_kg_pk_gen(const o_params *p, const uint16_t *irr, const uint32_t *perm,
+                uint8_t *pk, int16_t *pi);
+void o_kg_controlbits(int m, const int16_t *pi, uint8_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -151,6 +151,34 @@ class Oracle:
             keys[c] = np.frombuffer(hashlib.shake_256(pre + cts[c].tobytes()).digest(32), np.uint8)
         return keys, acc
 
+    # -- key generation (crypto_kem_keypair, kem/common/core/operations.c:36-107)
+    def kg_genpoly(self, f: np.ndarray):
+        f = np.ascontiguousarray(f, np.uint16)
+        irr = np.zeros(self.t, np.uint16)
+        rc = self.lib.o_kg_genpoly(ctypes.byref(self.p), _ptr(f, _u16p), _ptr(irr, _u16p))
+        return (irr if rc == 0 else None)
+
+    def kg_pk_gen(self, irr: np.ndarray, perm: np.ndarray):
+        irr = np.ascontiguousarray(irr, np.uint16)
+        perm = np.ascontiguousarray(perm, np.uint32)
+        mt = self.m * self.t
+        pk = np.zeros(mt * ((self.n - mt + 7) // 8), np.uint8)
+        pi = np.zeros(1 << self.m, np.int16)
+        rc = self.lib.o_kg_pk_gen(ctypes.byref(self.p), _ptr(irr, _u16p), perm.ctypes.data_as(ctypes.c_void_p),
+                                  _ptr(pk, _u8p), pi.ctypes.data_as(ctypes.c_void_p))
+        return (pk, pi) if rc == 0 else None
+
+    def kg_controlbits(self, pi: np.ndarray) -> np.ndarray:
+        pi = np.ascontiguousarray(pi, np.int16)
+        out = np.zeros(self.p.cond_bytes, np.uint8)
+        self.lib.o_kg_controlbits(self.m, pi.ctypes.data_as(ctypes.c_void_p), _ptr(out, _u8p))
+        return out
+
+    def keypair(self, seed: bytes, max_attempts: int = 256):
+        """Returns (pk bytes, sk bytes, attempts) of crypto_kem_keypair with
+        randombytes() yielding `seed`; see keypair_from_seed."""
+        return keypair_from_seed(self, seed, max_attempts)
+
     def errorstream(self, err: np.ndarray) -> bytes:
         err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n // 8)
         cap = err.shape[0] * (1 + 6 * self.n // 8 * 8) + 16
@@ -160,6 +188,78 @@ class Oracle:
         if got < 0:
             raise RuntimeError("errorstream buffer too small")
         return buf.raw[:got]
+
+
+def keypair_from_seed(stages, seed: bytes, max_attempts: int = 256):
+    """crypto_kem_keypair (kem/common/core/operations.c:36-107) with
+    randombytes() yielding the 32-byte `seed`, over a stage provider (the
+    restatement ``Oracle`` or the reference's own ``RefKeygen``).  Each attempt
+    expands 0x40 || seed with SHAKE256 into r = s (n/8) | perm (4 * 2^m) |
+    f (2t) | next seed (32); a rejected attempt continues with the next seed.
+    sk = seed | 0xFFFFFFFF as 8 bytes | irr (2t) | control bits | s."""
+    import hashlib
+    m, n, t = stages.m, stages.n, stages.t
+    q = 1 << m
+    rlen = n // 8 + 4 * q + 2 * t + 32
+    seed = bytes(seed)
+    assert len(seed) == 32
+    for attempt in range(1, max_attempts + 1):
+        r = hashlib.shake_256(b"\x40" + seed).digest(rlen)
+        f = np.frombuffer(r, "<u2", t, rlen - 32 - 2 * t) & (q - 1)
+        irr = stages.kg_genpoly(f)
+        if irr is not None:
+            perm = np.frombuffer(r, "<u4", q, rlen - 32 - 2 * t - 4 * q)
+            got = stages.kg_pk_gen(irr, perm)
+            if got is not None:
+                pk, pi = got
+                cond = stages.kg_controlbits(pi)
+                sk = seed + bytes.fromhex("ffffffff00000000") + irr.astype("<u2").tobytes() + cond.tobytes() + r[: n // 8]
+                return pk.tobytes(), sk, attempt
+        seed = r[rlen - 32:]
+    raise RuntimeError("no key after max_attempts")
+
+
+class RefKeygen:
+    """The reference's own kem/ key generation for one set
+    (oracle/_ref/libkeygen_<set>.so): genpoly_gen, pk_gen, controlbits."""
+
+    def __init__(self, set_id: int):
+        path = os.path.join(HERE, "_ref", f"libkeygen_{set_id}.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        info = (ctypes.c_int * 6)()
+        self.lib.ref_kg_info(info)
+        self.m, self.n, self.t, self.pk_rows, self.pk_row_bytes, self.cond_bytes = list(info)
+        self.set_id = set_id
+
+    @staticmethod
+    def available(set_id: int) -> bool:
+        return os.path.exists(os.path.join(HERE, "_ref", f"libkeygen_{set_id}.so"))
+
+    def kg_genpoly(self, f: np.ndarray):
+        f = np.ascontiguousarray(f, np.uint16)
+        irr = np.zeros(self.t, np.uint16)
+        rc = self.lib.ref_kg_genpoly(f.ctypes.data_as(ctypes.c_void_p), irr.ctypes.data_as(ctypes.c_void_p))
+        return irr if rc == 0 else None
+
+    def kg_pk_gen(self, irr: np.ndarray, perm: np.ndarray):
+        irr_b = np.ascontiguousarray(irr, "<u2").tobytes()
+        perm = np.ascontiguousarray(perm, np.uint32)
+        pk = np.zeros(self.pk_rows * self.pk_row_bytes, np.uint8)
+        pi = np.zeros(1 << self.m, np.int16)
+        rc = self.lib.ref_kg_pk_gen(pk.ctypes.data_as(ctypes.c_void_p), ctypes.c_char_p(irr_b),
+                                    perm.ctypes.data_as(ctypes.c_void_p), pi.ctypes.data_as(ctypes.c_void_p))
+        return (pk, pi) if rc == 0 else None
+
+    def kg_controlbits(self, pi: np.ndarray) -> np.ndarray:
+        pi = np.ascontiguousarray(pi, np.int16)
+        out = np.zeros(self.cond_bytes, np.uint8)
+        self.lib.ref_kg_controlbits(out.ctypes.data_as(ctypes.c_void_p), pi.ctypes.data_as(ctypes.c_void_p))
+        return out
+
+    def keypair(self, seed: bytes, max_attempts: int = 256):
+        return keypair_from_seed(self, seed, max_attempts)
 
 
 class RefLib:
