@@ -62,6 +62,7 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--serve-keys", type=int, default=1024)
     ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--no-keygen", action="store_true", help="skip the key-generation leg")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the all-sets (2^20 each) and mixed-batch (2^18) measurements")
     return ap.parse_args()
@@ -281,6 +282,57 @@ def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3) -> di
         del d_ct, d_err, d_w
         key.free()
     return out
+
+
+def keygen_leg(cmd, eng, set_id: int = 6960119, count: int = 64, cpu_seconds: float = 12.0) -> dict:
+    """Key generation (crypto_kem_keypair, kem/common/core/operations.c:36-107)
+    for `count` seeds in one batched call, host seeds in and host key pairs
+    out, against the reference's own key generation (oracle/_ref
+    libkeygen_<set>, its SHAKE256 seed expansion done with hashlib) on all
+    host cores over a bounded sample of seeds.  Rates count whole key pairs,
+    rejected attempts included (about 3.5 attempts per key on average)."""
+    import concurrent.futures as cf
+    import threading
+
+    from oracle import oracle as o
+    g = np.random.default_rng(0xC0FFEE)
+    seeds = np.frombuffer(g.bytes(32 * count), np.uint8).reshape(count, 32)
+    cmd.kem_keypair_batch(eng, set_id, np.frombuffer(g.bytes(64), np.uint8).reshape(2, 32))  # warm-up
+    t0 = time.perf_counter()
+    one = cmd.kem_keypair(eng, set_id, seeds[0].tobytes())
+    single_s = time.perf_counter() - t0
+    l0 = eng.launch_count()
+    t0 = time.perf_counter()
+    pks, sks, att = cmd.kem_keypair_batch(eng, set_id, seeds)
+    dt = time.perf_counter() - t0
+    launches = eng.launch_count() - l0
+    checker = o.RefKeygen(set_id) if o.RefKeygen.available(set_id) else o.Oracle(set_id)
+    ok = all(checker.keypair(seeds[i].tobytes()) == (pks[i].tobytes(), sks[i].tobytes(), int(att[i]))
+             for i in range(2)) and (one[0], one[1]) == (pks[0].tobytes(), sks[0].tobytes())
+    # CPU: the reference's keygen, one key per thread (ctypes drops the GIL)
+    cores = os.cpu_count() or 1
+    threading.stack_size(64 << 20)  # pk_gen keeps its matrix on the stack
+    cpu_seeds = [np.random.default_rng(1000 + i).bytes(32) for i in range(4 * cores)]
+    done, attempts = 0, 0
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        futs = [ex.submit(checker.keypair, sd) for sd in cpu_seeds]
+        for f in futs:
+            _, _, a = f.result()
+            done += 1
+            attempts += a
+            if time.perf_counter() - t0 > cpu_seconds and done >= cores:
+                break
+        for f in futs:
+            f.cancel()
+    cpu_dt = time.perf_counter() - t0
+    threading.stack_size(0)
+    return {"set": set_id, "keys": count, "attempts": int(att.sum()), "seconds": dt,
+            "keypairs_per_s": count / dt, "attempts_per_s": float(att.sum()) / dt, "gpu_launches": launches,
+            "single_key_ms": single_s * 1e3, "single_key_attempts": one[2], "matches_reference": bool(ok),
+            "cpu_baseline": {"keypairs_per_s": done / cpu_dt, "attempts": attempts, "keys": done, "cores": cores,
+                             "kind": "reference" if isinstance(checker, o.RefKeygen) else "port",
+                             "sample": f"{done} seeds on {cores} threads, {cpu_dt:.1f} s"}}
 
 
 def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3) -> dict:
@@ -578,6 +630,8 @@ def main() -> None:
                            "mixed_64keys_2^18": config_mixed(cmd, eng, stream)}
     for g_ in graphs:
         g_.close()
+    if world == 1 and not args.no_keygen:
+        line["keygen"] = keygen_leg(cmd, eng)
     if world == 1 and not args.no_serve:
         fused_rate = value
         rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, round(0.5 * fused_rate, -5)})

@@ -190,6 +190,7 @@ void cmd_engine_destroy(cmd_engine *eng)
     eng->scratch.release(eng);
     eng->io.release(eng);
     eng->fused.release(eng);
+    eng->keygen.release(eng);
     eng->host_scratch.release();
     release_fft_plans(eng);
     for (int i = 0; i < BATCH_STREAMS; i++)

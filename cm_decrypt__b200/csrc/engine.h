@@ -79,6 +79,7 @@ struct cmd_engine {
     cmd::Scratch scratch;          // plain-path intermediates
     cmd::Scratch io;               // device staging for host-buffer calls
     cmd::Scratch fused;            // fused-kernel work lists
+    cmd::Scratch keygen;           // key-generation workspace (kept between calls)
     cmd::HostScratch host_scratch; // pinned staging
     uint32_t *tile_counter = nullptr;
     cudaStream_t piece_stream[cmd::BATCH_STREAMS] = {};  // host-buffer batches, created on first use

@@ -21,8 +21,9 @@
 //                     missing, i.e. the left block is singular)
 //  5. k_kg_controlbits Benes control bits of pi by the cycle-labelling
 //                     recursion (controlbits.c:22-170), all sub-networks of a
-//                     level at once over segmented bitonic sorts, then checked
-//                     by running the network (controlbits.c:180-220)
+//                     level at once; the reference's sorts become the
+//                     permutation inverses and compositions they compute.
+//                     Checked by running the network (controlbits.c:180-220)
 //  6. k_kg_output     pk rows (bytes mt/8 .. of each reduced row,
 //                     pk_gen.c:145-146) and sk = seed | pivots | g | control
 //                     bits | s (operations.c:60-100)
@@ -31,9 +32,9 @@
 // reference's loop does, so a seed yields the reference's key pair.
 //
 // Not constant-time: the GF(2^m) arithmetic uses log/antilog tables in shared
-// memory and the elimination reads the pivot rows it selects, so kernel timing
-// depends on secret values.  The sorts and the control-bit recursion have
-// data-independent access patterns.
+// memory, the elimination reads the pivot rows it selects and the control-bit
+// recursion indexes by permutation values, so kernel timing depends on secret
+// values.  Only the support sort has a data-independent access pattern.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -137,50 +138,58 @@ __device__ void load_tables(const GfTables *g, uint16_t *lg, uint16_t *ex, int q
 }
 
 // ---- 1. seed expansion ----------------------------------------------------
-__global__ void k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work, KgDims d, int K)
+// Key k's attempts j < D fill slots k*D + j: attempt 0 expands the key's seed,
+// attempt j + 1 the last 32 bytes of attempt j's expansion (the seed the
+// reference's loop moves on to after a rejected attempt).  slot_seed keeps
+// each slot's seed for its secret key.
+__global__ void __launch_bounds__(32, 1) k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work,
+                                                     uint8_t *__restrict__ slot_seed, KgDims d, int K, int D)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= K)
         return;
-    const uint8_t *sd = seeds + (size_t)k * 32;
-    uint8_t *r = work + (size_t)k * d.stride + d.off_r;
-    reinterpret_cast<PanelInfo *>(work + (size_t)k * d.stride + d.off_panel)->status = KG_OK;
-    // absorb 64 || seed (33 bytes) in one block with the SHAKE padding
-    uint64_t A[25];
-#pragma unroll
-    for (int i = 0; i < 25; i++)
-        A[i] = 0;
-    uint8_t blk[40];
-    blk[0] = 64;
-    for (int i = 0; i < 32; i++)
-        blk[1 + i] = sd[i];
-    blk[33] = 0x1F;
-    for (int i = 34; i < 40; i++)
-        blk[i] = 0;
-#pragma unroll
-    for (int l = 0; l < 5; l++) {
-        uint64_t v = 0;
-#pragma unroll
-        for (int b = 0; b < 8; b++)
-            v |= (uint64_t)blk[8 * l + b] << (8 * b);
-        A[l] = v;
-    }
-    A[16] ^= 0x8000000000000000ull;  // last byte of the 136-byte block
     constexpr int RATE = 136;
+    for (int j = 0; j < D; j++) {
+        const int slot = k * D + j;
+        const uint8_t *sd = j == 0 ? seeds + (size_t)k * 32 : work + (size_t)(slot - 1) * d.stride + d.off_r + d.rlen - 32;
+        uint8_t *r = work + (size_t)slot * d.stride + d.off_r;
+        reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
+        for (int i = 0; i < 32; i++)
+            slot_seed[(size_t)slot * 32 + i] = sd[i];
+        // absorb 64 || seed (33 bytes) in one block with the SHAKE padding
+        uint64_t A[25];
+#pragma unroll
+        for (int i = 0; i < 25; i++)
+            A[i] = 0;
+        uint8_t blk[40];
+        blk[0] = 64;
+        for (int i = 0; i < 32; i++)
+            blk[1 + i] = sd[i];
+        blk[33] = 0x1F;
+        for (int i = 34; i < 40; i++)
+            blk[i] = 0;
+#pragma unroll
+        for (int l = 0; l < 5; l++) {
+            uint64_t v = 0;
+#pragma unroll
+            for (int b = 0; b < 8; b++)
+                v |= (uint64_t)blk[8 * l + b] << (8 * b);
+            A[l] = v;
+        }
+        A[16] ^= 0x8000000000000000ull;  // last byte of the 136-byte block
 #pragma unroll 1
-    for (int off = 0; off < d.rlen; off += RATE) {
-        keccak_f(A);
-        const int len = min(RATE, d.rlen - off);
+        for (int off = 0; off < d.rlen; off += RATE) {
+            keccak_f(A);
+            const int len = min(RATE, d.rlen - off);
 #pragma unroll
-        for (int l = 0; l < RATE / 8; l++) {
-            const uint64_t v = A[l];
-            if (8 * l + 8 <= len) {
-#pragma unroll
-                for (int b = 0; b < 8; b++)
-                    r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
-            } else if (8 * l < len) {
-                for (int b = 0; b < len - 8 * l; b++)
-                    r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
+            for (int l = 0; l < RATE / 8; l++) {
+                const uint64_t v = A[l];
+                if (8 * l + 8 <= len) {
+                    reinterpret_cast<uint64_t *>(r + off)[l] = v;  // r and off are 8-byte aligned
+                } else if (8 * l < len) {
+                    for (int b = 0; b < len - 8 * l; b++)
+                        r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
+                }
             }
         }
     }
@@ -203,10 +212,10 @@ __host__ __device__ inline ExtPoly ext_poly(int set)
     }
 }
 
-constexpr int GP_THREADS = 256;
+constexpr int GP_THREADS = 1024;
 
 // Shared memory: tables, the t x (t+1) system (row = coordinate, column =
-// power), the current power, the product, the column of multipliers.
+// power), the current power, the product, the first fold, the multipliers.
 size_t genpoly_smem(const KgDims &d)
 {
     return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 3 * 256 * 2 + 256 * 2 + 64;
@@ -222,15 +231,15 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
     uint16_t *pw = A + (size_t)d.t * (d.t + 1);  // 256
     uint16_t *pr = pw + 256;                     // product, 2t - 1 <= 255
     uint16_t *v1 = pr + 256;                     // first fold, t + 10
-    uint16_t *col = v1 + 256;                    // multipliers
+    uint16_t *col = v1 + 256;                    // f, then the multipliers
     __shared__ int s_piv;
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
-    const int tid = threadIdx.x, t = d.t, q1 = d.q - 1, W = t + 1;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = d.t, q1 = d.q - 1, W = t + 1;
     load_tables(tabs, lg, ex, d.q);
     const uint8_t *fr = wk + d.off_r + d.rlen - 32 - 2 * t;
     if (tid < t) {
-        col[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);  // f (col is free until the elimination)
+        col[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);
         pw[tid] = tid == 0 ? 1 : 0;
     }
     __syncthreads();
@@ -239,18 +248,24 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
     for (int u = 0; u < F.nt; u++)
         offmax = max(offmax, F.off[u]);
     // powers f^0 .. f^t into the columns of A
+    const int ko = tid >> 2, part = tid & 3;  // four threads per product coefficient
     for (int c = 0; c <= t; c++) {
         if (tid < t)
             A[tid * W + c] = pw[tid];
         if (c == t)
             break;
         // pr = pw * f (degree <= 2t - 2)
-        if (tid < 2 * t - 1) {
+        {
             uint16_t acc = 0;
-            const int lo = max(0, tid - t + 1), hi = min(tid, t - 1);
-            for (int i = lo; i <= hi; i++)
-                acc ^= gmul(lg, ex, q1, pw[i], col[tid - i]);
-            pr[tid] = acc;
+            if (ko < 2 * t - 1) {
+                const int lo = max(0, ko - t + 1), hi = min(ko, t - 1);
+                for (int i = lo + part; i <= hi; i += 4)
+                    acc ^= gmul(lg, ex, q1, pw[i], col[ko - i]);
+            }
+            acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 1);
+            acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 2);
+            if (part == 0 && ko < 2 * t - 1)
+                pr[ko] = acc;
         }
         __syncthreads();
         // fold y^(t+i) = sum_u c_u y^(i+off_u): twice, the second for the at
@@ -277,14 +292,14 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
         __syncthreads();
     }
     __syncthreads();
-    // Gauss-Jordan: sum_{j<t} g_j f^j = f^t
+    // Gauss-Jordan: sum_{j<t} g_j f^j = f^t.  Warp w updates rows w, w + 32,
+    // ...; lane l columns c + l, c + l + 32, ...
     for (int c = 0; c < t; c++) {
         if (tid == 0)
             s_piv = t;
         __syncthreads();
-        for (int r = c + tid; r < t; r += GP_THREADS)
-            if (A[r * W + c])
-                atomicMin(&s_piv, r);
+        if (tid >= c && tid < t && A[tid * W + c])
+            atomicMin(&s_piv, tid);
         __syncthreads();
         const int piv = s_piv;
         if (piv >= t) {
@@ -292,25 +307,24 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
                 pinfo->status = KG_GENPOLY;
             return;
         }
-        if (piv != c)
-            for (int x = c + tid; x <= t; x += GP_THREADS) {
-                const uint16_t a = A[piv * W + x];
-                A[piv * W + x] = A[c * W + x];
-                A[c * W + x] = a;
-            }
+        if (piv != c && tid >= c && tid <= t) {
+            const uint16_t a = A[piv * W + tid];
+            A[piv * W + tid] = A[c * W + tid];
+            A[c * W + tid] = a;
+        }
         __syncthreads();
         const uint16_t inv = ginv(lg, ex, q1, A[c * W + c]);
         __syncthreads();
-        for (int x = c + tid; x <= t; x += GP_THREADS)
-            A[c * W + x] = gmul(lg, ex, q1, A[c * W + x], inv);
-        for (int r = tid; r < t; r += GP_THREADS)
-            col[r] = r == c ? 0 : A[r * W + c];
+        if (tid >= c && tid <= t)
+            A[c * W + tid] = gmul(lg, ex, q1, A[c * W + tid], inv);
+        if (tid < t)
+            col[tid] = tid == c ? 0 : A[tid * W + c];
         __syncthreads();
-        const int width = t + 1 - c;
-        for (int e = tid; e < t * width; e += GP_THREADS) {
-            const int r = e / width, x = c + e % width;
+        for (int r = warp; r < t; r += GP_THREADS / 32) {
             const uint16_t k = col[r];
-            if (k)
+            if (!k)
+                continue;
+            for (int x = c + lane; x <= t; x += 32)
                 A[r * W + x] ^= gmul(lg, ex, q1, A[c * W + x], k);
         }
         __syncthreads();
@@ -525,13 +539,22 @@ __global__ void k_ge_pivots(uint8_t *__restrict__ work, KgDims d, int p)
     }
 }
 
-constexpr int APPLY_THREADS = 256;
+constexpr int APPLY_THREADS = 1024;
+constexpr int APPLY_ROWS = 384;  // row slots per block
+
+// Shared memory of k_ge_apply: 8 groups x 16 combinations x the active width.
+size_t apply_smem(int width) { return (size_t)8 * 16 * width * 4; }
 
 // Every row slot of the matrix, words p..: window slots take the pivot rows,
-// the others their (possibly moved) row with the panel columns cleared.
+// the others their (possibly moved) row with the panel columns cleared.  The
+// XOR of the pivot rows a row's panel word selects is found four bits at a
+// time in tables of all 16 combinations of four pivot rows (the "four
+// Russians" method), built per block in shared memory.
 __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p)
 {
-    extern __shared__ __align__(16) uint32_t s_pv[];  // npiv x width
+    extern __shared__ __align__(16) uint32_t s_tab[];  // [8][16][width]
+    __shared__ uint32_t s_pw[APPLY_ROWS];
+    __shared__ int16_t s_src[APPLY_ROWS];  // -2 window, -1 own row, else moved row index
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     const PanelInfo *pi = reinterpret_cast<const PanelInfo *>(wk + d.off_panel);
     if (pi->status != KG_OK)
@@ -539,42 +562,61 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
     uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
     const uint32_t *pv = reinterpret_cast<const uint32_t *>(wk + d.off_pv);
     const uint32_t *mv = reinterpret_cast<const uint32_t *>(wk + d.off_mv);
-    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p, c0 = PANEL * p;
+    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p, c0 = PANEL * p, tid = threadIdx.x;
     const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
-    for (int e = threadIdx.x; e < npiv * width; e += APPLY_THREADS)
-        s_pv[e] = pv[(e / width) * d.rw + p + e % width];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t to_l = lane < nmove ? pi->to[lane] : 0xFFFFFFFFu;
-    for (int slot = blockIdx.y * (APPLY_THREADS / 32) + warp; slot < d.mt; slot += gridDim.y * (APPLY_THREADS / 32)) {
-        uint32_t *dst = mat + (size_t)slot * d.rw + p;
+    const int r0 = blockIdx.y * APPLY_ROWS, nrows = min(APPLY_ROWS, d.mt - r0);
+    // tables: tab[g][c][w] = XOR of pivot rows 4g + b for the bits b of c
+    for (int e = tid; e < 8 * width; e += APPLY_THREADS) {
+        const int g = e / width, w = e - g * width;
+        uint32_t v[4];
+#pragma unroll
+        for (int b = 0; b < 4; b++)
+            v[b] = 4 * g + b < npiv ? pv[(4 * g + b) * d.rw + p + w] : 0u;
+        uint32_t *t = s_tab + (size_t)g * 16 * width + w;
+#pragma unroll
+        for (int c = 0; c < 16; c++)
+            t[c * width] = ((c & 1) ? v[0] : 0u) ^ ((c & 2) ? v[1] : 0u) ^ ((c & 4) ? v[2] : 0u) ^ ((c & 8) ? v[3] : 0u);
+    }
+    // each row's panel word and source, read before any row is written
+    for (int t = tid; t < nrows; t += APPLY_THREADS) {
+        const int slot = r0 + t;
+        int src = -1;
         if (slot >= c0 && slot < c0 + npiv) {
-            const uint32_t *src = s_pv + (slot - c0) * width;
-            for (int w = lane; w < width; w += 32)
-                dst[w] = src[w];
-            continue;
+            src = -2;
+        } else {
+            for (int i = 0; i < nmove; i++)
+                if ((int)pi->to[i] == slot)
+                    src = i;
         }
-        const uint32_t hit = __ballot_sync(0xFFFFFFFFu, to_l == (uint32_t)slot);
-        const uint32_t *src = hit ? mv + (__ffs(hit) - 1) * d.rw + p : dst;
-        // the row's panel word, read before any lane overwrites word 0
-        const uint32_t pw = __shfl_sync(0xFFFFFFFFu, lane == 0 ? src[0] : 0u, 0) & pmask;
-        for (int w = lane; w < width; w += 32) {
-            uint32_t acc = src[w], bits = pw;
-            while (bits) {
-                const int b = __ffs(bits) - 1;
-                bits &= bits - 1;
-                acc ^= s_pv[b * width + w];
-            }
-            dst[w] = acc;
+        s_src[t] = (int16_t)src;
+        s_pw[t] = src == -2 ? 0u : (src >= 0 ? mv[src * d.rw + p] : mat[(size_t)slot * d.rw + p]) & pmask;
+    }
+    __syncthreads();
+    // thread (t0, w): word w of rows t0, t0 + 4, ... (a warp shares a row)
+    const int w = tid & 255;
+    if (w >= width)
+        return;
+    for (int t = tid >> 8; t < nrows; t += APPLY_THREADS / 256) {
+        const int slot = r0 + t, src = s_src[t];
+        uint32_t acc;
+        if (src == -2) {
+            acc = pv[(slot - c0) * d.rw + p + w];
+        } else {
+            acc = src >= 0 ? mv[src * d.rw + p + w] : mat[(size_t)slot * d.rw + p + w];
+            const uint32_t x = s_pw[t];
+#pragma unroll
+            for (int g = 0; g < 8; g++)
+                acc ^= s_tab[((size_t)g * 16 + ((x >> (4 * g)) & 15u)) * width + w];
         }
+        mat[(size_t)slot * d.rw + p + w] = acc;
     }
 }
 
 // ---- 5. control bits ----------------------------------------------------------
 constexpr int CB_THREADS = 1024;
-constexpr int CB_PER = KG_MAX_Q / CB_THREADS;  // elements per thread (m = 13)
 
-size_t cbits_smem(const KgDims &d) { return (size_t)d.q * 4 + (size_t)d.q * 2 + (size_t)(d.cond + 3) / 4 * 4; }
+// Six int16 arrays of 2^m entries and the bit array.
+size_t cbits_smem(const KgDims &d) { return (size_t)6 * d.q * 2 + (size_t)(d.cond + 3) / 4 * 4; }
 
 __device__ __forceinline__ uint32_t rev_bits(uint32_t s, int nb) { return nb ? __brev(s) >> (32 - nb) : 0; }
 
@@ -585,181 +627,120 @@ __device__ __forceinline__ void put_bit(uint32_t *bits, long gb, uint32_t v)
         atomicOr(&bits[gb >> 5], 1u << (gb & 31));
 }
 
+// All sub-networks of a recursion level at once: at level lev the 2^lev
+// segments of ns = 2^(m - lev) entries each hold one inner permutation (local
+// values 0..ns-1).  controlbits.c:22-170 reaches each quantity below with
+// constant-time sorts; here each is the permutation inverse or composition
+// that sort performs, by scatter or gather in shared memory.
 __global__ void __launch_bounds__(CB_THREADS) k_kg_controlbits(uint8_t *__restrict__ work, KgDims d)
 {
     extern __shared__ __align__(16) uint8_t sm_cb[];
-    int32_t *A = reinterpret_cast<int32_t *>(sm_cb);       // sort buffer, q entries
-    int16_t *X = reinterpret_cast<int16_t *>(A + d.q);     // exchange buffer
-    uint32_t *bits = reinterpret_cast<uint32_t *>(X + d.q);
+    int16_t *Pa = reinterpret_cast<int16_t *>(sm_cb);  // current permutations
+    int16_t *Ia = Pa + d.q;                             // their inverses
+    int16_t *Ba = Ia + d.q;                             // pibar, later M
+    int16_t *Ca = Ba + d.q;                             // cycle labels c
+    int16_t *Qa = Ca + d.q;                             // pibar^(2^k)
+    int16_t *Ta = Qa + d.q;                             // F(pi(x))
+    uint32_t *bits = reinterpret_cast<uint32_t *>(Ta + d.q);
     __shared__ int s_bad;
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
     if (pinfo->status != KG_OK)
         return;
-    const int tid = threadIdx.x, m = d.m, n = d.q, per = n / CB_THREADS;
+    const int tid = threadIdx.x, m = d.m, n = d.q, half = n / 2;
     const int16_t *pig = reinterpret_cast<const int16_t *>(wk + d.off_pi);
     for (int i = tid; i < (d.cond + 3) / 4; i += CB_THREADS)
         bits[i] = 0;
+    for (int x = tid; x < n; x += CB_THREADS)
+        Pa[x] = pig[x];
     if (tid == 0)
         s_bad = 0;
-    int P[CB_PER];
-#pragma unroll
-    for (int e = 0; e < CB_PER; e++)
-        if (e < per)
-            P[e] = pig[tid + CB_THREADS * e];
-    // element x = tid + CB_THREADS * e; local index lx = x mod ns
+    __syncthreads();
     for (int lev = 0; lev < m - 1; lev++) {
-        const int w = m - lev, ns = n >> lev, half = n / 2;
-        int c[CB_PER], pp[CB_PER], tmp[CB_PER];
-        // (a) pibar(y) = pi(pi^-1(y ^ 1) ^ 1): sort (pi(x)^1, pi(x^1))
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per)
-                X[tid + CB_THREADS * e] = (int16_t)P[e];
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e;
-                A[x] = ((P[e] ^ 1) << 16) | X[x ^ 1];
-            }
-        seg_sort(A, n, w);
-        // c = min(x, pibar(x)); pp = pibar^2 via pibar^-1
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), pb = A[x] & 0xFFFF;
-                c[e] = min(lx, pb);
-                tmp[e] = pb;
-                A[x] = (pb << 16) | lx;
-            }
-        seg_sort(A, n, w);
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e;
-                A[x] = ((A[x] & 0xFFFF) << 16) | tmp[e];  // (pibar^-1(x), pibar(x))
-            }
-        seg_sort(A, n, w);
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per)
-                pp[e] = A[tid + CB_THREADS * e] & 0xFFFF;
-        // w - 2 times: c <- min(c, c o pp), pp <- pp o pp
-        for (int it = 1; it < w - 1; it++) {
-#pragma unroll
-            for (int e = 0; e < CB_PER; e++)
-                if (e < per) {
-                    const int x = tid + CB_THREADS * e;
-                    A[x] = (pp[e] << 16) | (x & (ns - 1));
-                }
-            seg_sort(A, n, w);
-#pragma unroll
-            for (int e = 0; e < CB_PER; e++)
-                if (e < per) {
-                    const int x = tid + CB_THREADS * e;
-                    tmp[e] = A[x] & 0xFFFF;  // pp^-1(x)
-                    A[x] = (tmp[e] << 16) | c[e];
-                }
-            seg_sort(A, n, w);
-#pragma unroll
-            for (int e = 0; e < CB_PER; e++)
-                if (e < per)
-                    c[e] = min(c[e], A[tid + CB_THREADS * e] & 0xFFFF);
-            if (it < w - 2) {
-                __syncthreads();
-#pragma unroll
-                for (int e = 0; e < CB_PER; e++)
-                    if (e < per)
-                        A[tid + CB_THREADS * e] = (tmp[e] << 16) | pp[e];
-                seg_sort(A, n, w);
-#pragma unroll
-                for (int e = 0; e < CB_PER; e++)
-                    if (e < per)
-                        pp[e] = A[tid + CB_THREADS * e] & 0xFFFF;
-            }
+        const int w = m - lev, ns = n >> lev, h = ns / 2;
+        // inverse
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx;
+            Ia[base + Pa[x]] = (int16_t)lx;
         }
-        // first layer: pair j of a segment swaps when c(2j) is odd
         __syncthreads();
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per)
-                X[tid + CB_THREADS * e] = (int16_t)c[e];
+        // pibar(y) = pi(pi^-1(y ^ 1) ^ 1)
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx;
+            Ba[x] = Pa[base + (Ia[base + (lx ^ 1)] ^ 1)];
+        }
         __syncthreads();
-        int F[CB_PER];
+        // c = min(x, pibar(x)); Q = pibar^2
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx, pb = Ba[x];
+            Ca[x] = (int16_t)min(lx, pb);
+            Qa[x] = Ba[base + pb];
+        }
+        __syncthreads();
+        // w - 2 times: c <- min(c, c o Q), Q <- Q o Q
+        for (int it = 1; it < w - 1; it++) {
+            int cn[KG_MAX_Q / CB_THREADS], qn[KG_MAX_Q / CB_THREADS];
 #pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), s = x / ns;
-                const int f = X[x & ~1] & 1;
-                F[e] = lx ^ f;
-                if (!(lx & 1))
-                    put_bit(bits, (long)lev * half + rev_bits(s, lev) + (long)(lx >> 1) * (1 << lev), f);
-                A[x] = (P[e] << 16) | lx;  // for pi^-1
-            }
-        seg_sort(A, n, w);
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
+            for (int e = 0; e < KG_MAX_Q / CB_THREADS; e++) {
                 const int x = tid + CB_THREADS * e;
-                A[x] = ((A[x] & 0xFFFF) << 16) | F[e];  // (pi^-1(x), F(x))
+                if (x < n) {
+                    const int lx = x & (ns - 1), base = x - lx, qx = base + Qa[x];
+                    cn[e] = min((int)Ca[x], (int)Ca[qx]);
+                    qn[e] = Qa[qx];
+                }
             }
-        seg_sort(A, n, w);
-        // last layer: pair k swaps when F(pi(2k)) is odd; M(L(x)) = F(pi(x))
+            __syncthreads();
 #pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
+            for (int e = 0; e < KG_MAX_Q / CB_THREADS; e++) {
                 const int x = tid + CB_THREADS * e;
-                tmp[e] = A[x] & 0xFFFF;  // F(pi(x))
-                X[x] = (int16_t)tmp[e];
+                if (x < n) {
+                    Ca[x] = (int16_t)cn[e];
+                    Qa[x] = (int16_t)qn[e];
+                }
             }
+            __syncthreads();
+        }
+        // first layer: pair j swaps when c(2j) is odd (F); T = F o pi
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx, s = x / ns;
+            if (!(lx & 1))
+                put_bit(bits, (long)lev * half + rev_bits(s, lev) + (long)(lx >> 1) * (1 << lev), Ca[x] & 1);
+            const int px = Pa[x];
+            Ta[x] = (int16_t)(px ^ (Ca[base + (px & ~1)] & 1));
+        }
         __syncthreads();
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), s = x / ns;
-                const int l = X[x & ~1] & 1;
-                if (!(lx & 1))
-                    put_bit(bits,
-                            (long)lev * half + rev_bits(s, lev) + (long)(2 * w - 2) * half + (long)(lx >> 1) * (1 << lev),
-                            l);
-                tmp[e] = ((lx ^ l) << 16) | tmp[e];
-            }
+        // last layer: pair k swaps when T(2k) is odd (L); M(L(x)) = T(x)
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx, s = x / ns;
+            const int l = Ta[base + (lx & ~1)] & 1;
+            if (!(lx & 1))
+                put_bit(bits, (long)lev * half + rev_bits(s, lev) + (long)(2 * w - 2) * half + (long)(lx >> 1) * (1 << lev),
+                        l);
+            Ba[base + (lx ^ l)] = Ta[x];
+        }
         __syncthreads();
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per)
-                A[tid + CB_THREADS * e] = tmp[e];
-        seg_sort(A, n, w);
-        // halves of M become the two inner problems: q0(j) = M(2j)/2 in the
-        // first half of the segment, q1(j) = M(2j+1)/2 in the second
-#pragma unroll
-        for (int e = 0; e < CB_PER; e++)
-            if (e < per) {
-                const int x = tid + CB_THREADS * e, lx = x & (ns - 1), base = x - lx, h = ns / 2;
-                const int src = lx < h ? base + 2 * lx : base + 2 * (lx - h) + 1;
-                P[e] = (A[src] & 0xFFFF) >> 1;
-            }
+        // the two inner problems: M(2j)/2 in the first half, M(2j+1)/2 in the second
+        for (int x = tid; x < n; x += CB_THREADS) {
+            const int lx = x & (ns - 1), base = x - lx;
+            const int src = lx < h ? base + 2 * lx : base + 2 * (lx - h) + 1;
+            Pa[x] = (int16_t)(Ba[src] >> 1);
+        }
+        __syncthreads();
     }
     // w = 1: the pair swaps when pi(0) = 1
-#pragma unroll
-    for (int e = 0; e < CB_PER; e++)
-        if (e < per) {
-            const int x = tid + CB_THREADS * e;
-            if (!(x & 1))
-                put_bit(bits, (long)(m - 1) * (n / 2) + rev_bits(x >> 1, m - 1), P[e] & 1);
-        }
+    for (int x = 2 * tid; x < n; x += 2 * CB_THREADS)
+        put_bit(bits, (long)(m - 1) * half + rev_bits(x >> 1, m - 1), Pa[x] & 1);
     __syncthreads();
     // check: layers 0..m-1 then m-2..0 (stride 2^s) applied to the identity
     // must give pi (controlbits.c:193-212)
+    int16_t *X = Ia;
     for (int i = tid; i < n; i += CB_THREADS)
         X[i] = (int16_t)i;
     for (int layer = 0; layer < 2 * m - 1; layer++) {
         const int sh = layer < m ? layer : 2 * m - 2 - layer;
         __syncthreads();
-        for (int k = tid; k < n / 2; k += CB_THREADS) {
-            const long gb = (long)layer * (n / 2) + k;
+        for (int k = tid; k < half; k += CB_THREADS) {
+            const long gb = (long)layer * half + k;
             const int blk = k >> sh, j = k & ((1 << sh) - 1);
             const int a = blk * (2 << sh) + j, b = a + (1 << sh);
             if ((bits[gb >> 5] >> (gb & 31)) & 1u) {
@@ -783,38 +764,53 @@ __global__ void __launch_bounds__(CB_THREADS) k_kg_controlbits(uint8_t *__restri
 }
 
 // ---- 6. outputs ---------------------------------------------------------------
-// sk = seed | 0xFFFFFFFF as 8 little-endian bytes | g (2t) | control bits | s
-// (operations.c:60-100); pk row r = bytes mt/8 .. of reduced row r.
-__global__ void k_kg_output(const uint8_t *__restrict__ work, const uint8_t *__restrict__ seeds, const int *__restrict__ idx,
-                            uint8_t *__restrict__ pk, uint8_t *__restrict__ sk, KgDims d)
+// For each accepted slot of the list: sk = seed | 0xFFFFFFFF as 8 little-endian
+// bytes | g (2t) | control bits | s (operations.c:60-100) and pk row r =
+// bytes mt/8 .. of reduced row r, into output position i of the list.
+__global__ void k_kg_output(const uint8_t *__restrict__ work, const uint8_t *__restrict__ slot_seed,
+                            const int *__restrict__ slots, uint8_t *__restrict__ pk, uint8_t *__restrict__ sk, KgDims d)
 {
-    const int k = blockIdx.x;
-    const uint8_t *wk = work + (size_t)k * d.stride;
-    if (reinterpret_cast<const PanelInfo *>(wk + d.off_panel)->status != KG_OK)
-        return;
-    const int out = idx[k];
-    uint8_t *skp = sk + (size_t)out * d.sk;
+    const int i = blockIdx.x, slot = slots[i];
+    const uint8_t *wk = work + (size_t)slot * d.stride;
+    uint8_t *skp = sk + (size_t)i * d.sk;
     const int off_irr = 40, off_cond = 40 + 2 * d.t, off_s = off_cond + d.cond;
-    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < d.sk; i += gridDim.y * blockDim.x) {
+    for (int x = blockIdx.y * blockDim.x + threadIdx.x; x < d.sk; x += gridDim.y * blockDim.x) {
         uint8_t v;
-        if (i < 32)
-            v = seeds[(size_t)k * 32 + i];
-        else if (i < 40)
-            v = i < 36 ? 0xFF : 0;
-        else if (i < off_cond)
-            v = wk[d.off_irr + (i - off_irr)];
-        else if (i < off_s)
-            v = wk[d.off_cond + (i - off_cond)];
+        if (x < 32)
+            v = slot_seed[(size_t)slot * 32 + x];
+        else if (x < 40)
+            v = x < 36 ? 0xFF : 0;
+        else if (x < off_cond)
+            v = wk[d.off_irr + (x - off_irr)];
+        else if (x < off_s)
+            v = wk[d.off_cond + (x - off_cond)];
         else
-            v = wk[d.off_r + (i - off_s)];
-        skp[i] = v;
+            v = wk[d.off_r + (x - off_s)];
+        skp[x] = v;
     }
     const uint8_t *mat = wk + d.off_mat;
-    uint8_t *pkp = pk + (size_t)out * d.mt * d.pk_row;
+    uint8_t *pkp = pk + (size_t)i * d.mt * d.pk_row;
     const size_t total = (size_t)d.mt * d.pk_row;
     for (size_t e = (size_t)blockIdx.y * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.y * blockDim.x) {
         const int r = (int)(e / d.pk_row), b = (int)(e % d.pk_row);
         pkp[e] = mat[(size_t)r * d.rw * 4 + d.mt / 8 + b];
+    }
+}
+
+// Status and next seed of every key of the round, packed for one copy.
+__global__ void k_kg_collect(const uint8_t *__restrict__ work, KgDims d, int K, uint8_t *__restrict__ out)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < K * 9; e += gridDim.x * blockDim.x) {
+        const int k = e / 9, w = e % 9;
+        const uint8_t *wk = work + (size_t)k * d.stride;
+        uint32_t v;
+        if (w == 0) {
+            v = (uint32_t)reinterpret_cast<const PanelInfo *>(wk + d.off_panel)->status;
+        } else {
+            const uint8_t *sd = wk + d.off_r + d.rlen - 32 + 4 * (w - 1);
+            v = sd[0] | (sd[1] << 8) | (sd[2] << 16) | ((uint32_t)sd[3] << 24);
+        }
+        reinterpret_cast<uint32_t *>(out)[e] = v;
     }
 }
 
@@ -885,127 +881,129 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     cudaSetDevice(eng->device);
     const KgDims d = kg_dims(set);
     const size_t pk_bytes = (size_t)d.mt * d.pk_row;
-    // workspace for up to `chunk` keys at once, within the budget
-    size_t chunk = std::min<size_t>(count, 256);
-    const size_t fixed = sizeof(GfTables) + 256;
-    auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 4 + pk_bytes + d.sk); };
-    while (chunk > 1 && !budget_take(eng, need(chunk)))
-        chunk /= 2;
-    if (chunk == 1 && !budget_take(eng, need(1))) {
-        set_last_error("key generation workspace exceeds the engine HBM budget");
+    // Attempt slots per round: about two support CTAs per SM; up to
+    // SPEC attempts of one key run side by side (the reference's retries
+    // of a key form a fixed chain of seeds, so later attempts can start
+    // before earlier ones are judged; the first accepted one is kept).
+    constexpr int SPEC = 4;
+    size_t cap = (size_t)std::max(32, 2 * eng->num_sms);
+    const size_t fixed = sizeof(GfTables) + 1024;
+    // per slot: workspace, seed, key seed, collect record, list entry, one pk and sk
+    auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 32 + 36 + 4 + pk_bytes + d.sk); };
+    while (cap > 1 && eng->keygen.reserve(eng, need(cap)) != CMD_OK)
+        cap /= 2;
+    if (cap == 1 && eng->keygen.reserve(eng, need(1)) != CMD_OK)
         return CMD_E_BUDGET;
-    }
-    const size_t bytes = need(chunk);
-    uint8_t *mem = nullptr;
-    cudaError_t e = cudaMalloc(&mem, bytes);
-    if (e != cudaSuccess) {
-        budget_give(eng, bytes);
-        return cuda_fail(e, "keygen workspace");
-    }
+    uint8_t *mem = static_cast<uint8_t *>(eng->keygen.ptr);
     uint8_t *d_work = mem;
-    uint8_t *d_seed = d_work + chunk * d.stride;
-    int *d_idx = reinterpret_cast<int *>(d_seed + chunk * 32);
-    uint8_t *d_pk = reinterpret_cast<uint8_t *>(d_idx + chunk);
-    uint8_t *d_sk = d_pk + chunk * pk_bytes;
-    GfTables *d_tab = reinterpret_cast<GfTables *>(d_sk + chunk * d.sk);
-    d_tab = reinterpret_cast<GfTables *>((reinterpret_cast<uintptr_t>(d_tab) + 255) / 256 * 256);
+    uint8_t *d_slot_seed = d_work + cap * d.stride;
+    uint8_t *d_key_seed = d_slot_seed + cap * 32;
+    uint32_t *d_col = reinterpret_cast<uint32_t *>(d_key_seed + cap * 32);  // 9 words a slot
+    int *d_list = reinterpret_cast<int *>(d_col + cap * 9);
+    uint8_t *d_pk = reinterpret_cast<uint8_t *>(d_list + cap);
+    uint8_t *d_sk = d_pk + cap * pk_bytes;
+    GfTables *d_tab = reinterpret_cast<GfTables *>((reinterpret_cast<uintptr_t>(d_sk + cap * d.sk) + 255) / 256 * 256);
     cudaStream_t s = eng->stream;
     LaunchCounter lc{&eng->launches};
     int rc = CMD_OK;
     const size_t smem_gp = genpoly_smem(d), smem_sup = support_smem(d), smem_cb = cbits_smem(d);
-    const size_t smem_apply = (size_t)PANEL * d.rw * 4;
+    const size_t smem_apply = apply_smem(d.rw);
     if ((rc = set_smem_attr((const void *)k_kg_genpoly, smem_gp)) || (rc = set_smem_attr((const void *)k_kg_support, smem_sup)) ||
         (rc = set_smem_attr((const void *)k_kg_controlbits, smem_cb)) ||
-        (rc = set_smem_attr((const void *)k_ge_apply, smem_apply))) {
-        cudaFree(mem);
-        budget_give(eng, bytes);
+        (rc = set_smem_attr((const void *)k_ge_apply, smem_apply)))
         return rc;
-    }
-    e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
     // keys still to finish: their output index and current seed
     std::vector<int> pend(count);
     std::vector<uint8_t> seeds(h_seeds, h_seeds + 32 * count);
-    for (size_t i = 0; i < count; i++) {
+    std::vector<uint32_t> tries(count, 0);
+    for (size_t i = 0; i < count; i++)
         pend[i] = (int)i;
-        if (h_attempts)
-            h_attempts[i] = 0;
-    }
-    std::vector<int> status;
-    std::vector<uint8_t> nxt;
-    std::vector<uint8_t> cur_seed;
-    for (uint32_t round = 0; round < max_attempts && !pend.empty() && e == cudaSuccess; round++) {
+    std::vector<uint32_t> col;
+    std::vector<uint8_t> key_seed;
+    std::vector<int> list, list_out;
+    while (!pend.empty() && e == cudaSuccess && rc == CMD_OK) {
         std::vector<int> still;
-        for (size_t base = 0; base < pend.size() && e == cudaSuccess; base += chunk) {
-            const int K = (int)std::min(chunk, pend.size() - base);
-            cur_seed.resize((size_t)K * 32);
-            std::vector<int> idx(K);
-            for (int k = 0; k < K; k++) {
-                idx[k] = k;
-                memcpy(&cur_seed[(size_t)k * 32], &seeds[(size_t)pend[base + k] * 32], 32);
-            }
-            if ((e = cudaMemcpyAsync(d_seed, cur_seed.data(), (size_t)K * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(d_idx, idx.data(), (size_t)K * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        const size_t keys_per_chunk = std::min(pend.size(), cap);
+        const int D = (int)std::max<size_t>(1, std::min<size_t>(SPEC, cap / keys_per_chunk));
+        for (size_t base = 0; base < pend.size() && e == cudaSuccess && rc == CMD_OK; base += keys_per_chunk) {
+            const int K = (int)std::min(keys_per_chunk, pend.size() - base), S = K * D;
+            key_seed.resize((size_t)K * 32);
+            for (int k = 0; k < K; k++)
+                memcpy(&key_seed[(size_t)k * 32], &seeds[(size_t)pend[base + k] * 32], 32);
+            if ((e = cudaMemcpyAsync(d_key_seed, key_seed.data(), (size_t)K * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess)
                 break;
-            k_kg_expand<<<(K + 31) / 32, 32, 0, s>>>(d_seed, d_work, d, K);
-            k_kg_genpoly<<<K, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
-            k_kg_support<<<K, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
+            k_kg_expand<<<(K + 31) / 32, 32, 0, s>>>(d_key_seed, d_work, d_slot_seed, d, K, D);
+            k_kg_genpoly<<<S, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
+            k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
-            const int gy = std::max(1, std::min(64, 2 * eng->num_sms / K));
+            const int gy = (d.mt + APPLY_ROWS - 1) / APPLY_ROWS;
             for (int p = 0; p < npanels; p++) {
-                k_ge_panel<<<K, PANEL_THREADS, 0, s>>>(d_work, d, p);
-                k_ge_pivots<<<dim3(K, 8), 256, 0, s>>>(d_work, d, p);
-                k_ge_apply<<<dim3(K, gy), APPLY_THREADS, (size_t)PANEL * (d.rw - p) * 4, s>>>(d_work, d, p);
+                k_ge_panel<<<S, PANEL_THREADS, 0, s>>>(d_work, d, p);
+                k_ge_pivots<<<dim3(S, 8), 256, 0, s>>>(d_work, d, p);
+                k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - p), s>>>(d_work, d, p);
             }
-            k_kg_controlbits<<<K, CB_THREADS, smem_cb, s>>>(d_work, d);
-            k_kg_output<<<dim3(K, 16), 256, 0, s>>>(d_work, d_seed, d_idx, d_pk, d_sk, d);
+            k_kg_controlbits<<<S, CB_THREADS, smem_cb, s>>>(d_work, d);
+            k_kg_collect<<<(S * 9 + 255) / 256, 256, 0, s>>>(d_work, d, S, reinterpret_cast<uint8_t *>(d_col));
             lc.bump(5 + 3 * (uint64_t)npanels);
-            if ((e = cudaGetLastError()) != cudaSuccess)
+            col.resize((size_t)S * 9);
+            if ((e = cudaGetLastError()) != cudaSuccess ||
+                (e = cudaMemcpyAsync(col.data(), d_col, (size_t)S * 36, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(s)) != cudaSuccess)
                 break;
-            // statuses and next seeds
-            status.resize(K);
-            nxt.resize((size_t)K * 32);
-            for (int k = 0; k < K && e == cudaSuccess; k++) {
-                e = cudaMemcpyAsync(&status[k], d_work + (size_t)k * d.stride + d.off_panel, 4, cudaMemcpyDeviceToHost, s);
-                if (e == cudaSuccess)
-                    e = cudaMemcpyAsync(&nxt[(size_t)k * 32], d_work + (size_t)k * d.stride + d.off_r + d.rlen - 32, 32,
-                                        cudaMemcpyDeviceToHost, s);
+            // per key: the first attempt that is accepted (or fails its
+            // self-check) ends it; otherwise it continues after its last slot
+            list.clear();
+            list_out.clear();
+            for (int k = 0; k < K; k++) {
+                const int out = pend[base + k];
+                int j = 0;
+                while (j < D && (int)col[(size_t)(k * D + j) * 9] != KG_OK && (int)col[(size_t)(k * D + j) * 9] != KG_CBITS)
+                    j++;
+                if (j == D) {
+                    tries[out] += D;
+                    memcpy(&seeds[(size_t)out * 32], &col[(size_t)(k * D + D - 1) * 9 + 1], 32);
+                    if (tries[out] < max_attempts) {
+                        still.push_back(out);
+                    } else {
+                        rc = CMD_E_KEYGEN;
+                        set_last_error("key generation: attempt limit reached");
+                    }
+                    continue;
+                }
+                tries[out] += j + 1;
+                if ((int)col[(size_t)(k * D + j) * 9] == KG_CBITS) {
+                    rc = CMD_E_KEYGEN;
+                    set_last_error("key generation: control bits do not reproduce the permutation");
+                    continue;
+                }
+                list.push_back(k * D + j);
+                list_out.push_back(out);
+            }
+            if (list.empty())
+                continue;
+            const int nl = (int)list.size();
+            if ((e = cudaMemcpyAsync(d_list, list.data(), (size_t)nl * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                break;
+            k_kg_output<<<dim3(nl, 16), 256, 0, s>>>(d_work, d_slot_seed, d_list, d_pk, d_sk, d);
+            lc.bump();
+            for (int i = 0; i < nl && e == cudaSuccess; i++) {
+                const int out = list_out[i];
+                if ((e = cudaMemcpyAsync(h_pk + (size_t)out * pk_bytes, d_pk + (size_t)i * pk_bytes, pk_bytes,
+                                         cudaMemcpyDeviceToHost, s)) == cudaSuccess)
+                    e = cudaMemcpyAsync(h_sk + (size_t)out * d.sk, d_sk + (size_t)i * d.sk, d.sk, cudaMemcpyDeviceToHost, s);
             }
             if (e == cudaSuccess)
                 e = cudaStreamSynchronize(s);
-            if (e != cudaSuccess)
-                break;
-            for (int k = 0; k < K; k++) {
-                const int out = pend[base + k];
-                if (h_attempts)
-                    h_attempts[out]++;
-                if (status[k] == KG_OK) {
-                    if ((e = cudaMemcpy(h_pk + (size_t)out * pk_bytes, d_pk + (size_t)k * pk_bytes, pk_bytes,
-                                        cudaMemcpyDeviceToHost)) != cudaSuccess ||
-                        (e = cudaMemcpy(h_sk + (size_t)out * d.sk, d_sk + (size_t)k * d.sk, d.sk, cudaMemcpyDeviceToHost)) !=
-                            cudaSuccess)
-                        break;
-                } else if (status[k] == KG_CBITS) {
-                    rc = CMD_E_KEYGEN;
-                    set_last_error("key generation: control bits do not reproduce the permutation");
-                } else {
-                    memcpy(&seeds[(size_t)out * 32], &nxt[(size_t)k * 32], 32);
-                    still.push_back(out);
-                }
-            }
         }
         pend.swap(still);
     }
-    cudaFree(mem);
-    budget_give(eng, bytes);
+    if (h_attempts)
+        for (size_t i = 0; i < count; i++)
+            h_attempts[i] = tries[i];
     if (e != cudaSuccess)
         return cuda_fail(e, "key generation");
-    if (rc)
-        return rc;
-    if (!pend.empty()) {
-        set_last_error("key generation: attempt limit reached");
-        return CMD_E_KEYGEN;
-    }
-    return CMD_OK;
+    return rc;
 }
 
 int cmd_kem_keypair(cmd_engine *eng, cmd_set set, const uint8_t *h_seed, uint8_t *h_pk, uint8_t *h_sk,

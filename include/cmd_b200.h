@@ -326,7 +326,10 @@ int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *
 int cmd_kem_keypair(cmd_engine *eng, cmd_set set, const uint8_t *h_seed, uint8_t *h_pk,
                     uint8_t *h_sk, uint32_t *attempts);
 /* count (1..4096) seeds of 32 bytes: key pairs in pk/sk rows of the sizes
- * above; attempts[i] per key (may be NULL); max_attempts 0 = 1000. */
+ * above; attempts[i] per key (may be NULL).  Up to four consecutive attempts
+ * of a key run side by side and the first accepted one is kept, so results
+ * and attempt counts are those of the sequential loop.  A key is given up
+ * (CMD_E_KEYGEN) once at least max_attempts (0 = 1000) have failed. */
 int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, size_t count,
                           uint8_t *h_pk, uint8_t *h_sk, uint32_t *attempts, uint32_t max_attempts);
 
