@@ -138,60 +138,101 @@ __device__ void load_tables(const GfTables *g, uint16_t *lg, uint16_t *ex, int q
 }
 
 // ---- 1. seed expansion ----------------------------------------------------
+// Keccak-f[1600] with one state lane per thread of a warp (lane i = x + 5y,
+// threads 25..31 idle): theta's column parities, pi's lane moves and chi's
+// row neighbours by warp shuffles, rho's rotation per thread.
+struct WarpKeccak {
+    int x, y, src, rho;  // this thread's lane; the lane pi moves here and its rho offset
+    __device__ WarpKeccak(int lane)
+    {
+        const int l = lane < 25 ? lane : 0;
+        x = l % 5;
+        y = l / 5;
+        // B[y, 2x + 3y] = A[x, y]: this position (X, Y) = (x, y) takes lane
+        // (x0, y0) with y0 = X and 2 x0 + 3 y0 = Y (mod 5), so x0 = 3 (Y - 3 X)
+        const int y0 = x, x0 = (3 * (((y - 3 * x) % 5 + 5) % 5)) % 5;
+        src = x0 + 5 * y0;
+        rho = keccak_rot(x0, y0);
+    }
+    __device__ uint64_t permute(uint64_t a) const
+    {
+        const unsigned F = 0xFFFFFFFFu;
+#pragma unroll 1
+        for (int round = 0; round < 24; round++) {
+            // theta: threads x (y = 0) form the parity of column x
+            uint64_t c = a;
+#pragma unroll
+            for (int k = 1; k < 5; k++)
+                c ^= __shfl_sync(F, a, x + 5 * ((y + k) % 5));
+            const uint64_t cm = __shfl_sync(F, c, (x + 4) % 5), cp = __shfl_sync(F, c, (x + 1) % 5);
+            a ^= cm ^ rotl64(cp, 1);
+            // rho and pi
+            const uint64_t b = rotl64(__shfl_sync(F, a, src), rho);
+            // chi along the row
+            const uint64_t b1 = __shfl_sync(F, b, (x + 1) % 5 + 5 * y), b2 = __shfl_sync(F, b, (x + 2) % 5 + 5 * y);
+            a = b ^ (~b1 & b2);
+            if (x == 0 && y == 0)
+                a ^= kRC[round];
+        }
+        return a;
+    }
+};
+
 // Key k's attempts j < D fill slots k*D + j: attempt 0 expands the key's seed,
 // attempt j + 1 the last 32 bytes of attempt j's expansion (the seed the
 // reference's loop moves on to after a rejected attempt).  slot_seed keeps
-// each slot's seed for its secret key.
-__global__ void __launch_bounds__(32, 1) k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work,
-                                                     uint8_t *__restrict__ slot_seed, KgDims d, int K, int D)
+// each slot's seed for its secret key.  One warp per key.
+__global__ void __launch_bounds__(32) k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work,
+                                                  uint8_t *__restrict__ slot_seed, KgDims d, int K, int D)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.x, lane = threadIdx.x;
     if (k >= K)
         return;
     constexpr int RATE = 136;
+    const WarpKeccak kc(lane);
     for (int j = 0; j < D; j++) {
         const int slot = k * D + j;
         const uint8_t *sd = j == 0 ? seeds + (size_t)k * 32 : work + (size_t)(slot - 1) * d.stride + d.off_r + d.rlen - 32;
         uint8_t *r = work + (size_t)slot * d.stride + d.off_r;
-        reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
-        for (int i = 0; i < 32; i++)
-            slot_seed[(size_t)slot * 32 + i] = sd[i];
-        // absorb 64 || seed (33 bytes) in one block with the SHAKE padding
-        uint64_t A[25];
+        if (lane == 0)
+            reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
+        uint8_t sb = lane < 32 ? sd[lane] : 0;
+        slot_seed[(size_t)slot * 32 + lane] = sb;
+        // absorb 64 || seed || 0x1F, pad to 136 bytes with 0x80 at the end:
+        // block byte i is 64 (i = 0), seed[i - 1] (1..32), 0x1F (33)
+        uint64_t a = 0;
+        if (lane < 5) {
 #pragma unroll
-        for (int i = 0; i < 25; i++)
-            A[i] = 0;
-        uint8_t blk[40];
-        blk[0] = 64;
-        for (int i = 0; i < 32; i++)
-            blk[1 + i] = sd[i];
-        blk[33] = 0x1F;
-        for (int i = 34; i < 40; i++)
-            blk[i] = 0;
-#pragma unroll
-        for (int l = 0; l < 5; l++) {
-            uint64_t v = 0;
-#pragma unroll
-            for (int b = 0; b < 8; b++)
-                v |= (uint64_t)blk[8 * l + b] << (8 * b);
-            A[l] = v;
+            for (int b = 0; b < 8; b++) {
+                const int i = 8 * lane + b;
+                uint32_t v = 0;
+                if (i == 0)
+                    v = 64;
+                else if (i <= 32)
+                    v = sd[i - 1];
+                else if (i == 33)
+                    v = 0x1F;
+                a |= (uint64_t)v << (8 * b);
+            }
         }
-        A[16] ^= 0x8000000000000000ull;  // last byte of the 136-byte block
+        if (lane == 16)
+            a ^= 0x8000000000000000ull;
+        if (lane >= 25)
+            a = 0;
 #pragma unroll 1
         for (int off = 0; off < d.rlen; off += RATE) {
-            keccak_f(A);
+            a = kc.permute(a);
             const int len = min(RATE, d.rlen - off);
-#pragma unroll
-            for (int l = 0; l < RATE / 8; l++) {
-                const uint64_t v = A[l];
-                if (8 * l + 8 <= len) {
-                    reinterpret_cast<uint64_t *>(r + off)[l] = v;  // r and off are 8-byte aligned
-                } else if (8 * l < len) {
-                    for (int b = 0; b < len - 8 * l; b++)
-                        r[off + 8 * l + b] = (uint8_t)(v >> (8 * b));
+            if (lane < RATE / 8) {
+                if (8 * lane + 8 <= len) {
+                    reinterpret_cast<uint64_t *>(r + off)[lane] = a;  // r and off are 8-byte aligned
+                } else if (8 * lane < len) {
+                    for (int b = 0; b < len - 8 * lane; b++)
+                        r[off + 8 * lane + b] = (uint8_t)(a >> (8 * b));
                 }
             }
         }
+        __syncwarp();  // the next attempt reads this one's last 32 bytes
     }
 }
 
@@ -933,7 +974,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
                 memcpy(&key_seed[(size_t)k * 32], &seeds[(size_t)pend[base + k] * 32], 32);
             if ((e = cudaMemcpyAsync(d_key_seed, key_seed.data(), (size_t)K * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess)
                 break;
-            k_kg_expand<<<(K + 31) / 32, 32, 0, s>>>(d_key_seed, d_work, d_slot_seed, d, K, D);
+            k_kg_expand<<<K, 32, 0, s>>>(d_key_seed, d_work, d_slot_seed, d, K, D);
             k_kg_genpoly<<<S, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
             k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
