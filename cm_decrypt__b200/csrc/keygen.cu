@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_ge_panel(uint8_t *__restrict_
     }
 }
 
-// Reduced pivot rows PV[b] and copies MV[i] of the rows that move, words p..
+// Reduced pivot rows PV[b] and copies MV[i] of the rows that move, words p & ~3 ..
 __global__ void k_ge_pivots(uint8_t *__restrict__ work, KgDims d, int p)
 {
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
@@ -561,10 +561,11 @@ __global__ void k_ge_pivots(uint8_t *__restrict__ work, KgDims d, int p)
         return;
     const uint32_t *mat = reinterpret_cast<const uint32_t *>(wk + d.off_mat);
     uint32_t *pv = reinterpret_cast<uint32_t *>(wk + d.off_pv), *mv = reinterpret_cast<uint32_t *>(wk + d.off_mv);
-    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p;
+    // words from p & ~3: the update works on 16-byte columns
+    const int p4 = p & ~3, npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p4;
     const int items = (npiv + nmove) * width;
     for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < items; e += gridDim.y * blockDim.x) {
-        const int row = e / width, w = p + e % width;
+        const int row = e / width, w = p4 + e % width;
         if (row < npiv) {
             uint32_t acc = 0, T = pi->T[row];
             while (T) {
@@ -586,14 +587,16 @@ constexpr int APPLY_ROWS = 384;  // row slots per block
 // Shared memory of k_ge_apply: 8 groups x 16 combinations x the active width.
 size_t apply_smem(int width) { return (size_t)8 * 16 * width * 4; }
 
-// Every row slot of the matrix, words p..: window slots take the pivot rows,
-// the others their (possibly moved) row with the panel columns cleared.  The
-// XOR of the pivot rows a row's panel word selects is found four bits at a
-// time in tables of all 16 combinations of four pivot rows (the "four
-// Russians" method), built per block in shared memory.
+// Every row slot of the matrix, words p4 = p & ~3 ..: window slots take the
+// pivot rows, the others their (possibly moved) row with the panel columns
+// cleared.  The XOR of the pivot rows a row's panel word selects is found
+// four bits at a time in tables of all 16 combinations of four pivot rows
+// (the "four Russians" method), built per block in shared memory.  Each
+// thread carries four consecutive words (16-byte loads, stores and table
+// reads); words p4 .. p - 1 are zero in every pivot and moved row.
 __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p)
 {
-    extern __shared__ __align__(16) uint32_t s_tab[];  // [8][16][width]
+    extern __shared__ __align__(16) uint4 s_tab4[];  // [8][16][W4]
     __shared__ uint32_t s_pw[APPLY_ROWS];
     __shared__ int16_t s_src[APPLY_ROWS];  // -2 window, -1 own row, else moved row index
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
@@ -603,20 +606,32 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
     uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
     const uint32_t *pv = reinterpret_cast<const uint32_t *>(wk + d.off_pv);
     const uint32_t *mv = reinterpret_cast<const uint32_t *>(wk + d.off_mv);
-    const int npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p, c0 = PANEL * p, tid = threadIdx.x;
+    const int npiv = pi->npiv, nmove = pi->nmove, p4 = p & ~3, W4 = (d.rw - p4) / 4, c0 = PANEL * p, tid = threadIdx.x;
+    const int rw4 = d.rw / 4;
     const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
     const int r0 = blockIdx.y * APPLY_ROWS, nrows = min(APPLY_ROWS, d.mt - r0);
-    // tables: tab[g][c][w] = XOR of pivot rows 4g + b for the bits b of c
-    for (int e = tid; e < 8 * width; e += APPLY_THREADS) {
-        const int g = e / width, w = e - g * width;
-        uint32_t v[4];
+    // tables: tab[g][c][w4] = XOR of pivot rows 4g + b for the bits b of c
+    const uint4 *pv4 = reinterpret_cast<const uint4 *>(pv + p4);
+    for (int e = tid; e < 8 * W4; e += APPLY_THREADS) {
+        const int g = e / W4, w4 = e - g * W4;
+        uint4 v[4];
 #pragma unroll
         for (int b = 0; b < 4; b++)
-            v[b] = 4 * g + b < npiv ? pv[(4 * g + b) * d.rw + p + w] : 0u;
-        uint32_t *t = s_tab + (size_t)g * 16 * width + w;
+            v[b] = 4 * g + b < npiv ? pv4[(4 * g + b) * rw4 + w4] : make_uint4(0, 0, 0, 0);
+        uint4 *t = s_tab4 + g * 16 * W4 + w4;
 #pragma unroll
-        for (int c = 0; c < 16; c++)
-            t[c * width] = ((c & 1) ? v[0] : 0u) ^ ((c & 2) ? v[1] : 0u) ^ ((c & 4) ? v[2] : 0u) ^ ((c & 8) ? v[3] : 0u);
+        for (int c = 0; c < 16; c++) {
+            uint4 x = make_uint4(0, 0, 0, 0);
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+                if (c & (1 << b)) {
+                    x.x ^= v[b].x;
+                    x.y ^= v[b].y;
+                    x.z ^= v[b].z;
+                    x.w ^= v[b].w;
+                }
+            t[c * W4] = x;
+        }
     }
     // each row's panel word and source, read before any row is written
     for (int t = tid; t < nrows; t += APPLY_THREADS) {
@@ -633,23 +648,32 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
         s_pw[t] = src == -2 ? 0u : (src >= 0 ? mv[src * d.rw + p] : mat[(size_t)slot * d.rw + p]) & pmask;
     }
     __syncthreads();
-    // thread (t0, w): word w of rows t0, t0 + 4, ... (a warp shares a row)
-    const int w = tid & 255;
-    if (w >= width)
+    // thread (t0, w4): 16-byte column w4 of rows t0, t0 + 16, ...
+    const int w4 = tid & 63;
+    if (w4 >= W4)
         return;
-    for (int t = tid >> 8; t < nrows; t += APPLY_THREADS / 256) {
+    uint4 *col = reinterpret_cast<uint4 *>(mat + p4) + w4;  // row r: col[r * rw4]
+    const uint4 *pcol = pv4 + w4, *mcol = reinterpret_cast<const uint4 *>(mv + p4) + w4;
+    const uint4 *tg = s_tab4 + w4;  // table g, combination c: tg[(16 g + c) * W4]
+    constexpr int STEP = APPLY_THREADS / 64;
+    for (int t = tid >> 6; t < nrows; t += STEP) {
         const int slot = r0 + t, src = s_src[t];
-        uint32_t acc;
+        uint4 acc;
         if (src == -2) {
-            acc = pv[(slot - c0) * d.rw + p + w];
+            acc = pcol[(slot - c0) * rw4];
         } else {
-            acc = src >= 0 ? mv[src * d.rw + p + w] : mat[(size_t)slot * d.rw + p + w];
+            acc = src >= 0 ? mcol[src * rw4] : col[slot * rw4];
             const uint32_t x = s_pw[t];
 #pragma unroll
-            for (int g = 0; g < 8; g++)
-                acc ^= s_tab[((size_t)g * 16 + ((x >> (4 * g)) & 15u)) * width + w];
+            for (int g = 0; g < 8; g++) {
+                const uint4 v = tg[(16 * g + (int)((x >> (4 * g)) & 15u)) * W4];
+                acc.x ^= v.x;
+                acc.y ^= v.y;
+                acc.z ^= v.z;
+                acc.w ^= v.w;
+            }
         }
-        mat[(size_t)slot * d.rw + p + w] = acc;
+        col[slot * rw4] = acc;
     }
 }
 
@@ -982,7 +1006,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             for (int p = 0; p < npanels; p++) {
                 k_ge_panel<<<S, PANEL_THREADS, 0, s>>>(d_work, d, p);
                 k_ge_pivots<<<dim3(S, 8), 256, 0, s>>>(d_work, d, p);
-                k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - p), s>>>(d_work, d, p);
+                k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - (p & ~3)), s>>>(d_work, d, p);
             }
             k_kg_controlbits<<<S, CB_THREADS, smem_cb, s>>>(d_work, d);
             k_kg_collect<<<(S * 9 + 255) / 256, 256, 0, s>>>(d_work, d, S, reinterpret_cast<uint8_t *>(d_col));
