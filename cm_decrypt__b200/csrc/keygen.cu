@@ -655,25 +655,35 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
     uint4 *col = reinterpret_cast<uint4 *>(mat + p4) + w4;  // row r: col[r * rw4]
     const uint4 *pcol = pv4 + w4, *mcol = reinterpret_cast<const uint4 *>(mv + p4) + w4;
     const uint4 *tg = s_tab4 + w4;  // table g, combination c: tg[(16 g + c) * W4]
-    constexpr int STEP = APPLY_THREADS / 64;
-    for (int t = tid >> 6; t < nrows; t += STEP) {
-        const int slot = r0 + t, src = s_src[t];
-        uint4 acc;
-        if (src == -2) {
-            acc = pcol[(slot - c0) * rw4];
-        } else {
-            acc = src >= 0 ? mcol[src * rw4] : col[slot * rw4];
-            const uint32_t x = s_pw[t];
+    constexpr int STEP = APPLY_THREADS / 64, U = 2;  // two rows in flight per thread
+    for (int t = tid >> 6; t < nrows; t += U * STEP) {
+        uint4 acc[U];
 #pragma unroll
-            for (int g = 0; g < 8; g++) {
-                const uint4 v = tg[(16 * g + (int)((x >> (4 * g)) & 15u)) * W4];
-                acc.x ^= v.x;
-                acc.y ^= v.y;
-                acc.z ^= v.z;
-                acc.w ^= v.w;
+        for (int u = 0; u < U; u++) {
+            const int tu = t + u * STEP;
+            if (tu < nrows) {
+                const int slot = r0 + tu, src = s_src[tu];
+                acc[u] = src == -2 ? pcol[(slot - c0) * rw4] : (src >= 0 ? mcol[src * rw4] : col[slot * rw4]);
             }
         }
-        col[slot * rw4] = acc;
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int tu = t + u * STEP;
+            if (tu >= nrows)
+                continue;
+            if (s_src[tu] != -2) {
+                const uint32_t x = s_pw[tu];
+#pragma unroll
+                for (int g = 0; g < 8; g++) {
+                    const uint4 v = tg[(16 * g + (int)((x >> (4 * g)) & 15u)) * W4];
+                    acc[u].x ^= v.x;
+                    acc[u].y ^= v.y;
+                    acc[u].z ^= v.z;
+                    acc[u].w ^= v.w;
+                }
+            }
+            col[(r0 + tu) * rw4] = acc[u];
+        }
     }
 }
 
