@@ -63,6 +63,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--serve-keys", type=int, default=1024)
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--no-keygen", action="store_true", help="skip the key-generation leg")
+    ap.add_argument("--keygen-only", action="store_true",
+                    help="run only the key-generation leg and print its JSON (for profiling)")
+    ap.add_argument("--keygen-count", type=int, default=64, help="seeds in the key-generation batch")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the all-sets (2^20 each) and mixed-batch (2^18) measurements")
     return ap.parse_args()
@@ -309,6 +312,11 @@ def keygen_leg(cmd, eng, set_id: int = 6960119, count: int = 64, cpu_seconds: fl
     checker = o.RefKeygen(set_id) if o.RefKeygen.available(set_id) else o.Oracle(set_id)
     ok = all(checker.keypair(seeds[i].tobytes()) == (pks[i].tobytes(), sks[i].tobytes(), int(att[i]))
              for i in range(2)) and (one[0], one[1]) == (pks[0].tobytes(), sks[0].tobytes())
+    out = {"set": set_id, "keys": count, "attempts": int(att.sum()), "seconds": dt,
+           "keypairs_per_s": count / dt, "attempts_per_s": float(att.sum()) / dt, "gpu_launches": launches,
+           "single_key_ms": single_s * 1e3, "single_key_attempts": one[2], "matches_reference": bool(ok)}
+    if cpu_seconds <= 0:
+        return out
     # CPU: the reference's keygen, one key per thread (ctypes drops the GIL)
     cores = os.cpu_count() or 1
     threading.stack_size(64 << 20)  # pk_gen keeps its matrix on the stack
@@ -327,12 +335,10 @@ def keygen_leg(cmd, eng, set_id: int = 6960119, count: int = 64, cpu_seconds: fl
             f.cancel()
     cpu_dt = time.perf_counter() - t0
     threading.stack_size(0)
-    return {"set": set_id, "keys": count, "attempts": int(att.sum()), "seconds": dt,
-            "keypairs_per_s": count / dt, "attempts_per_s": float(att.sum()) / dt, "gpu_launches": launches,
-            "single_key_ms": single_s * 1e3, "single_key_attempts": one[2], "matches_reference": bool(ok),
-            "cpu_baseline": {"keypairs_per_s": done / cpu_dt, "attempts": attempts, "keys": done, "cores": cores,
-                             "kind": "reference" if isinstance(checker, o.RefKeygen) else "port",
-                             "sample": f"{done} seeds on {cores} threads, {cpu_dt:.1f} s"}}
+    out["cpu_baseline"] = {"keypairs_per_s": done / cpu_dt, "attempts": attempts, "keys": done, "cores": cores,
+                           "kind": "reference" if isinstance(checker, o.RefKeygen) else "port",
+                           "sample": f"{done} seeds on {cores} threads, {cpu_dt:.1f} s"}
+    return out
 
 
 def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3) -> dict:
@@ -437,6 +443,12 @@ def main() -> None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.keygen_only:
+        eng = cmd.Engine(local)
+        print(json.dumps(keygen_leg(cmd, eng, count=args.keygen_count,
+                                    cpu_seconds=0.0 if args.no_cpu_baseline else 12.0)), flush=True)
+        eng.close()
+        return
     if world > 1:
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
@@ -631,7 +643,7 @@ def main() -> None:
     for g_ in graphs:
         g_.close()
     if world == 1 and not args.no_keygen:
-        line["keygen"] = keygen_leg(cmd, eng)
+        line["keygen"] = keygen_leg(cmd, eng, count=args.keygen_count)
     if world == 1 and not args.no_serve:
         fused_rate = value
         rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, round(0.5 * fused_rate, -5)})
