@@ -151,7 +151,7 @@ SERVER_CONFIG = {"max_batch": 8192, "slots": 8, "max_wait_us": 150, "fused_thres
 
 def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: int = 16384,
                 server_config: dict | None = None) -> dict:
-    """Poisson arrivals over `nkeys` seeded keys drawn from
+    """Serving workload: Poisson arrivals over `nkeys` seeded keys drawn from
     the five sets weighted 30/15/20/20/15, 5% malformed ciphertexts, keys
     device-resident, continuous batching.  Returns per-rate p50/p99 latency and
     sustained decaps/s; valid requests are checked against their planted
@@ -250,7 +250,7 @@ def _time_stream(fn, stream, reps: int, warmup: int) -> float:
 
 
 def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3) -> dict:
-    """each parameter set in turn, `count` ciphertexts of one
+    """All five parameter sets in turn, `count` ciphertexts of one
     seeded key (the reference kem/ key of the set), autotuned fused kernel
     replayed as a CUDA graph; every output checked against its planted error
     vector and weight t.  Inputs (>= 100 MB per set) exceed L2.  The plain
@@ -342,7 +342,7 @@ def keygen_leg(cmd, eng, set_id: int = 6960119, count: int = 64, cpu_seconds: fl
 
 
 def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3) -> dict:
-    """64 seeded keys spread 13/13/13/13/12 over the five
+    """Mixed batch: 64 seeded keys spread 13/13/13/13/12 over the five
     sets, `count` ciphertexts with the set drawn uniformly per ciphertext (key
     uniform within the set), 10% uniformly random mt-bit strings, all in one
     cmd_decrypt_mixed_device launch.  Valid ciphertexts are checked against

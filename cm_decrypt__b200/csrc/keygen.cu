@@ -959,7 +959,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     // Attempt slots per round: about two support CTAs per SM; up to
     // SPEC attempts of one key run side by side (the reference's retries
     // of a key form a fixed chain of seeds, so later attempts can start
-    // before earlier ones are judged; the first accepted one is kept).
+    // before earlier ones are decided; the first accepted one is kept).
     constexpr int SPEC = 4;
     size_t cap = (size_t)std::max(32, 2 * eng->num_sms);
     const size_t fixed = sizeof(GfTables) + 1024;

@@ -191,7 +191,7 @@ def test_mixed_batch(oracle_mod, engine):
 
 @pytest.mark.parametrize("path", ["plain", "fused"])
 def test_full_size_properties(engine, keys, path):
-    """BASELINE-size batch at 6960119 (65,536 ciphertexts): every valid
+    """Full-size batch at 6960119 (65,536 ciphertexts): every valid
     ciphertext decodes to exactly its planted weight-119 error vector."""
     s = 6960119
     pk = cmd.PubKey(s, golden_sk(s))
