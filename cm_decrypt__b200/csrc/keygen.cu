@@ -12,10 +12,13 @@
 //                     parity-check matrix, 32 columns per warp by ballots
 //                     (pk_gen.c:52-113)
 //  4. elimination     blocked Gauss-Jordan on the first mt columns, 32 pivot
-//                     columns per panel: k_ge_panel finds the pivot rows and
-//                     the 32 x 32 transform on the panel words alone,
-//                     k_ge_pivots forms the reduced pivot rows, k_ge_apply
-//                     clears the panel columns of every other row.  The
+//                     columns per panel: k_ge_panel takes pivot rows from the
+//                     rows not yet used, building a reduced basis of their
+//                     panel words (a warp, 32 candidate rows at a time), and
+//                     the 32 x 32 transform to the reduced pivot rows;
+//                     k_ge_apply replaces the pivot rows by reduced ones and
+//                     clears the panel columns of every other row.  Rows stay
+//                     in place: a map gives the row holding each pivot.  The
 //                     result is the unique reduced form [I | T] that
 //                     pk_gen.c:115-143 reaches (rejected when a pivot is
 //                     missing, i.e. the left block is singular)
@@ -56,17 +59,16 @@ enum KgStatus : int { KG_OK = 0, KG_GENPOLY = 1, KG_PERM = 2, KG_SINGULAR = 3, K
 // Runtime sizes of one set's key generation and the per-key workspace.
 struct KgDims {
     int set, m, n, t, q, mt, rlen, rw, pk_row, cond, sk;
-    size_t off_r, off_irr, off_pi, off_cond, off_panel, off_pv, off_mv, off_mat, stride;
+    size_t off_r, off_irr, off_pi, off_cond, off_panel, off_src, off_prow, off_used, off_mat, stride;
 };
 
 struct PanelInfo {
-    int status;         // KgStatus of this key's attempt
-    int npiv, nmove;    // pivots in the current panel; rows moved out of its window
+    int status;          // KgStatus of this key's attempt
+    int npiv;            // pivot columns in the current panel
+    int scan0;           // every row below it holds a pivot
     int pad;
-    uint32_t src[PANEL];   // pivot b comes from (pre-panel) row src[b]
-    uint32_t T[PANEL];     // pivot b = XOR over bits j of T[b] of row src[j]
-    uint32_t from[PANEL];  // non-pivot rows inside the window ...
-    uint32_t to[PANEL];    // ... and the vacated pivot rows they move to
+    uint32_t src[PANEL];  // the rows chosen for this panel; row src[b] receives pivot b
+    uint32_t T[PANEL];    // reduced pivot b = XOR over bits j of T[b] of (pre-panel) row src[j]
 };
 
 KgDims kg_dims(int set)
@@ -96,10 +98,12 @@ KgDims kg_dims(int set)
     o = al(o + d.cond);
     d.off_panel = o;
     o = al(o + sizeof(PanelInfo));
-    d.off_pv = o;
+    d.off_src = o;  // copies of the panel's chosen rows
     o = al(o + (size_t)PANEL * d.rw * 4);
-    d.off_mv = o;
-    o = al(o + (size_t)PANEL * d.rw * 4);
+    d.off_prow = o;  // row holding pivot i
+    o = al(o + (size_t)d.mt * 4);
+    d.off_used = o;  // 1: the row already holds a pivot
+    o = al(o + (size_t)d.mt);
     d.off_mat = o;
     o = al(o + (size_t)d.mt * d.rw * 4);
     d.stride = o;
@@ -477,147 +481,164 @@ __global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict_
 }
 
 // ---- 4. elimination ---------------------------------------------------------
-constexpr int PANEL_THREADS = 1024;
-constexpr int MAX_MT = 13 * 128;
+constexpr int PANEL_THREADS = 256;
 
-// Pivot rows and transform of panel p (columns 32p .. 32p + npiv - 1) from
-// the panel words of rows >= 32p: Gauss-Jordan on those words, tracking for
-// every row which selected rows it has absorbed.
+// Pivot rows of panel p (columns 32p .. 32p + npiv - 1).  Warp 0 walks the
+// rows not yet holding a pivot, 32 at a time, and keeps a reduced basis of
+// their panel words (lane b holds the vector with leading bit b and which
+// chosen rows it combines); a row whose word is independent of the basis is
+// chosen.  When npiv rows are chosen the basis is the identity on the panel
+// columns and its combinations are the transform T.  Then the chosen rows are
+// copied aside for k_ge_apply, which overwrites them.
 __global__ void __launch_bounds__(PANEL_THREADS) k_ge_panel(uint8_t *__restrict__ work, KgDims d, int p)
 {
-    __shared__ uint32_t P[MAX_MT], tag[MAX_MT];
-    __shared__ uint8_t sel[MAX_MT];
-    __shared__ int s_piv;
+    __shared__ uint32_t s_src[PANEL];
+    __shared__ int s_n;
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     PanelInfo *pi = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
     if (pi->status != KG_OK)
         return;
     const uint32_t *mat = reinterpret_cast<const uint32_t *>(wk + d.off_mat);
-    const int tid = threadIdx.x, c0 = PANEL * p, rows = d.mt - c0, npiv = min(PANEL, d.mt - c0);
-    for (int r = tid; r < rows; r += PANEL_THREADS) {
-        P[r] = mat[(size_t)(c0 + r) * d.rw + p];
-        tag[r] = 0;
-        sel[r] = 0;
-    }
-    for (int b = 0; b < npiv; b++) {
+    uint8_t *used = wk + d.off_used;
+    const int tid = threadIdx.x, lane = tid & 31, c0 = PANEL * p, npiv = min(PANEL, d.mt - c0);
+    const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
+    if (p == 0) {
+        for (int r = tid; r < d.mt; r += PANEL_THREADS)
+            used[r] = 0;
         if (tid == 0)
-            s_piv = rows;
-        __syncthreads();
-        for (int r = tid; r < rows; r += PANEL_THREADS)
-            if (!sel[r] && ((P[r] >> b) & 1u))
-                atomicMin(&s_piv, r);
-        __syncthreads();
-        const int sr = s_piv;
-        if (sr >= rows) {
-            if (tid == 0)
-                pi->status = KG_SINGULAR;
-            return;
-        }
-        if (tid == 0) {
-            sel[sr] = 1;
-            tag[sr] |= 1u << b;
-            pi->src[b] = (uint32_t)(c0 + sr);
-        }
-        __syncthreads();
-        const uint32_t ps = P[sr], ts = tag[sr];
-        __syncthreads();
-        for (int r = tid; r < rows; r += PANEL_THREADS)
-            if (r != sr && ((P[r] >> b) & 1u)) {
-                P[r] ^= ps;
-                tag[r] ^= ts;
-            }
-        __syncthreads();
+            pi->scan0 = 0;
     }
-    if (tid < npiv)
-        pi->T[tid] = tag[pi->src[tid] - c0];
-    if (tid == 0) {
-        // rows of the window [c0, c0 + npiv) that are not pivots move to the
-        // pivot rows outside it (both lists ascending)
-        int na = 0, nb = 0;
-        for (int r = 0; r < npiv; r++)
-            if (!sel[r])
-                pi->from[na++] = (uint32_t)(c0 + r);
-        for (int b = 0; b < npiv; b++)
-            if ((int)pi->src[b] >= c0 + npiv)
-                pi->to[nb++] = pi->src[b];
-        // pivot rows are found in row order only per column: sort `to`
-        for (int x = 1; x < nb; x++)
-            for (int y = x; y > 0 && pi->to[y - 1] > pi->to[y]; y--) {
-                const uint32_t tmp = pi->to[y];
-                pi->to[y] = pi->to[y - 1];
-                pi->to[y - 1] = tmp;
+    __syncthreads();
+    if (tid < 32) {
+        const unsigned F = 0xFFFFFFFFu;
+        uint32_t basis = 0, btag = 0;  // this lane's basis vector (leading bit = lane)
+        bool have = false;
+        int nsel = 0;
+        for (int base = pi->scan0; base < d.mt && nsel < npiv; base += 32) {
+            const int r = base + lane;
+            const uint32_t w = (r < d.mt && !used[r]) ? mat[(size_t)r * d.rw + p] & pmask : 0u;
+            uint32_t cm = __ballot_sync(F, w != 0);
+            while (cm && nsel < npiv) {
+                const int j = __ffs(cm) - 1;
+                cm &= cm - 1;
+                uint32_t v = __shfl_sync(F, w, j);
+                // the basis is reduced, so its vectors for v's set leading bits
+                // clear exactly those bits
+                const bool hit = have && ((v >> lane) & 1u);
+                v ^= __reduce_xor_sync(F, hit ? basis : 0u);
+                const uint32_t tg = __reduce_xor_sync(F, hit ? btag : 0u);
+                if (v) {
+                    const int lb = __ffs(v) - 1;
+                    const uint32_t ntag = tg ^ (1u << nsel);
+                    if (have && ((basis >> lb) & 1u)) {
+                        basis ^= v;
+                        btag ^= ntag;
+                    }
+                    if (lane == lb) {
+                        basis = v;
+                        btag = ntag;
+                        have = true;
+                    }
+                    if (lane == 0)
+                        s_src[nsel] = (uint32_t)(base + j);
+                    nsel++;
+                }
             }
-        pi->npiv = npiv;
-        pi->nmove = na;
+        }
+        if (lane == 0)
+            s_n = nsel;
+        if (nsel == npiv && lane < npiv)
+            pi->T[lane] = btag;
     }
-}
-
-// Reduced pivot rows PV[b] and copies MV[i] of the rows that move, words p & ~3 ..
-__global__ void k_ge_pivots(uint8_t *__restrict__ work, KgDims d, int p)
-{
-    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
-    const PanelInfo *pi = reinterpret_cast<const PanelInfo *>(wk + d.off_panel);
-    if (pi->status != KG_OK)
+    __syncthreads();
+    if (s_n < npiv) {
+        if (tid == 0)
+            pi->status = KG_SINGULAR;
         return;
-    const uint32_t *mat = reinterpret_cast<const uint32_t *>(wk + d.off_mat);
-    uint32_t *pv = reinterpret_cast<uint32_t *>(wk + d.off_pv), *mv = reinterpret_cast<uint32_t *>(wk + d.off_mv);
-    // words from p & ~3: the update works on 16-byte columns
-    const int p4 = p & ~3, npiv = pi->npiv, nmove = pi->nmove, width = d.rw - p4;
-    const int items = (npiv + nmove) * width;
-    for (int e = blockIdx.y * blockDim.x + threadIdx.x; e < items; e += gridDim.y * blockDim.x) {
-        const int row = e / width, w = p4 + e % width;
-        if (row < npiv) {
-            uint32_t acc = 0, T = pi->T[row];
-            while (T) {
-                const int j = __ffs(T) - 1;
-                T &= T - 1;
-                acc ^= mat[(size_t)pi->src[j] * d.rw + w];
+    }
+    uint32_t *prow = reinterpret_cast<uint32_t *>(wk + d.off_prow);
+    if (tid < npiv) {
+        pi->src[tid] = s_src[tid];
+        prow[c0 + tid] = s_src[tid];
+        used[s_src[tid]] = 1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        pi->npiv = npiv;
+        int z = pi->scan0;
+        while (z < d.mt && used[z])
+            z++;
+        pi->scan0 = z;
+    }
+    // copies of the chosen rows, 16-byte columns from word p & ~3 (the
+    // update's layout), four loads in flight per thread
+    uint4 *cp = reinterpret_cast<uint4 *>(wk + d.off_src);
+    const uint4 *m4 = reinterpret_cast<const uint4 *>(mat);
+    const int rw4 = d.rw / 4, q0 = p / 4, W4 = rw4 - q0, items = npiv * W4;
+    for (int e0 = tid; e0 < items; e0 += 4 * PANEL_THREADS) {
+        uint4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = e0 + u * PANEL_THREADS;
+            if (e < items) {
+                const int j = e / W4, w = q0 + e % W4;
+                v[u] = m4[(size_t)s_src[j] * rw4 + w];
             }
-            pv[row * d.rw + w] = acc;
-        } else {
-            const int i = row - npiv;
-            mv[i * d.rw + w] = mat[(size_t)pi->from[i] * d.rw + w];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int e = e0 + u * PANEL_THREADS;
+            if (e < items) {
+                const int j = e / W4, w = q0 + e % W4;
+                cp[j * rw4 + w] = v[u];
+            }
         }
     }
 }
 
 constexpr int APPLY_THREADS = 1024;
-constexpr int APPLY_ROWS = 384;  // row slots per block
+constexpr int APPLY_ROWS = 384;  // rows per block
 
 // Shared memory of k_ge_apply: 8 groups x 16 combinations x the active width.
 size_t apply_smem(int width) { return (size_t)8 * 16 * width * 4; }
 
-// Every row slot of the matrix, words p4 = p & ~3 ..: window slots take the
-// pivot rows, the others their (possibly moved) row with the panel columns
-// cleared.  The XOR of the pivot rows a row's panel word selects is found
-// four bits at a time in tables of all 16 combinations of four pivot rows
-// (the "four Russians" method), built per block in shared memory.  Each
-// thread carries four consecutive words (16-byte loads, stores and table
-// reads); words p4 .. p - 1 are zero in every pivot and moved row.
+// Every row, words p4 = p & ~3 ..: a chosen row becomes its reduced pivot
+// row, every other row gets its panel columns cleared.  Both are XORs of the
+// copied chosen rows: row r with panel word x absorbs the reduced pivots of
+// x's bits, i.e. the chosen rows selected by x' = XOR of T[b] over the bits b
+// of x.  That XOR is found four bits of x' at a time in tables of all 16
+// combinations of four chosen rows (the "four Russians" method), built per
+// block in shared memory.  Each thread carries four consecutive words
+// (16-byte loads, stores and table reads); words p4 .. p - 1 are zero in
+// every chosen row.
 __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p)
 {
     extern __shared__ __align__(16) uint4 s_tab4[];  // [8][16][W4]
-    __shared__ uint32_t s_pw[APPLY_ROWS];
-    __shared__ int16_t s_src[APPLY_ROWS];  // -2 window, -1 own row, else moved row index
+    __shared__ uint32_t s_x[APPLY_ROWS];             // x' of each row
+    __shared__ uint8_t s_own[APPLY_ROWS];            // 0: chosen row (its own content is replaced)
+    __shared__ uint32_t s_T[PANEL], s_srcr[PANEL];
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     const PanelInfo *pi = reinterpret_cast<const PanelInfo *>(wk + d.off_panel);
     if (pi->status != KG_OK)
         return;
     uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
-    const uint32_t *pv = reinterpret_cast<const uint32_t *>(wk + d.off_pv);
-    const uint32_t *mv = reinterpret_cast<const uint32_t *>(wk + d.off_mv);
-    const int npiv = pi->npiv, nmove = pi->nmove, p4 = p & ~3, W4 = (d.rw - p4) / 4, c0 = PANEL * p, tid = threadIdx.x;
+    const uint32_t *cp = reinterpret_cast<const uint32_t *>(wk + d.off_src);
+    const int npiv = pi->npiv, p4 = p & ~3, W4 = (d.rw - p4) / 4, tid = threadIdx.x;
     const int rw4 = d.rw / 4;
     const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
     const int r0 = blockIdx.y * APPLY_ROWS, nrows = min(APPLY_ROWS, d.mt - r0);
-    // tables: tab[g][c][w4] = XOR of pivot rows 4g + b for the bits b of c
-    const uint4 *pv4 = reinterpret_cast<const uint4 *>(pv + p4);
+    if (tid < PANEL) {
+        s_T[tid] = tid < npiv ? pi->T[tid] : 0u;
+        s_srcr[tid] = tid < npiv ? pi->src[tid] : 0xFFFFFFFFu;
+    }
+    // tables: tab[g][c][w4] = XOR of chosen rows 4g + b for the bits b of c
+    const uint4 *cp4 = reinterpret_cast<const uint4 *>(cp + p4);
     for (int e = tid; e < 8 * W4; e += APPLY_THREADS) {
         const int g = e / W4, w4 = e - g * W4;
         uint4 v[4];
 #pragma unroll
         for (int b = 0; b < 4; b++)
-            v[b] = 4 * g + b < npiv ? pv4[(4 * g + b) * rw4 + w4] : make_uint4(0, 0, 0, 0);
+            v[b] = 4 * g + b < npiv ? cp4[(4 * g + b) * rw4 + w4] : make_uint4(0, 0, 0, 0);
         uint4 *t = s_tab4 + g * 16 * W4 + w4;
 #pragma unroll
         for (int c = 0; c < 16; c++) {
@@ -633,19 +654,28 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
             t[c * W4] = x;
         }
     }
-    // each row's panel word and source, read before any row is written
+    __syncthreads();
+    // each row's x' and whether it keeps its own content, read before any
+    // row is written
     for (int t = tid; t < nrows; t += APPLY_THREADS) {
-        const int slot = r0 + t;
-        int src = -1;
-        if (slot >= c0 && slot < c0 + npiv) {
-            src = -2;
+        const int r = r0 + t;
+        int b = -1;
+        for (int i = 0; i < npiv; i++)
+            if ((int)s_srcr[i] == r)
+                b = i;
+        uint32_t x;
+        if (b >= 0) {
+            x = s_T[b];
         } else {
-            for (int i = 0; i < nmove; i++)
-                if ((int)pi->to[i] == slot)
-                    src = i;
+            uint32_t pw = mat[(size_t)r * d.rw + p] & pmask;
+            x = 0;
+            while (pw) {
+                x ^= s_T[__ffs(pw) - 1];
+                pw &= pw - 1;
+            }
         }
-        s_src[t] = (int16_t)src;
-        s_pw[t] = src == -2 ? 0u : (src >= 0 ? mv[src * d.rw + p] : mat[(size_t)slot * d.rw + p]) & pmask;
+        s_x[t] = x;
+        s_own[t] = b < 0;
     }
     __syncthreads();
     // thread (t0, w4): 16-byte column w4 of rows t0, t0 + 16, ...
@@ -653,7 +683,6 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
     if (w4 >= W4)
         return;
     uint4 *col = reinterpret_cast<uint4 *>(mat + p4) + w4;  // row r: col[r * rw4]
-    const uint4 *pcol = pv4 + w4, *mcol = reinterpret_cast<const uint4 *>(mv + p4) + w4;
     const uint4 *tg = s_tab4 + w4;  // table g, combination c: tg[(16 g + c) * W4]
     constexpr int STEP = APPLY_THREADS / 64, U = 2;  // two rows in flight per thread
     for (int t = tid >> 6; t < nrows; t += U * STEP) {
@@ -661,26 +690,23 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int tu = t + u * STEP;
-            if (tu < nrows) {
-                const int slot = r0 + tu, src = s_src[tu];
-                acc[u] = src == -2 ? pcol[(slot - c0) * rw4] : (src >= 0 ? mcol[src * rw4] : col[slot * rw4]);
-            }
+            acc[u] = make_uint4(0, 0, 0, 0);
+            if (tu < nrows && s_own[tu])
+                acc[u] = col[(r0 + tu) * rw4];
         }
 #pragma unroll
         for (int u = 0; u < U; u++) {
             const int tu = t + u * STEP;
             if (tu >= nrows)
                 continue;
-            if (s_src[tu] != -2) {
-                const uint32_t x = s_pw[tu];
+            const uint32_t x = s_x[tu];
 #pragma unroll
-                for (int g = 0; g < 8; g++) {
-                    const uint4 v = tg[(16 * g + (int)((x >> (4 * g)) & 15u)) * W4];
-                    acc[u].x ^= v.x;
-                    acc[u].y ^= v.y;
-                    acc[u].z ^= v.z;
-                    acc[u].w ^= v.w;
-                }
+            for (int g = 0; g < 8; g++) {
+                const uint4 v = tg[(16 * g + (int)((x >> (4 * g)) & 15u)) * W4];
+                acc[u].x ^= v.x;
+                acc[u].y ^= v.y;
+                acc[u].z ^= v.z;
+                acc[u].w ^= v.w;
             }
             col[(r0 + tu) * rw4] = acc[u];
         }
@@ -841,7 +867,8 @@ __global__ void __launch_bounds__(CB_THREADS) k_kg_controlbits(uint8_t *__restri
 // ---- 6. outputs ---------------------------------------------------------------
 // For each accepted slot of the list: sk = seed | 0xFFFFFFFF as 8 little-endian
 // bytes | g (2t) | control bits | s (operations.c:60-100) and pk row r =
-// bytes mt/8 .. of reduced row r, into output position i of the list.
+// bytes mt/8 .. of the reduced row holding pivot r, into output position i
+// of the list.
 __global__ void k_kg_output(const uint8_t *__restrict__ work, const uint8_t *__restrict__ slot_seed,
                             const int *__restrict__ slots, uint8_t *__restrict__ pk, uint8_t *__restrict__ sk, KgDims d)
 {
@@ -864,11 +891,12 @@ __global__ void k_kg_output(const uint8_t *__restrict__ work, const uint8_t *__r
         skp[x] = v;
     }
     const uint8_t *mat = wk + d.off_mat;
+    const uint32_t *prow = reinterpret_cast<const uint32_t *>(wk + d.off_prow);
     uint8_t *pkp = pk + (size_t)i * d.mt * d.pk_row;
     const size_t total = (size_t)d.mt * d.pk_row;
     for (size_t e = (size_t)blockIdx.y * blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.y * blockDim.x) {
         const int r = (int)(e / d.pk_row), b = (int)(e % d.pk_row);
-        pkp[e] = mat[(size_t)r * d.rw * 4 + d.mt / 8 + b];
+        pkp[e] = mat[(size_t)prow[r] * d.rw * 4 + d.mt / 8 + b];
     }
 }
 
@@ -1015,12 +1043,11 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             const int gy = (d.mt + APPLY_ROWS - 1) / APPLY_ROWS;
             for (int p = 0; p < npanels; p++) {
                 k_ge_panel<<<S, PANEL_THREADS, 0, s>>>(d_work, d, p);
-                k_ge_pivots<<<dim3(S, 8), 256, 0, s>>>(d_work, d, p);
                 k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - (p & ~3)), s>>>(d_work, d, p);
             }
             k_kg_controlbits<<<S, CB_THREADS, smem_cb, s>>>(d_work, d);
             k_kg_collect<<<(S * 9 + 255) / 256, 256, 0, s>>>(d_work, d, S, reinterpret_cast<uint8_t *>(d_col));
-            lc.bump(5 + 3 * (uint64_t)npanels);
+            lc.bump(5 + 2 * (uint64_t)npanels);
             col.resize((size_t)S * 9);
             if ((e = cudaGetLastError()) != cudaSuccess ||
                 (e = cudaMemcpyAsync(col.data(), d_col, (size_t)S * 36, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
