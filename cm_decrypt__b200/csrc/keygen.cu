@@ -182,42 +182,47 @@ struct WarpKeccak {
     }
 };
 
-// Key k's attempts j < D fill slots k*D + j: attempt 0 expands the key's seed,
-// attempt j + 1 the last 32 bytes of attempt j's expansion (the seed the
-// reference's loop moves on to after a rejected attempt).  slot_seed keeps
-// each slot's seed for its secret key.  One warp per key.
-__global__ void __launch_bounds__(32) k_kg_expand(const uint8_t *__restrict__ seeds, uint8_t *__restrict__ work,
-                                                  uint8_t *__restrict__ slot_seed, KgDims d, int K, int D)
+constexpr int SPEC = 4;  // attempts of one key expanded ahead (its chain)
+
+// Warp k expands the next SPEC attempts of key keys[k] into its chain:
+// attempt 0 from seeds[k] when given, else from the last 32 bytes of the
+// key's previous chain entry Dprev - 1 (the seed the reference's loop moves
+// on to after a rejected attempt); attempt j + 1 from attempt j's last 32
+// bytes.  Chain entry j of key `out` is chain + (out * SPEC + j) * r_stride,
+// its seed chain_seed + (out * SPEC + j) * 32.
+__global__ void __launch_bounds__(32) k_kg_expand(const uint8_t *__restrict__ seeds, const int *__restrict__ keys,
+                                                  uint8_t *__restrict__ chain, uint8_t *__restrict__ chain_seed,
+                                                  KgDims d, int K, int Dprev, size_t r_stride)
 {
     const int k = blockIdx.x, lane = threadIdx.x;
     if (k >= K)
         return;
     constexpr int RATE = 136;
     const WarpKeccak kc(lane);
-    for (int j = 0; j < D; j++) {
-        const int slot = k * D + j;
-        const uint8_t *sd = j == 0 ? seeds + (size_t)k * 32 : work + (size_t)(slot - 1) * d.stride + d.off_r + d.rlen - 32;
-        uint8_t *r = work + (size_t)slot * d.stride + d.off_r;
-        if (lane == 0)
-            reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
-        uint8_t sb = lane < 32 ? sd[lane] : 0;
-        slot_seed[(size_t)slot * 32 + lane] = sb;
+    const int out = keys[k];
+    uint8_t *base = chain + (size_t)out * SPEC * r_stride;
+    // this lane's byte of the first seed, read before the chain is rewritten
+    uint8_t sb = seeds ? seeds[(size_t)k * 32 + lane] : base[(size_t)(Dprev - 1) * r_stride + d.rlen - 32 + lane];
+    __syncwarp();
+    for (int j = 0; j < SPEC; j++) {
+        uint8_t *r = base + (size_t)j * r_stride;
+        chain_seed[((size_t)out * SPEC + j) * 32 + lane] = sb;
         // absorb 64 || seed || 0x1F, pad to 136 bytes with 0x80 at the end:
         // block byte i is 64 (i = 0), seed[i - 1] (1..32), 0x1F (33)
         uint64_t a = 0;
-        if (lane < 5) {
 #pragma unroll
-            for (int b = 0; b < 8; b++) {
-                const int i = 8 * lane + b;
-                uint32_t v = 0;
-                if (i == 0)
-                    v = 64;
-                else if (i <= 32)
-                    v = sd[i - 1];
-                else if (i == 33)
-                    v = 0x1F;
+        for (int b = 0; b < 8; b++) {
+            const int i = 8 * (lane < 5 ? lane : 0) + b;
+            const uint32_t sv = __shfl_sync(0xFFFFFFFFu, (uint32_t)sb, (i - 1) & 31);
+            uint32_t v = 0;
+            if (i == 0)
+                v = 64;
+            else if (i <= 32)
+                v = sv;
+            else if (i == 33)
+                v = 0x1F;
+            if (lane < 5)
                 a |= (uint64_t)v << (8 * b);
-            }
         }
         if (lane == 16)
             a ^= 0x8000000000000000ull;
@@ -236,8 +241,27 @@ __global__ void __launch_bounds__(32) k_kg_expand(const uint8_t *__restrict__ se
                 }
             }
         }
-        __syncwarp();  // the next attempt reads this one's last 32 bytes
+        __syncwarp();  // the next attempt's seed is this one's last 32 bytes
+        sb = r[d.rlen - 32 + lane];
+        __syncwarp();
     }
+}
+
+// Slot k*D + j of the round takes chain entry j of key keys[k]: its
+// expansion, its seed, a fresh status.
+__global__ void k_kg_fill(const uint8_t *__restrict__ chain, const uint8_t *__restrict__ chain_seed,
+                          const int *__restrict__ keys, uint8_t *__restrict__ work, uint8_t *__restrict__ slot_seed,
+                          KgDims d, int D, size_t r_stride)
+{
+    const int slot = blockIdx.x, k = slot / D, j = slot - k * D, out = keys[k];
+    const uint4 *src = reinterpret_cast<const uint4 *>(chain + ((size_t)out * SPEC + j) * r_stride);
+    uint4 *dst = reinterpret_cast<uint4 *>(work + (size_t)slot * d.stride + d.off_r);
+    for (int i = threadIdx.x; i < (d.rlen + 15) / 16; i += blockDim.x)
+        dst[i] = src[i];
+    if (threadIdx.x < 32)
+        slot_seed[(size_t)slot * 32 + threadIdx.x] = chain_seed[((size_t)out * SPEC + j) * 32 + threadIdx.x];
+    if (threadIdx.x == 0)
+        reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
 }
 
 // ---- 2. Goppa polynomial --------------------------------------------------
@@ -984,24 +1008,30 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     cudaSetDevice(eng->device);
     const KgDims d = kg_dims(set);
     const size_t pk_bytes = (size_t)d.mt * d.pk_row;
-    // Attempt slots per round: about two support CTAs per SM; up to
-    // SPEC attempts of one key run side by side (the reference's retries
-    // of a key form a fixed chain of seeds, so later attempts can start
-    // before earlier ones are decided; the first accepted one is kept).
-    constexpr int SPEC = 4;
+    // Attempt slots per round: about two support CTAs per SM; up to SPEC
+    // attempts of one key run side by side (the reference's retries of a key
+    // form a fixed chain of seeds, so later attempts can start before earlier
+    // ones are decided; the first accepted one is kept).  Each pending key
+    // keeps its next SPEC expansions in a chain, refilled on a second stream
+    // while the round's other stages run.
     size_t cap = (size_t)std::max(32, 2 * eng->num_sms);
-    const size_t fixed = sizeof(GfTables) + 1024;
-    // per slot: workspace, seed, key seed, collect record, list entry, one pk and sk
-    auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 32 + 36 + 4 + pk_bytes + d.sk); };
+    const size_t r_stride = (d.rlen + 255) / 256 * 256;
+    const size_t chain_bytes = count * SPEC * (r_stride + 32) + count * (32 + 4);
+    const size_t fixed = sizeof(GfTables) + 2048 + chain_bytes;
+    // per slot: workspace, seed, collect record, list entry, one pk and sk
+    auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 36 + 4 + pk_bytes + d.sk); };
     while (cap > 1 && eng->keygen.reserve(eng, need(cap)) != CMD_OK)
         cap /= 2;
     if (cap == 1 && eng->keygen.reserve(eng, need(1)) != CMD_OK)
         return CMD_E_BUDGET;
     uint8_t *mem = static_cast<uint8_t *>(eng->keygen.ptr);
     uint8_t *d_work = mem;
-    uint8_t *d_slot_seed = d_work + cap * d.stride;
-    uint8_t *d_key_seed = d_slot_seed + cap * 32;
-    uint32_t *d_col = reinterpret_cast<uint32_t *>(d_key_seed + cap * 32);  // 9 words a slot
+    uint8_t *d_chain = d_work + cap * d.stride;                 // count x SPEC x r_stride
+    uint8_t *d_chain_seed = d_chain + count * SPEC * r_stride;  // count x SPEC x 32
+    uint8_t *d_seeds = d_chain_seed + count * SPEC * 32;        // count x 32
+    int *d_keys = reinterpret_cast<int *>(d_seeds + count * 32);  // count
+    uint8_t *d_slot_seed = reinterpret_cast<uint8_t *>(d_keys + count);
+    uint32_t *d_col = reinterpret_cast<uint32_t *>(d_slot_seed + cap * 32);  // 9 words a slot
     int *d_list = reinterpret_cast<int *>(d_col + cap * 9);
     uint8_t *d_pk = reinterpret_cast<uint8_t *>(d_list + cap);
     uint8_t *d_sk = d_pk + cap * pk_bytes;
@@ -1015,15 +1045,34 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         (rc = set_smem_attr((const void *)k_kg_controlbits, smem_cb)) ||
         (rc = set_smem_attr((const void *)k_ge_apply, smem_apply)))
         return rc;
-    cudaError_t e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
-    // keys still to finish: their output index and current seed
+    cudaStream_t s2 = nullptr;
+    cudaEvent_t ev_fill = nullptr, ev_exp = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&ev_fill, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaEventCreateWithFlags(&ev_exp, cudaEventDisableTiming);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
+    // every key's first chain, from its seed
+    std::vector<int> keys(count);
+    for (size_t i = 0; i < count; i++)
+        keys[i] = (int)i;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_seeds, h_seeds, count * 32, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_keys, keys.data(), count * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        k_kg_expand<<<(int)count, 32, 0, s>>>(d_seeds, d_keys, d_chain, d_chain_seed, d, (int)count, 0, r_stride);
+        lc.bump();
+        e = cudaEventRecord(ev_exp, s);
+    }
+    // keys still to finish, by output index
     std::vector<int> pend(count);
-    std::vector<uint8_t> seeds(h_seeds, h_seeds + 32 * count);
     std::vector<uint32_t> tries(count, 0);
     for (size_t i = 0; i < count; i++)
         pend[i] = (int)i;
     std::vector<uint32_t> col;
-    std::vector<uint8_t> key_seed;
     std::vector<int> list, list_out;
     while (!pend.empty() && e == cudaSuccess && rc == CMD_OK) {
         std::vector<int> still;
@@ -1031,12 +1080,21 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         const int D = (int)std::max<size_t>(1, std::min<size_t>(SPEC, cap / keys_per_chunk));
         for (size_t base = 0; base < pend.size() && e == cudaSuccess && rc == CMD_OK; base += keys_per_chunk) {
             const int K = (int)std::min(keys_per_chunk, pend.size() - base), S = K * D;
-            key_seed.resize((size_t)K * 32);
-            for (int k = 0; k < K; k++)
-                memcpy(&key_seed[(size_t)k * 32], &seeds[(size_t)pend[base + k] * 32], 32);
-            if ((e = cudaMemcpyAsync(d_key_seed, key_seed.data(), (size_t)K * 32, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            // the chains this chunk reads are complete (every expansion so far
+            // is on s2 before ev_exp); the key list goes to a free region
+            int *kd = d_keys + base;
+            if ((e = cudaStreamWaitEvent(s, ev_exp, 0)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(kd, pend.data() + base, (size_t)K * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
                 break;
-            k_kg_expand<<<K, 32, 0, s>>>(d_key_seed, d_work, d_slot_seed, d, K, D);
+            k_kg_fill<<<S, 256, 0, s>>>(d_chain, d_chain_seed, kd, d_work, d_slot_seed, d, D, r_stride);
+            // next chains of these keys (attempts D .. D + SPEC - 1 from now),
+            // overlapping the stages below
+            if ((e = cudaEventRecord(ev_fill, s)) != cudaSuccess || (e = cudaStreamWaitEvent(s2, ev_fill, 0)) != cudaSuccess)
+                break;
+            k_kg_expand<<<K, 32, 0, s2>>>(nullptr, kd, d_chain, d_chain_seed, d, K, D, r_stride);
+            if ((e = cudaEventRecord(ev_exp, s2)) != cudaSuccess)
+                break;
+            lc.bump(2);
             k_kg_genpoly<<<S, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
             k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
@@ -1064,7 +1122,6 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
                     j++;
                 if (j == D) {
                     tries[out] += D;
-                    memcpy(&seeds[(size_t)out * 32], &col[(size_t)(k * D + D - 1) * 9 + 1], 32);
                     if (tries[out] < max_attempts) {
                         still.push_back(out);
                     } else {
@@ -1103,6 +1160,16 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     if (h_attempts)
         for (size_t i = 0; i < count; i++)
             h_attempts[i] = tries[i];
+    // the last speculative chains may still run on s2
+    const cudaError_t e2 = s2 ? cudaStreamSynchronize(s2) : cudaSuccess;
+    if (e == cudaSuccess)
+        e = e2;
+    if (ev_fill)
+        cudaEventDestroy(ev_fill);
+    if (ev_exp)
+        cudaEventDestroy(ev_exp);
+    if (s2)
+        cudaStreamDestroy(s2);
     if (e != cudaSuccess)
         return cuda_fail(e, "key generation");
     return rc;
