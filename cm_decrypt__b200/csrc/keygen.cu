@@ -248,20 +248,27 @@ __global__ void __launch_bounds__(32) k_kg_expand(const uint8_t *__restrict__ se
 }
 
 // Slot k*D + j of the round takes chain entry j of key keys[k]: its
-// expansion, its seed, a fresh status.
+// expansion, its seed, its Goppa polynomial and status.
 __global__ void k_kg_fill(const uint8_t *__restrict__ chain, const uint8_t *__restrict__ chain_seed,
                           const int *__restrict__ keys, uint8_t *__restrict__ work, uint8_t *__restrict__ slot_seed,
                           KgDims d, int D, size_t r_stride)
 {
     const int slot = blockIdx.x, k = slot / D, j = slot - k * D, out = keys[k];
-    const uint4 *src = reinterpret_cast<const uint4 *>(chain + ((size_t)out * SPEC + j) * r_stride);
-    uint4 *dst = reinterpret_cast<uint4 *>(work + (size_t)slot * d.stride + d.off_r);
+    const uint8_t *eb = chain + ((size_t)out * SPEC + j) * r_stride;
+    const size_t r_al = (d.rlen + 255) / 256 * 256;
+    uint8_t *wk = work + (size_t)slot * d.stride;
+    const uint4 *src = reinterpret_cast<const uint4 *>(eb);
+    uint4 *dst = reinterpret_cast<uint4 *>(wk + d.off_r);
     for (int i = threadIdx.x; i < (d.rlen + 15) / 16; i += blockDim.x)
         dst[i] = src[i];
+    const uint16_t *gi = reinterpret_cast<const uint16_t *>(eb + r_al);
+    uint16_t *go = reinterpret_cast<uint16_t *>(wk + d.off_irr);
+    for (int i = threadIdx.x; i < d.t; i += blockDim.x)
+        go[i] = gi[i];
     if (threadIdx.x < 32)
         slot_seed[(size_t)slot * 32 + threadIdx.x] = chain_seed[((size_t)out * SPEC + j) * 32 + threadIdx.x];
     if (threadIdx.x == 0)
-        reinterpret_cast<PanelInfo *>(work + (size_t)slot * d.stride + d.off_panel)->status = KG_OK;
+        reinterpret_cast<PanelInfo *>(wk + d.off_panel)->status = *reinterpret_cast<const int *>(eb + r_al + 256);
 }
 
 // ---- 2. Goppa polynomial --------------------------------------------------
@@ -290,8 +297,11 @@ size_t genpoly_smem(const KgDims &d)
     return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 3 * 256 * 2 + 256 * 2 + 64;
 }
 
-__global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__ work, const GfTables *__restrict__ tabs,
-                                                           KgDims d)
+// One CTA per chain entry (key keys[blockIdx.x / SPEC], attempt
+// blockIdx.x % SPEC): reads f from the entry's expansion, writes g and the
+// attempt's status beside it.
+__global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__ chain, const int *__restrict__ keys,
+                                                           const GfTables *__restrict__ tabs, KgDims d, size_t r_stride)
 {
     extern __shared__ __align__(16) uint8_t sm_gp[];
     uint16_t *lg = reinterpret_cast<uint16_t *>(sm_gp);
@@ -302,11 +312,12 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
     uint16_t *v1 = pr + 256;                     // first fold, t + 10
     uint16_t *col = v1 + 256;                    // f, then the multipliers
     __shared__ int s_piv;
-    uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
-    PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
+    uint8_t *eb = chain + ((size_t)keys[blockIdx.x / SPEC] * SPEC + blockIdx.x % SPEC) * r_stride;
+    const size_t r_al = (d.rlen + 255) / 256 * 256;
+    int *status = reinterpret_cast<int *>(eb + r_al + 256);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = d.t, q1 = d.q - 1, W = t + 1;
     load_tables(tabs, lg, ex, d.q);
-    const uint8_t *fr = wk + d.off_r + d.rlen - 32 - 2 * t;
+    const uint8_t *fr = eb + d.rlen - 32 - 2 * t;
     if (tid < t) {
         col[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);
         pw[tid] = tid == 0 ? 1 : 0;
@@ -373,7 +384,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
         const int piv = s_piv;
         if (piv >= t) {
             if (tid == 0)
-                pinfo->status = KG_GENPOLY;
+                *status = KG_GENPOLY;
             return;
         }
         if (piv != c && tid >= c && tid <= t) {
@@ -398,9 +409,11 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
         }
         __syncthreads();
     }
-    uint16_t *irr = reinterpret_cast<uint16_t *>(wk + d.off_irr);
+    uint16_t *irr = reinterpret_cast<uint16_t *>(eb + r_al);
     if (tid < t)
         irr[tid] = A[tid * W + t];
+    if (tid == 0)
+        *status = KG_OK;
 }
 
 // ---- bitonic sorts in shared memory ----------------------------------------
@@ -1015,7 +1028,8 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     // keeps its next SPEC expansions in a chain, refilled on a second stream
     // while the round's other stages run.
     size_t cap = (size_t)std::max(32, 2 * eng->num_sms);
-    const size_t r_stride = (d.rlen + 255) / 256 * 256;
+    // chain entry: expansion | g (2t bytes) | status
+    const size_t r_stride = (d.rlen + 255) / 256 * 256 + 512;
     const size_t chain_bytes = count * SPEC * (r_stride + 32) + count * (32 + 4);
     const size_t fixed = sizeof(GfTables) + 2048 + chain_bytes;
     // per slot: workspace, seed, collect record, list entry, one pk and sk
@@ -1064,7 +1078,8 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         e = cudaMemcpyAsync(d_keys, keys.data(), count * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         k_kg_expand<<<(int)count, 32, 0, s>>>(d_seeds, d_keys, d_chain, d_chain_seed, d, (int)count, 0, r_stride);
-        lc.bump();
+        k_kg_genpoly<<<(int)(count * SPEC), GP_THREADS, smem_gp, s>>>(d_chain, d_keys, d_tab, d, r_stride);
+        lc.bump(2);
         e = cudaEventRecord(ev_exp, s);
     }
     // keys still to finish, by output index
@@ -1092,10 +1107,10 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             if ((e = cudaEventRecord(ev_fill, s)) != cudaSuccess || (e = cudaStreamWaitEvent(s2, ev_fill, 0)) != cudaSuccess)
                 break;
             k_kg_expand<<<K, 32, 0, s2>>>(nullptr, kd, d_chain, d_chain_seed, d, K, D, r_stride);
+            k_kg_genpoly<<<K * SPEC, GP_THREADS, smem_gp, s2>>>(d_chain, kd, d_tab, d, r_stride);
             if ((e = cudaEventRecord(ev_exp, s2)) != cudaSuccess)
                 break;
-            lc.bump(2);
-            k_kg_genpoly<<<S, GP_THREADS, smem_gp, s>>>(d_work, d_tab, d);
+            lc.bump(3);
             k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
             const int gy = (d.mt + APPLY_ROWS - 1) / APPLY_ROWS;
@@ -1105,7 +1120,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             }
             k_kg_controlbits<<<S, CB_THREADS, smem_cb, s>>>(d_work, d);
             k_kg_collect<<<(S * 9 + 255) / 256, 256, 0, s>>>(d_work, d, S, reinterpret_cast<uint8_t *>(d_col));
-            lc.bump(5 + 2 * (uint64_t)npanels);
+            lc.bump(3 + 2 * (uint64_t)npanels);
             col.resize((size_t)S * 9);
             if ((e = cudaGetLastError()) != cudaSuccess ||
                 (e = cudaMemcpyAsync(col.data(), d_col, (size_t)S * 36, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
