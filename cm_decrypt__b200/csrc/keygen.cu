@@ -442,7 +442,7 @@ __device__ void seg_sort(T *x, int n, int seg_log)
 // ---- 3. support, 1/g(L) and the parity-check matrix ------------------------
 constexpr int SUP_THREADS = 1024;
 
-size_t support_smem(const KgDims &d) { return sizeof(GfTables) + (size_t)d.q * 8 + 256 * 2 + 16; }
+size_t support_smem(const KgDims &d) { return sizeof(GfTables) + (size_t)d.q * 8 + 512 * 2 + 16; }
 
 __global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict__ work, const GfTables *__restrict__ tabs,
                                                             KgDims d)
@@ -484,31 +484,58 @@ __global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict_
         pi[i] = (int16_t)(buf[i] & (uint64_t)q1);
     // Row j*m + k, column i: bit k of L_i^j / g(L_i); warp w owns 32-column
     // groups w, w + 32, ...; lane k < m stores row j*m + k of its group.
+    // Both g(L) = sum g_j L^j and L^j / g(L) are taken in the log domain
+    // (exponents j log L accumulate by additions), so every term is an
+    // independent table read rather than a chain of dependent multiplies.
     uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
+    uint16_t *lgg = g + 256;  // log g_j, or 0xFFFF for g_j = 0
+    for (int j = tid; j <= t; j += SUP_THREADS)
+        lgg[j] = g[j] ? lg[g[j]] : 0xFFFFu;
+    __syncthreads();
+    auto addm = [q1](uint32_t a, uint32_t b) {
+        const uint32_t x = a + b;
+        return x >= (uint32_t)q1 ? x - q1 : x;
+    };
     const int warp = tid >> 5, lane = tid & 31, groups = (n + 31) / 32;
     for (int grp = warp; grp < groups; grp += SUP_THREADS / 32) {
         const int i = 32 * grp + lane;
-        uint32_t L = 0, v = 0;
+        uint32_t L = 0, lgL = 0, lgv = 0;
+        bool live = false;
         if (i < n) {
             L = bitrev_m((uint32_t)(buf[i] & (uint64_t)q1), m);
-            uint32_t e = g[t];
-            for (int j = t - 1; j >= 0; j--)
-                e = gmul(lg, ex, q1, e, L) ^ g[j];
-            v = ginv(lg, ex, q1, e);
-        }
-        for (int j = 0; j < t; j++) {
-            uint32_t mine = 0;
-#pragma unroll
-            for (int k = 0; k < 13; k++) {
-                if (k < m) {
-                    const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (v >> k) & 1u);
-                    if (lane == k)
-                        mine = bal;
+            uint32_t e;
+            if (L == 0) {
+                e = g[0];
+            } else {
+                lgL = lg[L];
+                e = 0;
+                uint32_t ej = 0;  // j log L mod 2^m - 1
+                for (int j = 0; j <= t; j++) {
+                    if (lgg[j] != 0xFFFFu)
+                        e ^= ex[addm(lgg[j], ej)];
+                    ej = addm(ej, lgL);
                 }
             }
+            lgv = lg[e] ? q1 - lg[e] : 0;  // log 1/g(L); g has no roots in GF(2^m)
+            live = true;
+        }
+        uint32_t ej = 0;
+        for (int j = 0; j < t; j++) {
+            // v = L^j / g(L)
+            const uint32_t v = !live ? 0u : (L == 0 ? (j == 0 ? ex[lgv] : 0u) : ex[addm(lgv, ej)]);
+            ej = addm(ej, lgL);
+            // 32 x 32 bit transpose across the warp: lane k ends with bit k
+            // of every column's v, the word of row j*m + k
+            uint32_t x = v;
+#pragma unroll
+            for (int sh = 16; sh >= 1; sh >>= 1) {
+                const uint32_t lo = sh == 16 ? 0x0000FFFFu : sh == 8 ? 0x00FF00FFu : sh == 4 ? 0x0F0F0F0Fu
+                                  : sh == 2 ? 0x33333333u : 0x55555555u;
+                const uint32_t p = __shfl_xor_sync(0xFFFFFFFFu, x, sh);
+                x = (lane & sh) ? ((x & ~lo) | ((p & ~lo) >> sh)) : ((x & lo) | ((p & lo) << sh));
+            }
             if (lane < m)
-                mat[(size_t)(j * m + lane) * d.rw + grp] = mine;
-            v = gmul(lg, ex, q1, v, L);
+                mat[(size_t)(j * m + lane) * d.rw + grp] = x;
         }
     }
     for (int e = tid; e < d.mt * (d.rw - groups); e += SUP_THREADS) {
