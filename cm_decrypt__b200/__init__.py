@@ -478,14 +478,21 @@ def kem_keypair(engine: Engine, set_id: int, seed: bytes) -> tuple[bytes, bytes,
     return pk.tobytes(), sk.tobytes(), att.value
 
 
-def kem_keypair_batch(engine: Engine, set_id: int, seeds: np.ndarray,
-                      max_attempts: int = 0) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+def kem_keypair_batch(engine: Engine, set_id: int, seeds: np.ndarray, max_attempts: int = 0,
+                      pk_out: np.ndarray | None = None,
+                      sk_out: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Key pairs for a batch of 32-byte seeds: (pk uint8 [count, pk_bytes],
-    sk uint8 [count, sk_bytes], attempts uint32 [count])."""
+    sk uint8 [count, sk_bytes], attempts uint32 [count]).  pk_out / sk_out,
+    when given, are written in place (e.g. pinned host buffers, which make the
+    result copies faster)."""
     sd = np.ascontiguousarray(seeds, np.uint8).reshape(-1, 32)
     info = set_info(set_id)
-    pk = np.zeros((sd.shape[0], pk_bytes(set_id)), np.uint8)
-    sk = np.zeros((sd.shape[0], info.sk_bytes), np.uint8)
+    shape_pk, shape_sk = (sd.shape[0], pk_bytes(set_id)), (sd.shape[0], info.sk_bytes)
+    for name, arr, shape in (("pk_out", pk_out, shape_pk), ("sk_out", sk_out, shape_sk)):
+        if arr is not None and (arr.dtype != np.uint8 or arr.shape != shape or not arr.flags.c_contiguous):
+            raise ValueError(f"{name} must be a C-contiguous uint8 array of shape {shape}")
+    pk = pk_out if pk_out is not None else np.zeros(shape_pk, np.uint8)
+    sk = sk_out if sk_out is not None else np.zeros(shape_sk, np.uint8)
     att = np.zeros(sd.shape[0], np.uint32)
     _check(lib().cmd_kem_keypair_batch(engine.handle, set_index(set_id), _ptr(sd), sd.shape[0], _ptr(pk), _ptr(sk),
                                        _ptr(att), max_attempts), "cmd_kem_keypair_batch")
