@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_ge_panel(uint8_t *__restrict_
 }
 
 constexpr int APPLY_THREADS = 1024;
-constexpr int APPLY_ROWS = 384;  // rows per block
+constexpr int APPLY_ROWS = 384;  // most rows per block (fewer when few attempts run: more blocks)
 
 // Shared memory of k_ge_apply: 8 groups x 16 combinations x the active width.
 size_t apply_smem(int width) { return (size_t)8 * 16 * width * 4; }
@@ -675,7 +675,7 @@ size_t apply_smem(int width) { return (size_t)8 * 16 * width * 4; }
 // block in shared memory.  Each thread carries four consecutive words
 // (16-byte loads, stores and table reads); words p4 .. p - 1 are zero in
 // every chosen row.
-__global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p)
+__global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict__ work, KgDims d, int p, int rows)
 {
     extern __shared__ __align__(16) uint4 s_tab4[];  // [8][16][W4]
     __shared__ uint32_t s_x[APPLY_ROWS];             // x' of each row
@@ -690,7 +690,7 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_ge_apply(uint8_t *__restrict_
     const int npiv = pi->npiv, p4 = p & ~3, W4 = (d.rw - p4) / 4, tid = threadIdx.x;
     const int rw4 = d.rw / 4;
     const uint32_t pmask = npiv == 32 ? 0xFFFFFFFFu : (1u << npiv) - 1u;
-    const int r0 = blockIdx.y * APPLY_ROWS, nrows = min(APPLY_ROWS, d.mt - r0);
+    const int r0 = blockIdx.y * rows, nrows = min(rows, d.mt - r0);
     if (tid < PANEL) {
         s_T[tid] = tid < npiv ? pi->T[tid] : 0u;
         s_srcr[tid] = tid < npiv ? pi->src[tid] : 0xFFFFFFFFu;
@@ -1140,10 +1140,13 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             lc.bump(3);
             k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
-            const int gy = (d.mt + APPLY_ROWS - 1) / APPLY_ROWS;
+            // rows per update block: about two blocks per SM over the round's slots
+            const int per_slot = std::max(1, (2 * eng->num_sms + S - 1) / S);
+            const int rows = std::min(APPLY_ROWS, std::max(32, ((d.mt + per_slot - 1) / per_slot + 15) / 16 * 16));
+            const int gy = (d.mt + rows - 1) / rows;
             for (int p = 0; p < npanels; p++) {
                 k_ge_panel<<<S, PANEL_THREADS, 0, s>>>(d_work, d, p);
-                k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - (p & ~3)), s>>>(d_work, d, p);
+                k_ge_apply<<<dim3(S, gy), APPLY_THREADS, apply_smem(d.rw - (p & ~3)), s>>>(d_work, d, p, rows);
             }
             k_kg_controlbits<<<S, CB_THREADS, smem_cb, s>>>(d_work, d);
             k_kg_collect<<<(S * 9 + 255) / 256, 256, 0, s>>>(d_work, d, S, reinterpret_cast<uint8_t *>(d_col));
