@@ -124,10 +124,6 @@ __device__ __forceinline__ uint16_t gmul(const uint16_t *lg, const uint16_t *ex,
     s = s >= q1 ? s - q1 : s;
     return ex[s];
 }
-__device__ __forceinline__ uint16_t ginv(const uint16_t *lg, const uint16_t *ex, int q1, uint32_t a)
-{
-    return a ? ex[lg[a] ? q1 - lg[a] : 0] : 0;
-}
 __device__ __forceinline__ uint32_t bitrev_m(uint32_t v, int m) { return __brev(v) >> (32 - m); }
 
 // Copies both tables to shared memory.
@@ -291,10 +287,11 @@ __host__ __device__ inline ExtPoly ext_poly(int set)
 constexpr int GP_THREADS = 1024;
 
 // Shared memory: tables, the t x (t+1) system (row = coordinate, column =
-// power), the current power, the product, the first fold, the multipliers.
+// power), the current power, the product, the first fold, the multipliers,
+// and the logs of f, of the current power and of the pivot row.
 size_t genpoly_smem(const KgDims &d)
 {
-    return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 3 * 256 * 2 + 256 * 2 + 64;
+    return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 7 * 256 * 2 + 64;
 }
 
 // One CTA per chain entry (key keys[blockIdx.x / SPEC], attempt
@@ -307,27 +304,38 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
     uint16_t *lg = reinterpret_cast<uint16_t *>(sm_gp);
     uint16_t *ex = lg + KG_MAX_Q;
     uint16_t *A = ex + KG_MAX_Q;                 // [t][t+1]
-    uint16_t *pw = A + (size_t)d.t * (d.t + 1);  // 256
+    uint16_t *pw = A + (size_t)d.t * (d.t + 1);  // 256: current power
     uint16_t *pr = pw + 256;                     // product, 2t - 1 <= 255
     uint16_t *v1 = pr + 256;                     // first fold, t + 10
-    uint16_t *col = v1 + 256;                    // f, then the multipliers
+    uint16_t *col = v1 + 256;                    // the multipliers of an elimination step
+    uint16_t *lgf = col + 256;                   // log f_i (NZ: f_i = 0)
+    uint16_t *lgp = lgf + 256;                   // log of the current power's coefficients
+    uint16_t *lgr = lgp + 256;                   // log of the pivot row
+    constexpr uint16_t NZ = 0xFFFF;
     __shared__ int s_piv;
     uint8_t *eb = chain + ((size_t)keys[blockIdx.x / SPEC] * SPEC + blockIdx.x % SPEC) * r_stride;
     const size_t r_al = (d.rlen + 255) / 256 * 256;
     int *status = reinterpret_cast<int *>(eb + r_al + 256);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = d.t, q1 = d.q - 1, W = t + 1;
+    auto addm = [q1](uint32_t a, uint32_t b) {
+        const uint32_t x = a + b;
+        return x >= (uint32_t)q1 ? x - q1 : x;
+    };
     load_tables(tabs, lg, ex, d.q);
+    __syncthreads();
     const uint8_t *fr = eb + d.rlen - 32 - 2 * t;
     if (tid < t) {
-        col[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);
+        const uint16_t f = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);
+        lgf[tid] = f ? lg[f] : NZ;
         pw[tid] = tid == 0 ? 1 : 0;
+        lgp[tid] = tid == 0 ? 0 : NZ;
     }
     __syncthreads();
     const ExtPoly F = ext_poly(d.set);
     int offmax = 0;
     for (int u = 0; u < F.nt; u++)
         offmax = max(offmax, F.off[u]);
-    // powers f^0 .. f^t into the columns of A
+    // powers f^0 .. f^t into the columns of A; products in the log domain
     const int ko = tid >> 2, part = tid & 3;  // four threads per product coefficient
     for (int c = 0; c <= t; c++) {
         if (tid < t)
@@ -336,16 +344,19 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
             break;
         // pr = pw * f (degree <= 2t - 2)
         {
-            uint16_t acc = 0;
+            uint32_t acc = 0;
             if (ko < 2 * t - 1) {
                 const int lo = max(0, ko - t + 1), hi = min(ko, t - 1);
-                for (int i = lo + part; i <= hi; i += 4)
-                    acc ^= gmul(lg, ex, q1, pw[i], col[ko - i]);
+                for (int i = lo + part; i <= hi; i += 4) {
+                    const uint32_t a = lgp[i], b = lgf[ko - i];
+                    if (a != NZ && b != NZ)
+                        acc ^= ex[addm(a, b)];
+                }
             }
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 1);
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 2);
             if (part == 0 && ko < 2 * t - 1)
-                pr[ko] = acc;
+                pr[ko] = (uint16_t)acc;
         }
         __syncthreads();
         // fold y^(t+i) = sum_u c_u y^(i+off_u): twice, the second for the at
@@ -368,6 +379,7 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
                     acc ^= F.c[u] == 1 ? v1[t + i] : gmul(lg, ex, q1, v1[t + i], F.c[u]);
             }
             pw[tid] = acc;
+            lgp[tid] = acc ? lg[acc] : NZ;
         }
         __syncthreads();
     }
@@ -393,19 +405,28 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
             A[c * W + tid] = a;
         }
         __syncthreads();
-        const uint16_t inv = ginv(lg, ex, q1, A[c * W + c]);
+        const uint32_t lginv = q1 - lg[A[c * W + c]];  // the pivot is non-zero
         __syncthreads();
-        if (tid >= c && tid <= t)
-            A[c * W + tid] = gmul(lg, ex, q1, A[c * W + tid], inv);
+        // normalise the pivot row; keep its logs for the row updates
+        if (tid >= c && tid <= t) {
+            const uint32_t a = A[c * W + tid];
+            const uint32_t la = a ? addm(lg[a], lginv) : NZ;
+            lgr[tid] = (uint16_t)la;
+            A[c * W + tid] = a ? ex[la] : 0;
+        }
         if (tid < t)
             col[tid] = tid == c ? 0 : A[tid * W + c];
         __syncthreads();
         for (int r = warp; r < t; r += GP_THREADS / 32) {
-            const uint16_t k = col[r];
+            const uint32_t k = col[r];
             if (!k)
                 continue;
-            for (int x = c + lane; x <= t; x += 32)
-                A[r * W + x] ^= gmul(lg, ex, q1, A[c * W + x], k);
+            const uint32_t lk = lg[k];
+            for (int x = c + lane; x <= t; x += 32) {
+                const uint32_t la = lgr[x];
+                if (la != NZ)
+                    A[r * W + x] ^= ex[addm(la, lk)];
+            }
         }
         __syncthreads();
     }
