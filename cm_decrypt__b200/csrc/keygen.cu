@@ -9,8 +9,8 @@
 //  3. k_kg_support    pi = indices ordered by their random words (bitonic
 //                     sort of (word << 31 | index) in shared memory, rejected
 //                     on equal words), L = bitrev(pi), 1/g(L), and the mt x n
-//                     parity-check matrix, 32 columns per warp by ballots
-//                     (pk_gen.c:52-113)
+//                     parity-check matrix, 32 columns per thread in bitsliced
+//                     form (pk_gen.c:52-113)
 //  4. elimination     blocked Gauss-Jordan on the first mt columns, 32 pivot
 //                     columns per panel: k_ge_panel takes pivot rows from the
 //                     rows not yet used, building a reduced basis of their
@@ -34,10 +34,12 @@
 // A rejected attempt continues with the next seed from r, exactly as the
 // reference's loop does, so a seed yields the reference's key pair.
 //
-// Not constant-time: the GF(2^m) arithmetic uses log/antilog tables in shared
-// memory, the elimination reads the pivot rows it selects and the control-bit
-// recursion indexes by permutation values, so kernel timing depends on secret
-// values.  Only the support sort has a data-independent access pattern.
+// Not all constant-time.  The support stage (sort, L, g(L), 1/g(L), the
+// parity-check matrix) has a data-independent schedule: bitonic sorting and
+// the decrypt path's bitsliced arithmetic.  The Goppa polynomial uses
+// log/antilog tables in shared memory, the elimination reads the rows it
+// chooses, and the control-bit recursion indexes by permutation values, so
+// those kernels' timing depends on secret values.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,6 +48,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "gf.cuh"
 #include "keccak.cuh"
 
 namespace cmd {
@@ -461,33 +464,77 @@ __device__ void seg_sort(T *x, int n, int seg_log)
 }
 
 // ---- 3. support, 1/g(L) and the parity-check matrix ------------------------
-constexpr int SUP_THREADS = 1024;
+constexpr int SUP_THREADS = 512;
 
-size_t support_smem(const KgDims &d) { return sizeof(GfTables) + (size_t)d.q * 8 + 512 * 2 + 16; }
+// Shared memory: the sort buffer and g as bitsliced constants (t + 1 rows of
+// 13 words).
+size_t support_smem(const KgDims &d) { return (size_t)d.q * 8 + (size_t)(d.t + 1) * 13 * 4 + 16; }
 
-__global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict__ work, const GfTables *__restrict__ tabs,
-                                                            KgDims d)
+// Columns 32 grp .. 32 grp + 31 of the parity-check matrix, bitsliced: L of
+// the 32 columns as m plane words, g(L) by Horner, its inverse, then the
+// rows L^j / g(L) -- plane word k of row j is the matrix word of row j*m + k.
+// Multiplies and the inverse are the decrypt path's bitsliced routines:
+// no tables, no data-dependent branch or index.
+template <int M>
+__device__ void support_columns(const uint64_t *buf, const uint32_t *gb, uint32_t *mat, const KgDims &d, int grp)
+{
+    const int n = d.n, t = d.t;
+    uint32_t Lb[M];
+#pragma unroll
+    for (int k = 0; k < M; k++)
+        Lb[k] = 0;
+    uint32_t valid = 0;
+    for (int c = 0; c < 32; c++) {
+        const int i = 32 * grp + c;
+        if (i < n) {
+            const uint32_t L = bitrev_m((uint32_t)(buf[i] & (uint64_t)(d.q - 1)), M);
+            valid |= 1u << c;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                Lb[k] |= ((L >> k) & 1u) << c;
+        }
+    }
+    uint32_t e[M], v[M];
+#pragma unroll
+    for (int k = 0; k < M; k++)
+        e[k] = gb[t * 13 + k];
+    for (int j = t - 1; j >= 0; j--) {
+        bs_mul<M>(e, e, Lb);
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            e[k] ^= gb[j * 13 + k];
+    }
+    bs_inv<M>(v, e);  // g has no roots in GF(2^m): e is never 0 on a valid column
+    for (int j = 0; j < t; j++) {
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            mat[(size_t)(j * M + k) * d.rw + grp] = v[k] & valid;
+        bs_mul<M>(v, v, Lb);
+    }
+}
+
+__global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict__ work, KgDims d)
 {
     extern __shared__ __align__(16) uint8_t sm_sup[];
     uint64_t *buf = reinterpret_cast<uint64_t *>(sm_sup);
-    uint16_t *lg = reinterpret_cast<uint16_t *>(buf + d.q);
-    uint16_t *ex = lg + KG_MAX_Q;
-    uint16_t *g = ex + KG_MAX_Q;
+    uint32_t *gb = reinterpret_cast<uint32_t *>(buf + d.q);  // [t + 1][13]: g_j as bitsliced constants
     __shared__ int s_dup;
     uint8_t *wk = work + (size_t)blockIdx.x * d.stride;
     PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(wk + d.off_panel);
     if (pinfo->status != KG_OK)
         return;
     const int tid = threadIdx.x, q = d.q, q1 = q - 1, t = d.t, m = d.m, n = d.n;
-    load_tables(tabs, lg, ex, q);
     const uint8_t *pm = wk + d.off_r + d.n / 8;  // the 2^m random words
     for (int i = tid; i < q; i += SUP_THREADS) {
         const uint32_t w = pm[4 * i] | (pm[4 * i + 1] << 8) | (pm[4 * i + 2] << 16) | ((uint32_t)pm[4 * i + 3] << 24);
         buf[i] = ((uint64_t)w << 31) | (uint64_t)i;
     }
     const uint16_t *irr = reinterpret_cast<const uint16_t *>(wk + d.off_irr);
-    for (int i = tid; i <= t; i += SUP_THREADS)
-        g[i] = i < t ? irr[i] : 1;
+    for (int e = tid; e < (t + 1) * 13; e += SUP_THREADS) {
+        const int j = e / 13, k = e - j * 13;
+        const uint32_t gj = j < t ? irr[j] : 1u;
+        gb[e] = 0u - ((gj >> k) & 1u);
+    }
     if (tid == 0)
         s_dup = 0;
     seg_sort(buf, q, m);
@@ -503,61 +550,14 @@ __global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict_
     int16_t *pi = reinterpret_cast<int16_t *>(wk + d.off_pi);
     for (int i = tid; i < q; i += SUP_THREADS)
         pi[i] = (int16_t)(buf[i] & (uint64_t)q1);
-    // Row j*m + k, column i: bit k of L_i^j / g(L_i); warp w owns 32-column
-    // groups w, w + 32, ...; lane k < m stores row j*m + k of its group.
-    // Both g(L) = sum g_j L^j and L^j / g(L) are taken in the log domain
-    // (exponents j log L accumulate by additions), so every term is an
-    // independent table read rather than a chain of dependent multiplies.
+    // one thread per 32-column group
     uint32_t *mat = reinterpret_cast<uint32_t *>(wk + d.off_mat);
-    uint16_t *lgg = g + 256;  // log g_j, or 0xFFFF for g_j = 0
-    for (int j = tid; j <= t; j += SUP_THREADS)
-        lgg[j] = g[j] ? lg[g[j]] : 0xFFFFu;
-    __syncthreads();
-    auto addm = [q1](uint32_t a, uint32_t b) {
-        const uint32_t x = a + b;
-        return x >= (uint32_t)q1 ? x - q1 : x;
-    };
-    const int warp = tid >> 5, lane = tid & 31, groups = (n + 31) / 32;
-    for (int grp = warp; grp < groups; grp += SUP_THREADS / 32) {
-        const int i = 32 * grp + lane;
-        uint32_t L = 0, lgL = 0, lgv = 0;
-        bool live = false;
-        if (i < n) {
-            L = bitrev_m((uint32_t)(buf[i] & (uint64_t)q1), m);
-            uint32_t e;
-            if (L == 0) {
-                e = g[0];
-            } else {
-                lgL = lg[L];
-                e = 0;
-                uint32_t ej = 0;  // j log L mod 2^m - 1
-                for (int j = 0; j <= t; j++) {
-                    if (lgg[j] != 0xFFFFu)
-                        e ^= ex[addm(lgg[j], ej)];
-                    ej = addm(ej, lgL);
-                }
-            }
-            lgv = lg[e] ? q1 - lg[e] : 0;  // log 1/g(L); g has no roots in GF(2^m)
-            live = true;
-        }
-        uint32_t ej = 0;
-        for (int j = 0; j < t; j++) {
-            // v = L^j / g(L)
-            const uint32_t v = !live ? 0u : (L == 0 ? (j == 0 ? ex[lgv] : 0u) : ex[addm(lgv, ej)]);
-            ej = addm(ej, lgL);
-            // 32 x 32 bit transpose across the warp: lane k ends with bit k
-            // of every column's v, the word of row j*m + k
-            uint32_t x = v;
-#pragma unroll
-            for (int sh = 16; sh >= 1; sh >>= 1) {
-                const uint32_t lo = sh == 16 ? 0x0000FFFFu : sh == 8 ? 0x00FF00FFu : sh == 4 ? 0x0F0F0F0Fu
-                                  : sh == 2 ? 0x33333333u : 0x55555555u;
-                const uint32_t p = __shfl_xor_sync(0xFFFFFFFFu, x, sh);
-                x = (lane & sh) ? ((x & ~lo) | ((p & ~lo) >> sh)) : ((x & lo) | ((p & lo) << sh));
-            }
-            if (lane < m)
-                mat[(size_t)(j * m + lane) * d.rw + grp] = x;
-        }
+    const int groups = (n + 31) / 32;
+    for (int grp = tid; grp < groups; grp += SUP_THREADS) {
+        if (m == 12)
+            support_columns<12>(buf, gb, mat, d, grp);
+        else
+            support_columns<13>(buf, gb, mat, d, grp);
     }
     for (int e = tid; e < d.mt * (d.rw - groups); e += SUP_THREADS) {
         const int r = e / (d.rw - groups), w = groups + e % (d.rw - groups);
@@ -1159,7 +1159,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             if ((e = cudaEventRecord(ev_exp, s2)) != cudaSuccess)
                 break;
             lc.bump(3);
-            k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d_tab, d);
+            k_kg_support<<<S, SUP_THREADS, smem_sup, s>>>(d_work, d);
             const int npanels = (d.mt + PANEL - 1) / PANEL;
             // rows per update block: about two blocks per SM over the round's slots
             const int per_slot = std::max(1, (2 * eng->num_sms + S - 1) / S);
