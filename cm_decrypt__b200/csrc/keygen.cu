@@ -113,32 +113,7 @@ KgDims kg_dims(int set)
     return d;
 }
 
-// ---- GF(2^m) by log/antilog tables (built on the host) --------------------
-struct GfTables {
-    uint16_t lg[KG_MAX_Q];  // lg[0] unused
-    uint16_t ex[KG_MAX_Q];  // ex[i] = gen^i, i < 2^m - 1
-};
-
-__device__ __forceinline__ uint16_t gmul(const uint16_t *lg, const uint16_t *ex, int q1, uint32_t a, uint32_t b)
-{
-    if (!a || !b)
-        return 0;
-    int s = lg[a] + lg[b];
-    s = s >= q1 ? s - q1 : s;
-    return ex[s];
-}
 __device__ __forceinline__ uint32_t bitrev_m(uint32_t v, int m) { return __brev(v) >> (32 - m); }
-
-// Copies both tables to shared memory.
-__device__ void load_tables(const GfTables *g, uint16_t *lg, uint16_t *ex, int q)
-{
-    const uint32_t *s1 = reinterpret_cast<const uint32_t *>(g->lg), *s2 = reinterpret_cast<const uint32_t *>(g->ex);
-    uint32_t *d1 = reinterpret_cast<uint32_t *>(lg), *d2 = reinterpret_cast<uint32_t *>(ex);
-    for (int i = threadIdx.x; i < q / 2; i += blockDim.x) {
-        d1[i] = s1[i];
-        d2[i] = s2[i];
-    }
-}
 
 // ---- 1. seed expansion ----------------------------------------------------
 // Keccak-f[1600] with one state lane per thread of a warp (lane i = x + 5y,
@@ -289,72 +264,59 @@ __host__ __device__ inline ExtPoly ext_poly(int set)
 
 constexpr int GP_THREADS = 1024;
 
-// Shared memory: tables, the t x (t+1) system (row = coordinate, column =
-// power), the current power, the product, the first fold, the multipliers,
-// and the logs of f, of the current power and of the pivot row.
-size_t genpoly_smem(const KgDims &d)
-{
-    return sizeof(GfTables) + (size_t)d.t * (d.t + 1) * 2 + 7 * 256 * 2 + 64;
-}
+// Shared memory: the t x (t+1) system (row = coordinate, column = power),
+// the current power, the product, the first fold, f, the multipliers and the
+// pivot fix-up masks.
+size_t genpoly_smem(const KgDims &d) { return (size_t)d.t * (d.t + 1) * 2 + 5 * 256 * 2 + 256 + 64; }
 
 // One CTA per chain entry (key keys[blockIdx.x / SPEC], attempt
 // blockIdx.x % SPEC): reads f from the entry's expansion, writes g and the
-// attempt's status beside it.
-__global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__ chain, const int *__restrict__ keys,
-                                                           const GfTables *__restrict__ tabs, KgDims d, size_t r_stride)
+// attempt's status beside it.  Field arithmetic is the decrypt path's
+// shift-and-mask multiply and inversion chain (no tables); memory addresses
+// depend only on loop indices.
+template <int M>
+__device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t r_al)
 {
-    extern __shared__ __align__(16) uint8_t sm_gp[];
-    uint16_t *lg = reinterpret_cast<uint16_t *>(sm_gp);
-    uint16_t *ex = lg + KG_MAX_Q;
-    uint16_t *A = ex + KG_MAX_Q;                 // [t][t+1]
-    uint16_t *pw = A + (size_t)d.t * (d.t + 1);  // 256: current power
-    uint16_t *pr = pw + 256;                     // product, 2t - 1 <= 255
-    uint16_t *v1 = pr + 256;                     // first fold, t + 10
-    uint16_t *col = v1 + 256;                    // the multipliers of an elimination step
-    uint16_t *lgf = col + 256;                   // log f_i (NZ: f_i = 0)
-    uint16_t *lgp = lgf + 256;                   // log of the current power's coefficients
-    uint16_t *lgr = lgp + 256;                   // log of the pivot row
-    constexpr uint16_t NZ = 0xFFFF;
-    __shared__ int s_piv;
-    uint8_t *eb = chain + ((size_t)keys[blockIdx.x / SPEC] * SPEC + blockIdx.x % SPEC) * r_stride;
-    const size_t r_al = (d.rlen + 255) / 256 * 256;
+    uint16_t *A = reinterpret_cast<uint16_t *>(smem);  // [t][t+1]: row = coordinate, column = power
+    uint16_t *pw = A + (size_t)d.t * (d.t + 1);       // 256: current power
+    uint16_t *pr = pw + 256;                          // product, 2t - 1 <= 255
+    uint16_t *v1 = pr + 256;                          // first fold, t + 10
+    uint16_t *f = v1 + 256;                           // f
+    uint16_t *col = f + 256;                          // multipliers of an elimination step
+    uint8_t *add = reinterpret_cast<uint8_t *>(col + 256);  // rows added to fix a zero pivot
+    __shared__ int s_ok;
     int *status = reinterpret_cast<int *>(eb + r_al + 256);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = d.t, q1 = d.q - 1, W = t + 1;
-    auto addm = [q1](uint32_t a, uint32_t b) {
-        const uint32_t x = a + b;
-        return x >= (uint32_t)q1 ? x - q1 : x;
-    };
-    load_tables(tabs, lg, ex, d.q);
-    __syncthreads();
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, t = d.t, W = t + 1;
     const uint8_t *fr = eb + d.rlen - 32 - 2 * t;
     if (tid < t) {
-        const uint16_t f = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & q1);
-        lgf[tid] = f ? lg[f] : NZ;
+        f[tid] = (uint16_t)((fr[2 * tid] | (fr[2 * tid + 1] << 8)) & ((1u << M) - 1u));
         pw[tid] = tid == 0 ? 1 : 0;
-        lgp[tid] = tid == 0 ? 0 : NZ;
     }
     __syncthreads();
     const ExtPoly F = ext_poly(d.set);
     int offmax = 0;
     for (int u = 0; u < F.nt; u++)
         offmax = max(offmax, F.off[u]);
-    // powers f^0 .. f^t into the columns of A; products in the log domain
+    // powers f^0 .. f^t into the columns of A
     const int ko = tid >> 2, part = tid & 3;  // four threads per product coefficient
     for (int c = 0; c <= t; c++) {
         if (tid < t)
             A[tid * W + c] = pw[tid];
         if (c == t)
             break;
-        // pr = pw * f (degree <= 2t - 2)
-        {
+        __syncthreads();  // the squaring below may read column c itself (c = 1)
+        if ((c + 1) % 2 == 0) {
+            // f^(c+1) = (f^((c+1)/2))^2: squaring is linear in characteristic
+            // 2 -- coefficient k squared lands at 2k (degree <= 2t - 2)
+            if (tid < 2 * t - 1)
+                pr[tid] = (tid & 1) ? 0 : (uint16_t)gf_sq<M>(A[(tid >> 1) * W + (c + 1) / 2]);
+        } else {
+            // pr = pw * f (degree <= 2t - 2)
             uint32_t acc = 0;
             if (ko < 2 * t - 1) {
                 const int lo = max(0, ko - t + 1), hi = min(ko, t - 1);
-                for (int i = lo + part; i <= hi; i += 4) {
-                    const uint32_t a = lgp[i], b = lgf[ko - i];
-                    if (a != NZ && b != NZ)
-                        acc ^= ex[addm(a, b)];
-                }
+                for (int i = lo + part; i <= hi; i += 4)
+                    acc ^= gf_mul<M>(pw[i], f[ko - i]);
             }
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 1);
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 2);
@@ -365,71 +327,70 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
         // fold y^(t+i) = sum_u c_u y^(i+off_u): twice, the second for the at
         // most offmax coefficients the first pushes to degree >= t
         if (tid < t + offmax) {
-            uint16_t acc = tid < t ? pr[tid] : 0;
+            uint32_t acc = tid < t ? pr[tid] : 0;
             for (int u = 0; u < F.nt; u++) {
                 const int i = tid - F.off[u];
                 if (i >= 0 && i <= t - 2)
-                    acc ^= F.c[u] == 1 ? pr[t + i] : gmul(lg, ex, q1, pr[t + i], F.c[u]);
+                    acc ^= gf_mul<M>(pr[t + i], F.c[u]);
             }
-            v1[tid] = acc;
+            v1[tid] = (uint16_t)acc;
         }
         __syncthreads();
         if (tid < t) {
-            uint16_t acc = v1[tid];
+            uint32_t acc = v1[tid];
             for (int u = 0; u < F.nt; u++) {
                 const int i = tid - F.off[u];
                 if (i >= 0 && i < offmax)
-                    acc ^= F.c[u] == 1 ? v1[t + i] : gmul(lg, ex, q1, v1[t + i], F.c[u]);
+                    acc ^= gf_mul<M>(v1[t + i], F.c[u]);
             }
-            pw[tid] = acc;
-            lgp[tid] = acc ? lg[acc] : NZ;
+            pw[tid] = (uint16_t)acc;
         }
         __syncthreads();
     }
     __syncthreads();
-    // Gauss-Jordan: sum_{j<t} g_j f^j = f^t.  Warp w updates rows w, w + 32,
-    // ...; lane l columns c + l, c + l + 32, ...
+    // Gauss-Jordan: sum_{j<t} g_j f^j = f^t.  A zero pivot is fixed as
+    // sk_gen.c:46-53 does, by adding the following rows up to the first one
+    // with a non-zero entry (masks from a prefix over the rows, no branch on
+    // data); the pivot row is then scaled to 1 and cleared from the others.
+    if (tid == 0)
+        s_ok = 1;
     for (int c = 0; c < t; c++) {
-        if (tid == 0)
-            s_piv = t;
-        __syncthreads();
-        if (tid >= c && tid < t && A[tid * W + c])
-            atomicMin(&s_piv, tid);
-        __syncthreads();
-        const int piv = s_piv;
-        if (piv >= t) {
-            if (tid == 0)
-                *status = KG_GENPOLY;
-            return;
+        // add[k]: row k (> c) is added to row c -- when the pivot is zero,
+        // rows c + 1 .. first (the first row with a non-zero entry in
+        // column c); ballots over the rows, masks by comparison
+        if (warp == 0) {
+            int first = t;
+            for (int base = c + 1; base < t; base += 32) {
+                const int k = base + lane;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, k < t && A[k * W + c] != 0);
+                const int here = bal ? base + __ffs(bal) - 1 : t;
+                first = first < t ? first : here;
+            }
+            const uint32_t zero = A[c * W + c] == 0;
+            for (int k = c + 1 + lane; k < t; k += 32)
+                add[k] = (uint8_t)(zero & (uint32_t)(k <= first));
+            if (lane == 0)
+                s_ok &= !(zero && first == t);  // no pivot: f's minimal polynomial has degree < t
         }
-        if (piv != c && tid >= c && tid <= t) {
-            const uint16_t a = A[piv * W + tid];
-            A[piv * W + tid] = A[c * W + tid];
-            A[c * W + tid] = a;
+        __syncthreads();
+        for (int x = c + tid; x <= t; x += GP_THREADS) {
+            uint32_t acc = A[c * W + x];
+            for (int k = c + 1; k < t; k++)
+                acc ^= A[k * W + x] & (0u - (uint32_t)add[k]);
+            A[c * W + x] = (uint16_t)acc;
         }
         __syncthreads();
-        const uint32_t lginv = q1 - lg[A[c * W + c]];  // the pivot is non-zero
+        const uint32_t inv = gf_inv<M>(A[c * W + c]);  // 0 when singular (then s_ok = 0)
         __syncthreads();
-        // normalise the pivot row; keep its logs for the row updates
-        if (tid >= c && tid <= t) {
-            const uint32_t a = A[c * W + tid];
-            const uint32_t la = a ? addm(lg[a], lginv) : NZ;
-            lgr[tid] = (uint16_t)la;
-            A[c * W + tid] = a ? ex[la] : 0;
-        }
+        if (tid >= c && tid <= t)
+            A[c * W + tid] = (uint16_t)gf_mul<M>(A[c * W + tid], inv);
         if (tid < t)
             col[tid] = tid == c ? 0 : A[tid * W + c];
         __syncthreads();
         for (int r = warp; r < t; r += GP_THREADS / 32) {
             const uint32_t k = col[r];
-            if (!k)
-                continue;
-            const uint32_t lk = lg[k];
-            for (int x = c + lane; x <= t; x += 32) {
-                const uint32_t la = lgr[x];
-                if (la != NZ)
-                    A[r * W + x] ^= ex[addm(la, lk)];
-            }
+            for (int x = c + lane; x <= t; x += 32)
+                A[r * W + x] ^= (uint16_t)gf_mul<M>(A[c * W + x], k);
         }
         __syncthreads();
     }
@@ -437,7 +398,19 @@ __global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__
     if (tid < t)
         irr[tid] = A[tid * W + t];
     if (tid == 0)
-        *status = KG_OK;
+        *status = s_ok ? KG_OK : KG_GENPOLY;
+}
+
+__global__ void __launch_bounds__(GP_THREADS) k_kg_genpoly(uint8_t *__restrict__ chain, const int *__restrict__ keys,
+                                                           KgDims d, size_t r_stride)
+{
+    extern __shared__ __align__(16) uint8_t sm_gp[];
+    uint8_t *eb = chain + ((size_t)keys[blockIdx.x / SPEC] * SPEC + blockIdx.x % SPEC) * r_stride;
+    const size_t r_al = (d.rlen + 255) / 256 * 256;
+    if (d.m == 12)
+        genpoly_body<12>(eb, sm_gp, d, r_al);
+    else
+        genpoly_body<13>(eb, sm_gp, d, r_al);
 }
 
 // ---- bitonic sorts in shared memory ----------------------------------------
@@ -1002,49 +975,6 @@ __global__ void k_kg_collect(const uint8_t *__restrict__ work, KgDims d, int K, 
     }
 }
 
-// Log/antilog tables of GF(2^m) for the smallest generator.
-void host_tables(int m, GfTables &T)
-{
-    const uint32_t poly = m == 12 ? 0x1009u : 0x201Bu, q = 1u << m;
-    auto mul = [&](uint32_t a, uint32_t b) {
-        uint32_t r = 0;
-        for (int i = 0; i < m; i++)
-            if ((b >> i) & 1u)
-                r ^= a << i;
-        for (int k = 2 * m - 2; k >= m; k--)
-            if ((r >> k) & 1u)
-                r ^= poly << (k - m);
-        return r;
-    };
-    memset(&T, 0, sizeof T);
-    for (uint32_t gen = 2; gen < q; gen++) {
-        uint32_t x = 1, i = 0;
-        bool ok = true;
-        for (i = 0; i < q - 1; i++) {
-            if (x == 1 && i > 0) {
-                ok = false;
-                break;
-            }
-            T.ex[i] = (uint16_t)x;
-            T.lg[x] = (uint16_t)i;
-            x = mul(x, gen);
-        }
-        if (ok && x == 1)
-            return;
-    }
-}
-
-const GfTables &tables_for(int m)
-{
-    static GfTables t12, t13;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        host_tables(12, t12);
-        host_tables(13, t13);
-    });
-    return m == 12 ? t12 : t13;
-}
-
 int set_smem_attr(const void *fn, size_t bytes)
 {
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1079,7 +1009,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     // chain entry: expansion | g (2t bytes) | status
     const size_t r_stride = (d.rlen + 255) / 256 * 256 + 512;
     const size_t chain_bytes = count * SPEC * (r_stride + 32) + count * (32 + 4);
-    const size_t fixed = sizeof(GfTables) + 2048 + chain_bytes;
+    const size_t fixed = 2048 + chain_bytes;
     // per slot: workspace, seed, collect record, list entry, one pk and sk
     auto need = [&](size_t c) { return fixed + c * (d.stride + 32 + 36 + 4 + pk_bytes + d.sk); };
     while (cap > 1 && eng->keygen.reserve(eng, need(cap)) != CMD_OK)
@@ -1097,7 +1027,6 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
     int *d_list = reinterpret_cast<int *>(d_col + cap * 9);
     uint8_t *d_pk = reinterpret_cast<uint8_t *>(d_list + cap);
     uint8_t *d_sk = d_pk + cap * pk_bytes;
-    GfTables *d_tab = reinterpret_cast<GfTables *>((reinterpret_cast<uintptr_t>(d_sk + cap * d.sk) + 255) / 256 * 256);
     cudaStream_t s = eng->stream;
     LaunchCounter lc{&eng->launches};
     int rc = CMD_OK;
@@ -1114,8 +1043,6 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         e = cudaEventCreateWithFlags(&ev_fill, cudaEventDisableTiming);
     if (e == cudaSuccess)
         e = cudaEventCreateWithFlags(&ev_exp, cudaEventDisableTiming);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_tab, &tables_for(d.m), sizeof(GfTables), cudaMemcpyHostToDevice, s);
     // every key's first chain, from its seed
     std::vector<int> keys(count);
     for (size_t i = 0; i < count; i++)
@@ -1126,7 +1053,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         e = cudaMemcpyAsync(d_keys, keys.data(), count * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         k_kg_expand<<<(int)count, 32, 0, s>>>(d_seeds, d_keys, d_chain, d_chain_seed, d, (int)count, 0, r_stride);
-        k_kg_genpoly<<<(int)(count * SPEC), GP_THREADS, smem_gp, s>>>(d_chain, d_keys, d_tab, d, r_stride);
+        k_kg_genpoly<<<(int)(count * SPEC), GP_THREADS, smem_gp, s>>>(d_chain, d_keys, d, r_stride);
         lc.bump(2);
         e = cudaEventRecord(ev_exp, s);
     }
@@ -1155,7 +1082,7 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             if ((e = cudaEventRecord(ev_fill, s)) != cudaSuccess || (e = cudaStreamWaitEvent(s2, ev_fill, 0)) != cudaSuccess)
                 break;
             k_kg_expand<<<K, 32, 0, s2>>>(nullptr, kd, d_chain, d_chain_seed, d, K, D, r_stride);
-            k_kg_genpoly<<<K * SPEC, GP_THREADS, smem_gp, s2>>>(d_chain, kd, d_tab, d, r_stride);
+            k_kg_genpoly<<<K * SPEC, GP_THREADS, smem_gp, s2>>>(d_chain, kd, d, r_stride);
             if ((e = cudaEventRecord(ev_exp, s2)) != cudaSuccess)
                 break;
             lc.bump(3);

@@ -68,3 +68,19 @@ def test_keypair_argument_errors(engine):
         cmd.kem_keypair(engine, 6960119, b"short")
     with pytest.raises(Exception):
         cmd.kem_keypair_batch(engine, 6960119, np.zeros((0, 32), np.uint8))
+
+
+def test_keypair_batch_repeatable_and_matches_oracle(oracle_mod, engine):
+    """A larger batch twice: identical results both times (no ordering
+    dependence between the chained stages) and equal to the oracle."""
+    s = 348864
+    o = oracle_mod.Oracle(s)
+    seeds = np.frombuffer(rng(4242).bytes(32 * 24), np.uint8).reshape(24, 32)
+    first = cmd.kem_keypair_batch(engine, s, seeds)
+    again = cmd.kem_keypair_batch(engine, s, seeds)
+    for a, b in zip(first, again):
+        assert np.array_equal(a, b)
+    pks, sks, att = first
+    for i in range(seeds.shape[0]):
+        pk_o, sk_o, a_o = o.keypair(seeds[i].tobytes())
+        assert (int(att[i]), sks[i].tobytes(), pks[i].tobytes()) == (a_o, sk_o, pk_o), i
