@@ -5,7 +5,8 @@
 //  1. k_kg_expand     SHAKE256(64 || seed) -> r = s | perm | f | next seed
 //                     (one thread per key; Keccak-f[1600] in registers)
 //  2. k_kg_genpoly    minimal polynomial g of f in GF((2^m)^t): the powers
-//                     f^0..f^t, then Gauss-Jordan over GF(2^m) (sk_gen.c:24-85)
+//                     f^0..f^t (even ones by squaring), then Gauss-Jordan
+//                     over GF(2^m) (sk_gen.c:24-85); on the seed chains
 //  3. k_kg_support    pi = indices ordered by their random words (bitonic
 //                     sort of (word << 31 | index) in shared memory, rejected
 //                     on equal words), L = bitrev(pi), 1/g(L), and the mt x n
@@ -34,12 +35,14 @@
 // A rejected attempt continues with the next seed from r, exactly as the
 // reference's loop does, so a seed yields the reference's key pair.
 //
-// Not all constant-time.  The support stage (sort, L, g(L), 1/g(L), the
-// parity-check matrix) has a data-independent schedule: bitonic sorting and
-// the decrypt path's bitsliced arithmetic.  The Goppa polynomial uses
-// log/antilog tables in shared memory, the elimination reads the rows it
-// chooses, and the control-bit recursion indexes by permutation values, so
-// those kernels' timing depends on secret values.
+// Not all constant-time.  All field arithmetic is table-free: the Goppa
+// polynomial uses the decrypt path's shift-and-mask multiply and inversion
+// (its zero-pivot fix-up is a masked row sum), and the support stage (sort, L,
+// g(L), 1/g(L), the parity-check matrix) is bitonic sorting plus the bitsliced
+// routines.  The elimination reads the rows it chooses and indexes its
+// combination tables by panel words, and the control-bit recursion indexes
+// by permutation values, so those two stages' timing depends on secret
+// values.
 #include <cuda_runtime.h>
 
 #include <algorithm>

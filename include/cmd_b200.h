@@ -321,7 +321,8 @@ int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *
  * reference's loop does, so a seed yields the reference's key pair; the
  * secret key's first 32 bytes are the seed of the accepted attempt.
  * *attempts (may be NULL) receives the attempts taken.  Every stage runs on
- * the GPU; only the support stage is constant-time (see keygen.cu).
+ * the GPU; field arithmetic is table-free, the elimination and the control
+ * bits are not constant-time (see keygen.cu).
  * CMD_E_KEYGEN if the attempt limit is reached or the control bits fail their
  * self-check. */
 int cmd_kem_keypair(cmd_engine *eng, cmd_set set, const uint8_t *h_seed, uint8_t *h_pk,
