@@ -2,8 +2,9 @@
 // reference's kem/ tree (kem/common/core/operations.c:36-107) for a batch of
 // seeds, every stage on the GPU.  One attempt per pending key and round:
 //
-//  1. k_kg_expand     SHAKE256(64 || seed) -> r = s | perm | f | next seed
-//                     (one thread per key; Keccak-f[1600] in registers)
+//  1. k_kg_expand     SHAKE256(64 || seed) -> r = s | perm | f | next seed,
+//                     a chain of consecutive attempts per key (one warp per
+//                     key, a Keccak-f[1600] state lane per thread)
 //  2. k_kg_genpoly    minimal polynomial g of f in GF((2^m)^t): the powers
 //                     f^0..f^t (even ones by squaring), then Gauss-Jordan
 //                     over GF(2^m) (sk_gen.c:24-85); on the seed chains
@@ -47,6 +48,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <vector>
 
@@ -120,39 +122,71 @@ __device__ __forceinline__ uint32_t bitrev_m(uint32_t v, int m) { return __brev(
 
 // ---- 1. seed expansion ----------------------------------------------------
 // Keccak-f[1600] with one state lane per thread of a warp (lane i = x + 5y,
-// threads 25..31 idle): theta's column parities, pi's lane moves and chi's
-// row neighbours by warp shuffles, rho's rotation per thread.
+// threads 25..31 shadow lane 0), two levels of warp shuffles a round:
+//  1. the lanes of this thread's column (for its parity C[x]) and the three
+//     lanes that pi moves to (x, y), (x + 1, y) and (x + 2, y), the row
+//     neighbours chi combines;
+//  2. the parities C[x0 - 1] .. C[x0 + 3], where x0, x0 + 1 and x0 + 2 are the
+//     columns of those three lanes: theta's D for each of them.
+// Each thread then applies theta, rho and chi to its three lanes itself, so
+// pi and chi cost no further exchange.
 struct WarpKeccak {
-    int x, y, src, rho;  // this thread's lane; the lane pi moves here and its rho offset
+    int col[4];   // the other lanes of this thread's column
+    int src[3];   // the lanes pi moves to (x, y), (x + 1, y), (x + 2, y)
+    int rho[3];   // and their rotations mod 32
+    bool half[3]; // rotations of 32 or more: the halves swap first
+    int par[5];   // lanes holding C[x0 - 1], C[x0], .., C[x0 + 3]
+    bool iota;
     __device__ WarpKeccak(int lane)
     {
         const int l = lane < 25 ? lane : 0;
-        x = l % 5;
-        y = l / 5;
-        // B[y, 2x + 3y] = A[x, y]: this position (X, Y) = (x, y) takes lane
-        // (x0, y0) with y0 = X and 2 x0 + 3 y0 = Y (mod 5), so x0 = 3 (Y - 3 X)
-        const int y0 = x, x0 = (3 * (((y - 3 * x) % 5 + 5) % 5)) % 5;
-        src = x0 + 5 * y0;
-        rho = keccak_rot(x0, y0);
+        const int x = l % 5, y = l / 5;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            col[k] = x + 5 * ((y + 1 + k) % 5);
+        // B[y, 2x + 3y] = A[x, y]: position (X, Y) takes lane (x0, y0) with
+        // y0 = X and 2 x0 + 3 y0 = Y (mod 5), so x0 = 3 (Y - 3 X); position
+        // (X + k, Y) takes (x0 + k, X + k)
+        const int x0 = (3 * (((y - 3 * x) % 5 + 5) % 5)) % 5;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            src[k] = (x0 + k) % 5 + 5 * ((x + k) % 5);
+            const int r = keccak_rot((x0 + k) % 5, (x + k) % 5);
+            rho[k] = r & 31;
+            half[k] = r >= 32;
+        }
+#pragma unroll
+        for (int k = 0; k < 5; k++)
+            par[k] = (x0 + 4 + k) % 5;  // lane q < 5 holds C[q]
+        iota = l == 0;
+    }
+    // rotation by this thread's k-th offset: two funnel shifts on the halves
+    __device__ __forceinline__ uint64_t rot(uint64_t v, int k) const
+    {
+        const uint32_t lo = (uint32_t)v, hi = (uint32_t)(v >> 32);
+        const uint32_t h = half[k] ? lo : hi, l = half[k] ? hi : lo;
+        return ((uint64_t)__funnelshift_l(l, h, rho[k]) << 32) | __funnelshift_l(h, l, rho[k]);
     }
     __device__ uint64_t permute(uint64_t a) const
     {
         const unsigned F = 0xFFFFFFFFu;
 #pragma unroll 1
         for (int round = 0; round < 24; round++) {
-            // theta: threads x (y = 0) form the parity of column x
             uint64_t c = a;
 #pragma unroll
-            for (int k = 1; k < 5; k++)
-                c ^= __shfl_sync(F, a, x + 5 * ((y + k) % 5));
-            const uint64_t cm = __shfl_sync(F, c, (x + 4) % 5), cp = __shfl_sync(F, c, (x + 1) % 5);
-            a ^= cm ^ rotl64(cp, 1);
-            // rho and pi
-            const uint64_t b = rotl64(__shfl_sync(F, a, src), rho);
-            // chi along the row
-            const uint64_t b1 = __shfl_sync(F, b, (x + 1) % 5 + 5 * y), b2 = __shfl_sync(F, b, (x + 2) % 5 + 5 * y);
-            a = b ^ (~b1 & b2);
-            if (x == 0 && y == 0)
+            for (int k = 0; k < 4; k++)
+                c ^= __shfl_sync(F, a, col[k]);
+            const uint64_t a0 = __shfl_sync(F, a, src[0]), a1 = __shfl_sync(F, a, src[1]),
+                           a2 = __shfl_sync(F, a, src[2]);
+            const uint64_t cm1 = __shfl_sync(F, c, par[0]), c0 = __shfl_sync(F, c, par[1]),
+                           c1 = __shfl_sync(F, c, par[2]), c2 = __shfl_sync(F, c, par[3]),
+                           c3 = __shfl_sync(F, c, par[4]);
+            // theta (D[x] = C[x - 1] ^ rotl(C[x + 1], 1)), then rho
+            const uint64_t b0 = rot(a0 ^ cm1 ^ rotl64(c1, 1), 0);
+            const uint64_t b1 = rot(a1 ^ c0 ^ rotl64(c2, 1), 1);
+            const uint64_t b2 = rot(a2 ^ c1 ^ rotl64(c3, 1), 2);
+            a = b0 ^ (~b1 & b2);  // chi
+            if (iota)
                 a ^= kRC[round];
         }
         return a;
@@ -1039,13 +1073,16 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
         (rc = set_smem_attr((const void *)k_kg_controlbits, smem_cb)) ||
         (rc = set_smem_attr((const void *)k_ge_apply, smem_apply)))
         return rc;
-    cudaStream_t s2 = nullptr;
-    cudaEvent_t ev_fill = nullptr, ev_exp = nullptr;
+    // s2: the next chains (expansion, Goppa polynomial); s3: the copies of
+    // finished key pairs to the host, overlapping the next round on s
+    cudaStream_t s2 = nullptr, s3 = nullptr;
+    cudaEvent_t ev_fill = nullptr, ev_exp = nullptr, ev_out = nullptr, ev_copied = nullptr;
     cudaError_t e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
     if (e == cudaSuccess)
-        e = cudaEventCreateWithFlags(&ev_fill, cudaEventDisableTiming);
-    if (e == cudaSuccess)
-        e = cudaEventCreateWithFlags(&ev_exp, cudaEventDisableTiming);
+        e = cudaStreamCreateWithFlags(&s3, cudaStreamNonBlocking);
+    for (cudaEvent_t *ev : {&ev_fill, &ev_exp, &ev_out, &ev_copied})
+        if (e == cudaSuccess)
+            e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
     // every key's first chain, from its seed
     std::vector<int> keys(count);
     for (size_t i = 0; i < count; i++)
@@ -1138,34 +1175,41 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
             if (list.empty())
                 continue;
             const int nl = (int)list.size();
-            if ((e = cudaMemcpyAsync(d_list, list.data(), (size_t)nl * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+            // the previous round's key pairs have left d_pk / d_sk (a wait on
+            // an event not yet recorded passes)
+            if ((e = cudaMemcpyAsync(d_list, list.data(), (size_t)nl * 4, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+                (e = cudaStreamWaitEvent(s, ev_copied, 0)) != cudaSuccess)
                 break;
             k_kg_output<<<dim3(nl, 16), 256, 0, s>>>(d_work, d_slot_seed, d_list, d_pk, d_sk, d);
             lc.bump();
+            if ((e = cudaEventRecord(ev_out, s)) != cudaSuccess || (e = cudaStreamWaitEvent(s3, ev_out, 0)) != cudaSuccess)
+                break;
             for (int i = 0; i < nl && e == cudaSuccess; i++) {
                 const int out = list_out[i];
                 if ((e = cudaMemcpyAsync(h_pk + (size_t)out * pk_bytes, d_pk + (size_t)i * pk_bytes, pk_bytes,
-                                         cudaMemcpyDeviceToHost, s)) == cudaSuccess)
-                    e = cudaMemcpyAsync(h_sk + (size_t)out * d.sk, d_sk + (size_t)i * d.sk, d.sk, cudaMemcpyDeviceToHost, s);
+                                         cudaMemcpyDeviceToHost, s3)) == cudaSuccess)
+                    e = cudaMemcpyAsync(h_sk + (size_t)out * d.sk, d_sk + (size_t)i * d.sk, d.sk, cudaMemcpyDeviceToHost, s3);
             }
             if (e == cudaSuccess)
-                e = cudaStreamSynchronize(s);
+                e = cudaEventRecord(ev_copied, s3);
         }
         pend.swap(still);
     }
     if (h_attempts)
         for (size_t i = 0; i < count; i++)
             h_attempts[i] = tries[i];
-    // the last speculative chains may still run on s2
-    const cudaError_t e2 = s2 ? cudaStreamSynchronize(s2) : cudaSuccess;
-    if (e == cudaSuccess)
-        e = e2;
-    if (ev_fill)
-        cudaEventDestroy(ev_fill);
-    if (ev_exp)
-        cudaEventDestroy(ev_exp);
-    if (s2)
-        cudaStreamDestroy(s2);
+    // the last speculative chains may still run on s2, the last copies on s3
+    for (cudaStream_t st : {s3, s2}) {
+        const cudaError_t e2 = st ? cudaStreamSynchronize(st) : cudaSuccess;
+        if (e == cudaSuccess)
+            e = e2;
+    }
+    for (cudaEvent_t ev : {ev_fill, ev_exp, ev_out, ev_copied})
+        if (ev)
+            cudaEventDestroy(ev);
+    for (cudaStream_t st : {s2, s3})
+        if (st)
+            cudaStreamDestroy(st);
     if (e != cudaSuccess)
         return cuda_fail(e, "key generation");
     return rc;
