@@ -8,8 +8,9 @@
 //            &&  C == [I | T] e          (e re-encodes to C)
 //   K = SHAKE256(b || v || C),  b = accept,  v = accept ? e : s
 //
-// with T the systematic public key (derived from the secret key on the host,
-// once per key) and s the random string stored at the end of the secret key.
+// with T the systematic public key (derived once per key on the device from
+// the key's support and Goppa polynomial by the key generation's elimination)
+// and s the random string stored at the end of the secret key.
 //
 // k_decap: 8 warps per CTA, lane = ciphertext, 256 ciphertexts per CTA.
 //  1. re-encoding: each lane keeps the mt-bit word vector acc = T * e[mt..n)
@@ -23,7 +24,7 @@
 //     offsets derived from the standard's definitions at compile time); the
 //     preimage's v bytes are selected with masks.
 #include <cstring>
-#include <vector>
+#include <mutex>
 
 #include "engine.h"
 #include "fused_impl.cuh"
@@ -189,37 +190,6 @@ size_t decap_pk_words(int set)
     return dispatch_set(set, [&]<int S>() -> size_t { return (size_t)DecapDims<S>::XC * DecapDims<S>::CWP; });
 }
 
-// Column-major copy of the public key's T block for k_decap (host side).
-int decap_pk_columns(int set, const uint8_t *sk, std::vector<uint32_t> &out)
-{
-    cmd_pubkey *pk = nullptr;
-    int rc = cmd_synth_pubkey((cmd_set)set, sk, &pk);
-    if (rc)
-        return rc;
-    std::vector<uint64_t> cols;
-    size_t xw = 0;
-    rc = cmd_pubkey_columns(pk, nullptr, 0, &xw);
-    const SetInfo si = set_info(set);
-    const int mt = si.m * si.t, xc = si.n - mt;
-    cols.resize((size_t)xc * xw);
-    if (rc == CMD_OK)
-        rc = cmd_pubkey_columns(pk, cols.data(), cols.size(), &xw);
-    cmd_synth_pubkey_free(pk);
-    if (rc)
-        return rc;
-    dispatch_set(set, [&]<int S>() {
-        using Q = DecapDims<S>;
-        out.assign((size_t)Q::XC * Q::CWP, 0);
-        for (int cidx = 0; cidx < Q::XC; cidx++)
-            for (int w = 0; w < Q::CW; w++) {
-                const uint64_t v = cols[(size_t)cidx * xw + (w >> 1)];
-                out[(size_t)cidx * Q::CWP + w] = (uint32_t)(v >> (32 * (w & 1)));
-            }
-        return 0;
-    });
-    return CMD_OK;
-}
-
 cudaError_t launch_decap(int set, const uint8_t *d_cts, const uint32_t *d_err, const uint16_t *d_w,
                          const uint32_t *d_pk, const uint8_t *d_s, uint8_t *d_keys, uint8_t *d_accept, size_t count,
                          cudaStream_t s, LaunchCounter lc)
@@ -246,33 +216,33 @@ int cmd_key_prepare_decap(cmd_engine *eng, cmd_key *key)
 {
     if (!eng || !key || key->eng != eng)
         return CMD_E_ARG;
+    // one preparation at a time, so that two first calls for a key derive
+    // its columns once
+    static std::mutex prep_mu;
+    std::lock_guard<std::mutex> lk(prep_mu);
     if (key->pk)
         return CMD_OK;
     const int set = key->dev.set;
-    const SetInfo si = set_info(set);
-    std::vector<uint8_t> sk(si.sk);
-    cudaSetDevice(eng->device);
-    cudaError_t e = cudaMemcpy(sk.data(), key->dev.sk, si.sk, cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess)
-        return cuda_fail(e, "secret key D2H");
-    std::vector<uint32_t> cols;
-    int rc = decap_pk_columns(set, sk.data(), cols);
-    if (rc) {
-        set_last_error("the secret key's public key has no systematic form");
-        return rc;
-    }
-    const size_t bytes = cols.size() * 4;
+    const size_t bytes = decap_pk_words(set) * 4;
+    const int cwp = dispatch_set(set, [&]<int S>() { return DecapDims<S>::CWP; });
     if (!budget_take(eng, bytes)) {
         set_last_error("public key does not fit the engine HBM budget");
         return CMD_E_BUDGET;
     }
+    cudaSetDevice(eng->device);
     void *p = nullptr;
-    if ((e = cudaMalloc(&p, bytes)) != cudaSuccess || (e = cudaMemcpy(p, cols.data(), bytes, cudaMemcpyHostToDevice)) !=
-                                                          cudaSuccess) {
-        if (p)
-            cudaFree(p);
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
         budget_give(eng, bytes);
-        return cuda_fail(e, "public key upload");
+        return cuda_fail(e, "public key columns");
+    }
+    // the key's parity-check matrix from its device support and Goppa
+    // polynomial, reduced on the device
+    const int rc = kg_pubkey_columns(eng, set, key->dev.L, key->dev.g, static_cast<uint32_t *>(p), cwp);
+    if (rc) {
+        cudaFree(p);
+        budget_give(eng, bytes);
+        return rc;
     }
     key->pk = static_cast<uint32_t *>(p);
     key->pk_bytes = bytes;

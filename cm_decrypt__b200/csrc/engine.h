@@ -40,6 +40,11 @@ struct FusedConfig {
 };
 
 int cuda_fail(cudaError_t e, const char *what);
+// T of the public key [I | T] of a key, from its device support d_L (n
+// entries) and Goppa polynomial d_g (t + 1 coefficients): column c at
+// d_cols[c * cwp ..], cwp >= ceil(mt / 32) words.  CMD_E_ARG when the key's
+// parity-check matrix has no systematic form.  Takes eng->mu.
+int kg_pubkey_columns(cmd_engine *eng, int set, const uint16_t *d_L, const uint16_t *d_g, uint32_t *d_cols, int cwp);
 bool valid_set(int set);
 bool budget_take(cmd_engine *eng, size_t bytes);
 void budget_give(cmd_engine *eng, size_t bytes);

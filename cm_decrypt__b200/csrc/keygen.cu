@@ -36,6 +36,11 @@
 // A rejected attempt continues with the next seed from r, exactly as the
 // reference's loop does, so a seed yields the reference's key pair.
 //
+// The same parity-check matrix (from an existing key's support and Goppa
+// polynomial, k_kg_support_key), elimination and a column transpose
+// (k_kg_pk_columns) give the public-key columns that decapsulation checks
+// re-encodings against: kg_pubkey_columns.
+//
 // Not all constant-time.  All field arithmetic is table-free: the Goppa
 // polynomial uses the decrypt path's shift-and-mask multiply and inversion
 // (its zero-pivot fix-up is a masked row sum), and the support stage (sort, L,
@@ -485,8 +490,12 @@ size_t support_smem(const KgDims &d) { return (size_t)d.q * 8 + (size_t)(d.t + 1
 // rows L^j / g(L) -- plane word k of row j is the matrix word of row j*m + k.
 // Multiplies and the inverse are the decrypt path's bitsliced routines:
 // no tables, no data-dependent branch or index.
+//
+// The support comes from the sorted buffer (L = bitrev of the index part) or,
+// when Ls is given, from a key's support array.
 template <int M>
-__device__ void support_columns(const uint64_t *buf, const uint32_t *gb, uint32_t *mat, const KgDims &d, int grp)
+__device__ void support_columns(const uint64_t *buf, const uint16_t *Ls, const uint32_t *gb, uint32_t *mat,
+                                const KgDims &d, int grp)
 {
     const int n = d.n, t = d.t;
     uint32_t Lb[M];
@@ -497,7 +506,7 @@ __device__ void support_columns(const uint64_t *buf, const uint32_t *gb, uint32_
     for (int c = 0; c < 32; c++) {
         const int i = 32 * grp + c;
         if (i < n) {
-            const uint32_t L = bitrev_m((uint32_t)(buf[i] & (uint64_t)(d.q - 1)), M);
+            const uint32_t L = Ls ? (uint32_t)Ls[i] : bitrev_m((uint32_t)(buf[i] & (uint64_t)(d.q - 1)), M);
             valid |= 1u << c;
 #pragma unroll
             for (int k = 0; k < M; k++)
@@ -565,9 +574,41 @@ __global__ void __launch_bounds__(SUP_THREADS) k_kg_support(uint8_t *__restrict_
     const int groups = (n + 31) / 32;
     for (int grp = tid; grp < groups; grp += SUP_THREADS) {
         if (m == 12)
-            support_columns<12>(buf, gb, mat, d, grp);
+            support_columns<12>(buf, nullptr, gb, mat, d, grp);
         else
-            support_columns<13>(buf, gb, mat, d, grp);
+            support_columns<13>(buf, nullptr, gb, mat, d, grp);
+    }
+    for (int e = tid; e < d.mt * (d.rw - groups); e += SUP_THREADS) {
+        const int r = e / (d.rw - groups), w = groups + e % (d.rw - groups);
+        mat[(size_t)r * d.rw + w] = 0;
+    }
+}
+
+// The parity-check matrix of an existing key (its support L, n entries, and
+// Goppa polynomial g, t + 1 coefficients with g[t] = 1, as the key expansion
+// keeps them on the device) into workspace slot 0, for the elimination that
+// gives the key's public key (pk_gen.c:52-113 from a stored key).
+__global__ void __launch_bounds__(SUP_THREADS) k_kg_support_key(uint8_t *__restrict__ work, KgDims d,
+                                                                const uint16_t *__restrict__ L,
+                                                                const uint16_t *__restrict__ g)
+{
+    __shared__ uint32_t gb[(128 + 1) * 13];  // g_j as bitsliced constants
+    const int tid = threadIdx.x, t = d.t, n = d.n;
+    PanelInfo *pinfo = reinterpret_cast<PanelInfo *>(work + d.off_panel);
+    for (int e = tid; e < (t + 1) * 13; e += SUP_THREADS) {
+        const int j = e / 13, k = e - j * 13;
+        gb[e] = 0u - (((uint32_t)g[j] >> k) & 1u);
+    }
+    if (tid == 0)
+        pinfo->status = KG_OK;
+    __syncthreads();
+    uint32_t *mat = reinterpret_cast<uint32_t *>(work + d.off_mat);
+    const int groups = (n + 31) / 32;
+    for (int grp = tid; grp < groups; grp += SUP_THREADS) {
+        if (d.m == 12)
+            support_columns<12>(nullptr, L, gb, mat, d, grp);
+        else
+            support_columns<13>(nullptr, L, gb, mat, d, grp);
     }
     for (int e = tid; e < d.mt * (d.rw - groups); e += SUP_THREADS) {
         const int r = e / (d.rw - groups), w = groups + e % (d.rw - groups);
@@ -1012,6 +1053,41 @@ __global__ void k_kg_collect(const uint8_t *__restrict__ work, KgDims d, int K, 
     }
 }
 
+// T's columns from the reduced matrix of slot 0: column c (< n - mt) is bit
+// mt + c of the reduced pivot rows 0 .. mt - 1, word w of it (rows 32w ..
+// 32w + 31) at cols[c * cwp + w]; words from the last row on are zero.  Warp
+// (chunk, w): lane b takes 32 bits of pivot row 32w + b from column mt +
+// 32 chunk on, and 32 ballots turn the 32 x 32 block around.
+__global__ void __launch_bounds__(256) k_kg_pk_columns(const uint8_t *__restrict__ work, KgDims d,
+                                                      uint32_t *__restrict__ cols, int cwp)
+{
+    const PanelInfo *pinfo = reinterpret_cast<const PanelInfo *>(work + d.off_panel);
+    const int xc = d.n - d.mt, chunks = (xc + 31) / 32;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (pinfo->status != KG_OK || warp >= chunks * cwp)
+        return;
+    const int chunk = warp / cwp, w = warp - chunk * cwp, r = 32 * w + lane;
+    const uint32_t *mat = reinterpret_cast<const uint32_t *>(work + d.off_mat);
+    const uint32_t *prow = reinterpret_cast<const uint32_t *>(work + d.off_prow);
+    uint32_t bits = 0;
+    if (r < d.mt) {
+        const uint32_t *row = mat + (size_t)prow[r] * d.rw;
+        const int b0 = d.mt + 32 * chunk, w0 = b0 >> 5, sh = b0 & 31;
+        const uint32_t lo = row[w0], hi = w0 + 1 < d.rw ? row[w0 + 1] : 0u;
+        bits = __funnelshift_r(lo, hi, sh);
+    }
+    uint32_t mine = 0;
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, (bits >> k) & 1u);
+        if (lane == k)
+            mine = bal;
+    }
+    const int c = 32 * chunk + lane;
+    if (c < xc)
+        cols[(size_t)c * cwp + w] = mine;
+}
+
 int set_smem_attr(const void *fn, size_t bytes)
 {
     const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1019,6 +1095,47 @@ int set_smem_attr(const void *fn, size_t bytes)
 }
 
 }  // namespace
+
+int kg_pubkey_columns(cmd_engine *eng, int set, const uint16_t *d_L, const uint16_t *d_g, uint32_t *d_cols, int cwp)
+{
+    std::lock_guard<std::mutex> lk(eng->mu);
+    cudaSetDevice(eng->device);
+    const KgDims d = kg_dims(set);
+    int rc = eng->keygen.reserve(eng, d.stride);
+    if (rc)
+        return rc;
+    uint8_t *work = static_cast<uint8_t *>(eng->keygen.ptr);
+    if ((rc = set_smem_attr((const void *)k_ge_apply, apply_smem(d.rw))))
+        return rc;
+    cudaStream_t s = eng->stream;
+    LaunchCounter lc{&eng->launches};
+    k_kg_support_key<<<1, SUP_THREADS, 0, s>>>(work, d, d_L, d_g);
+    const int npanels = (d.mt + PANEL - 1) / PANEL;
+    // one key: small row blocks, about two per SM
+    const int rows = std::min(APPLY_ROWS, std::max(32, ((d.mt + 2 * eng->num_sms - 1) / (2 * eng->num_sms) + 15) / 16 * 16));
+    const int gy = (d.mt + rows - 1) / rows;
+    for (int p = 0; p < npanels; p++) {
+        k_ge_panel<<<1, PANEL_THREADS, 0, s>>>(work, d, p);
+        k_ge_apply<<<dim3(1, gy), APPLY_THREADS, apply_smem(d.rw - (p & ~3)), s>>>(work, d, p, rows);
+    }
+    const int warps = (d.n - d.mt + 31) / 32 * cwp;
+    k_kg_pk_columns<<<(warps + 7) / 8, 256, 0, s>>>(work, d, d_cols, cwp);
+    lc.bump(2 + 2 * (uint64_t)npanels);
+    int status = KG_SINGULAR;
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&status, work + d.off_panel, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "public key derivation");
+    if (status != KG_OK) {
+        set_last_error("the secret key's public key has no systematic form");
+        return CMD_E_ARG;
+    }
+    return CMD_OK;
+}
+
 }  // namespace cmd
 
 using namespace cmd;

@@ -219,10 +219,11 @@ int cmd_positions_to_errorstream(const char *binary_path, const char *text_path)
  * K = SHAKE256(b || v || C) with b = accept and v = e, or v = the secret
  * key's n/8-byte string s when rejected.  The re-encoding check reads every
  * column of T for every ciphertext, and v is selected with masks, so the
- * work does not depend on e.  The first call for a key derives T from the
- * secret key on the host (Gaussian elimination, ~0.3 s for 6960119) and
- * keeps it on the device, charged to the engine's budget (1.1 MB for
- * 6960119); cmd_key_prepare_decap does that step ahead of time.
+ * work does not depend on e.  The first call for a key derives T on the
+ * device from the key's support and Goppa polynomial (the key generation's
+ * elimination) and keeps it there, charged to the engine's budget (1.1 MB for
+ * 6960119); cmd_key_prepare_decap does that step ahead of time.  CMD_E_ARG
+ * when the key's parity-check matrix has no systematic form.
  * keys: 32 bytes per ciphertext; accept (may be NULL): 1 byte each. */
 int cmd_key_prepare_decap(cmd_engine *eng, cmd_key *key);
 int cmd_kem_decap(cmd_engine *eng, cmd_key *key, const uint8_t *h_cts, size_t count,

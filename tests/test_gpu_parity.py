@@ -282,6 +282,44 @@ def test_kem_decap(oracle_mod, engine, keys, s):
     assert np.array_equal(d_k.cpu().numpy(), k)
 
 
+def test_decap_key_preparation_on_device(oracle_mod, engine):
+    """The decapsulation's public-key columns are derived on the device from
+    the key's support and Goppa polynomial.  Keys made by flipping one
+    control bit of a golden key: one whose parity-check matrix stays
+    systematic decapsulates its own valid ciphertexts (made from the host's
+    public key) with the oracle's keys; one that has no systematic form (the
+    host derivation refuses it) is refused with CMD_E_ARG."""
+    s = 460896
+    sk = golden_sk(s)
+    info = cmd.set_info(s)
+    off = 40 + 2 * info.t
+
+    def flipped(i):
+        b = bytearray(sk)
+        b[off + 37 * i] ^= 0x01
+        return bytes(b)
+
+    def systematic(k):
+        try:
+            cmd.PubKey(s, k)
+            return True
+        except cmd.CmdError:
+            return False
+
+    good = next(flipped(i) for i in range(1, 40) if systematic(flipped(i)))
+    bad = next(flipped(i) for i in range(1, 40) if not systematic(flipped(i)))
+    key = cmd.Key(engine, s, good)
+    cmd.prepare_decap(engine, key)
+    cts, planted, valid = cmd.PubKey(s, good).ciphertexts(seed=5, count=96, malformed_permille=100)
+    k, a = cmd.kem_decap(engine, key, cts)
+    rk, ra = oracle_mod.Oracle(s).decap(good, cts, nthreads=8)
+    assert np.array_equal(a, ra) and np.array_equal(k, rk)
+    assert a.sum() == valid.sum() > 0
+    with pytest.raises(cmd.CmdError) as err:
+        cmd.prepare_decap(engine, cmd.Key(engine, s, bad))
+    assert err.value.code == cmd.CMD_E_ARG
+
+
 def test_binary_errorstream_files_and_cli(engine, tmp_path):
     s = 6960119
     b = str(tmp_path / "es.pos")
