@@ -71,14 +71,23 @@ static uint32_t round_size(cmd_engine *eng, int set, int wpb, size_t count, bool
     return (uint32_t)std::min<uint64_t>(std::max<uint64_t>(r, 32), full);
 }
 
+uint32_t fused_round(cmd_engine *eng, int set, size_t count)
+{
+    return round_size(eng, set, eng->fcfg[set].wpb, count, eng->fcfg[set].balanced);
+}
+
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced)
+                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced,
+                      uint32_t round_cts)
 {
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
     const int wpb = eng->fcfg[set].wpb;
-    const uint32_t round =
-        round_size(eng, set, wpb, count, balanced < 0 ? eng->fcfg[set].balanced : balanced != 0);
+    if (round_cts % 32 != 0 || round_cts > (uint32_t)wpb * 32)
+        return CMD_E_ARG;
+    const uint32_t round = round_cts ? round_cts
+                                     : round_size(eng, set, wpb, count,
+                                                  balanced < 0 ? eng->fcfg[set].balanced : balanced != 0);
     const uint64_t rounds = (count + round - 1) / round;
     if (rounds > 0xFFFFFFFFull)
         return CMD_E_ARG;

@@ -478,9 +478,12 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
     for (size_t c0 = 0; c0 < count; c0 += chunk) {
         const size_t n = std::min(chunk, count - c0);
         if (pieces) {
-            // pieces of a multiple of 256 ciphertexts: whole rounds, and every
-            // piece's ciphertexts start 16-byte aligned
-            const size_t per = (n + BATCH_STREAMS * 256 - 1) / (BATCH_STREAMS * 256) * 256;
+            // pieces of whole rounds of the size one launch over the chunk
+            // would use (equal shares per resident CTA when so tuned), so the
+            // pieces' rounds fill the same waves; a round is a multiple of 32
+            // ciphertexts, so every piece's ciphertexts start 16-byte aligned
+            const uint32_t round = fused_round(eng, key->dev.set, n);
+            const size_t per = (n + (size_t)BATCH_STREAMS * round - 1) / ((size_t)BATCH_STREAMS * round) * round;
             cudaError_t e = cudaSuccess;
             for (int i = 0; i < BATCH_STREAMS && e == cudaSuccess && rc == CMD_OK; i++) {
                 const size_t p0 = (size_t)i * per;
@@ -493,7 +496,7 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
                 if (e != cudaSuccess)
                     break;
                 rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, d_err + p0 * si.nw, d_w + p0, ps,
-                                       eng->tile_counter + 1 + i, nullptr, 0);
+                                       eng->tile_counter + 1 + i, nullptr, 0, round);
                 if (rc)
                     break;
                 e = cudaMemcpy2DAsync(h_err + (c0 + p0) * (si.n / 8), si.n / 8, d_err + p0 * si.nw, (size_t)si.nw * 4,
@@ -576,7 +579,8 @@ int cmd_decrypt_positions(cmd_engine *eng, const cmd_key *key, const uint8_t *h_
     for (size_t c0 = 0; c0 < count; c0 += chunk) {
         const size_t n = std::min(chunk, count - c0);
         if (pieces) {  // as in cmd_decrypt_batch
-            const size_t per = (n + BATCH_STREAMS * 256 - 1) / (BATCH_STREAMS * 256) * 256;
+            const uint32_t round = fused_round(eng, key->dev.set, n);
+            const size_t per = (n + (size_t)BATCH_STREAMS * round - 1) / ((size_t)BATCH_STREAMS * round) * round;
             cudaError_t e = cudaSuccess;
             for (int i = 0; i < BATCH_STREAMS && e == cudaSuccess && rc == CMD_OK; i++) {
                 const size_t p0 = (size_t)i * per;
@@ -589,7 +593,7 @@ int cmd_decrypt_positions(cmd_engine *eng, const cmd_key *key, const uint8_t *h_
                 if (e != cudaSuccess)
                     break;
                 rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, nullptr, nullptr, ps,
-                                       eng->tile_counter + 1 + i, d_pos + p0 * row, 0);
+                                       eng->tile_counter + 1 + i, d_pos + p0 * row, 0, round);
                 if (rc)
                     break;
                 e = cudaMemcpyAsync(h_pos + (c0 + p0) * row, d_pos + p0 * row, pn * row * 2, cudaMemcpyDeviceToHost,

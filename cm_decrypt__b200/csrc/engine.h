@@ -54,9 +54,14 @@ int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t
 int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                      uint16_t *d_weight, cudaStream_t s, uint16_t *d_pos = nullptr);
 // Explicit work counter and round schedule (balanced: -1 = the tuned choice,
-// 0 = full rounds, 1 = equal shares).
+// 0 = full rounds, 1 = equal shares; round_cts > 0 overrides all three with
+// rounds of that many ciphertexts, a multiple of 32 from fused_round).
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
-                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced);
+                      uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced,
+                      uint32_t round_cts = 0);
+// Ciphertexts per round of one launch over `count` ciphertexts of `set` under
+// the tuned schedule.
+uint32_t fused_round(cmd_engine *eng, int set, size_t count);
 int ensure_counter(cmd_engine *eng);  // eng->tile_counter: 64 u32 work counters
 constexpr int BATCH_STREAMS = 8;      // pieces of a host-buffer batch in flight
 size_t fused_smem(int set, int wpb);

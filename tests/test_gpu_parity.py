@@ -201,11 +201,13 @@ def test_full_size_properties(engine, keys, path):
     assert (w == 119).all()
 
 
-def test_host_batch_in_pieces(oracle_mod, engine, keys):
+@pytest.mark.parametrize("s", [460896, 6960119])
+def test_host_batch_in_pieces(oracle_mod, engine, keys, s):
     """A ragged host-buffer batch large enough to be split over the engine's
-    piece streams (four concurrent fused launches with their own counters)
-    equals the one-launch device path row for row."""
-    s = 460896
+    piece streams (eight concurrent fused launches with their own counters,
+    rounds sized as one launch over the batch would size them) equals the
+    one-launch device path row for row, for error vectors and for position
+    rows."""
     pk = cmd.PubKey(s, golden_sk(s))
     count = 4 * 8192 * 3 + 17
     cts, planted, valid = pk.ciphertexts(seed=5, count=count, malformed_permille=100)
@@ -221,6 +223,7 @@ def test_host_batch_in_pieces(oracle_mod, engine, keys):
     assert np.array_equal(d_w.cpu().numpy().view(np.uint16), w)
     bad = np.nonzero(valid == 0)[0][:64]
     assert np.array_equal(err[bad], oracle_mod.Oracle(s).decrypt(golden_sk(s), cts[bad], nthreads=8))
+    assert np.array_equal(cmd.decrypt_positions(engine, keys[s], cts), cmd.positions_from_errors(s, err))
 
 
 @pytest.mark.parametrize("s", SETS)
