@@ -46,6 +46,27 @@ template <int M> __device__ __forceinline__ uint32_t gf_mul(uint32_t a, uint32_t
     return gf_reduce<M>(p);
 }
 
+// The same product by integer multiplies on operands with holes (the
+// constant-time "ctmul" construction of T. Pornin's BearSSL GHASH): a and b
+// are split into four classes of bits, positions i = c (mod 4).  The integer
+// product of two classes counts, at each position, the bit pairs that meet
+// there; the four products landing on class k (i + j = k mod 4) sum to at
+// most 13 pairs per position, below 16, so no count reaches the class's next
+// position, and bit 0 of each count is the XOR.  16 multiply-adds (the FMA
+// pipe) and about 25 logic operations instead of 13 shift-and-mask steps on
+// the ALU pipe; multiplies take the same time for every operand.
+template <int M> __device__ __forceinline__ uint32_t gf_mul_im(uint32_t a, uint32_t b)
+{
+    constexpr uint32_t K0 = 0x11111111u, K1 = K0 << 1, K2 = K0 << 2, K3 = K0 << 3;
+    const uint32_t a0 = a & K0, a1 = a & K1, a2 = a & K2, a3 = a & K3;
+    const uint32_t b0 = b & K0, b1 = b & K1, b2 = b & K2, b3 = b & K3;
+    const uint32_t c0 = a0 * b0 + a1 * b3 + a2 * b2 + a3 * b1;
+    const uint32_t c1 = a0 * b1 + a1 * b0 + a2 * b3 + a3 * b2;
+    const uint32_t c2 = a0 * b2 + a1 * b1 + a2 * b0 + a3 * b3;
+    const uint32_t c3 = a0 * b3 + a1 * b2 + a2 * b1 + a3 * b0;
+    return gf_reduce<M>((c0 & K0) | (c1 & K1) | (c2 & K2) | (c3 & K3));
+}
+
 // Squaring is linear over GF(2): spread bit i to bit 2i, then reduce.
 template <int M> __device__ __forceinline__ uint32_t gf_sq(uint32_t a)
 {
@@ -68,19 +89,21 @@ template <int M, int K> __device__ __forceinline__ uint32_t gf_sqn(uint32_t a)
 // a^(2^M - 2) (= 1/a, and 0 -> 0) with an Itoh-Tsujii style chain:
 //   M = 13: a^3, a^15, a^255, a^4095, then one squaring  (4 mul, 12 sq)
 //   M = 12: a^3, a^7, a^15, a^255, a^2047, then one squaring (5 mul, 12 sq)
-template <int M> __device__ __forceinline__ uint32_t gf_inv(uint32_t a)
+// IM: the multiplies are gf_mul_im.
+template <int M, bool IM = false> __device__ __forceinline__ uint32_t gf_inv(uint32_t a)
 {
-    uint32_t a3 = gf_mul<M>(gf_sq<M>(a), a);
+    auto mul = [](uint32_t x, uint32_t y) { return IM ? gf_mul_im<M>(x, y) : gf_mul<M>(x, y); };
+    uint32_t a3 = mul(gf_sq<M>(a), a);
     if constexpr (M == 13) {
-        uint32_t a15 = gf_mul<M>(gf_sqn<M, 2>(a3), a3);
-        uint32_t a255 = gf_mul<M>(gf_sqn<M, 4>(a15), a15);
-        uint32_t a4095 = gf_mul<M>(gf_sqn<M, 4>(a255), a15);
+        uint32_t a15 = mul(gf_sqn<M, 2>(a3), a3);
+        uint32_t a255 = mul(gf_sqn<M, 4>(a15), a15);
+        uint32_t a4095 = mul(gf_sqn<M, 4>(a255), a15);
         return gf_sq<M>(a4095);
     } else {
-        uint32_t a7 = gf_mul<M>(gf_sq<M>(a3), a);
-        uint32_t a15 = gf_mul<M>(gf_sqn<M, 2>(a3), a3);
-        uint32_t a255 = gf_mul<M>(gf_sqn<M, 4>(a15), a15);
-        uint32_t a2047 = gf_mul<M>(gf_sqn<M, 3>(a255), a7);
+        uint32_t a7 = mul(gf_sq<M>(a3), a);
+        uint32_t a15 = mul(gf_sqn<M, 2>(a3), a3);
+        uint32_t a255 = mul(gf_sqn<M, 4>(a15), a15);
+        uint32_t a2047 = mul(gf_sqn<M, 3>(a255), a7);
         return gf_sq<M>(a2047);
     }
 }

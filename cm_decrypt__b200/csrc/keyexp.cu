@@ -56,7 +56,8 @@ template <int S> __global__ void __launch_bounds__(1024) k_support(KeyDev k)
 
 // Per support point: g(L_i) by Horner (root_13.c:216-230), 1/g(L_i)^2, and for
 // i < sb the syndrome-table row L_i^j / g(L_i)^2, j < 2t (util.c:86-100),
-// packed two coefficients per 32-bit word.
+// packed two coefficients per 32-bit word.  Multiplies by integer multiplies
+// on operands with holes (gf_mul_im).
 template <int S> __global__ void __launch_bounds__(256) k_key_tables(KeyDev k)
 {
     using P = Set<S>;
@@ -71,8 +72,8 @@ template <int S> __global__ void __launch_bounds__(256) k_key_tables(KeyDev k)
     const uint32_t a = k.L[i];
     uint32_t v = g[T];
     for (int j = T - 1; j >= 0; j--)
-        v = gf_mul<M>(v, a) ^ g[j];
-    const uint32_t inv = gf_inv<M>(gf_mul<M>(v, v));
+        v = gf_mul_im<M>(v, a) ^ g[j];
+    const uint32_t inv = gf_inv<M, true>(gf_mul_im<M>(v, v));
     k.ginv2[i] = (uint16_t)inv;
     if (i < P::SB) {
         uint32_t x = inv;
@@ -81,9 +82,9 @@ template <int S> __global__ void __launch_bounds__(256) k_key_tables(KeyDev k)
             row[w] = 0;
         for (int w = 0; w < P::TW; w++) {
             const uint32_t lo = x;
-            x = gf_mul<M>(x, a);
+            x = gf_mul_im<M>(x, a);
             const uint32_t hi = x;
-            x = gf_mul<M>(x, a);
+            x = gf_mul_im<M>(x, a);
             row[w] = lo | (hi << 16);
         }
     }

@@ -42,8 +42,8 @@
 // re-encodings against: kg_pubkey_columns.
 //
 // Not all constant-time.  All field arithmetic is table-free: the Goppa
-// polynomial uses the decrypt path's shift-and-mask multiply and inversion
-// (its zero-pivot fix-up is a masked row sum), and the support stage (sort, L,
+// polynomial uses a multiply by integer multiplies on operands with holes and
+// the inversion chain over it (its zero-pivot fix-up is a masked row sum), and the support stage (sort, L,
 // g(L), 1/g(L), the parity-check matrix) is bitonic sorting plus the bitsliced
 // routines.  The elimination reads the rows it chooses and indexes its
 // combination tables by panel words, and the control-bit recursion indexes
@@ -313,9 +313,9 @@ size_t genpoly_smem(const KgDims &d) { return (size_t)d.t * (d.t + 1) * 2 + 5 * 
 
 // One CTA per chain entry (key keys[blockIdx.x / SPEC], attempt
 // blockIdx.x % SPEC): reads f from the entry's expansion, writes g and the
-// attempt's status beside it.  Field arithmetic is the decrypt path's
-// shift-and-mask multiply and inversion chain (no tables); memory addresses
-// depend only on loop indices.
+// attempt's status beside it.  Field arithmetic is table-free: the multiply
+// by integer multiplies on operands with holes (gf_mul_im) and the inversion
+// chain over it; memory addresses depend only on loop indices.
 template <int M>
 __device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t r_al)
 {
@@ -358,7 +358,7 @@ __device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t
             if (ko < 2 * t - 1) {
                 const int lo = max(0, ko - t + 1), hi = min(ko, t - 1);
                 for (int i = lo + part; i <= hi; i += 4)
-                    acc ^= gf_mul<M>(pw[i], f[ko - i]);
+                    acc ^= gf_mul_im<M>(pw[i], f[ko - i]);
             }
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 1);
             acc ^= __shfl_xor_sync(0xFFFFFFFFu, acc, 2);
@@ -373,7 +373,7 @@ __device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t
             for (int u = 0; u < F.nt; u++) {
                 const int i = tid - F.off[u];
                 if (i >= 0 && i <= t - 2)
-                    acc ^= gf_mul<M>(pr[t + i], F.c[u]);
+                    acc ^= gf_mul_im<M>(pr[t + i], F.c[u]);
             }
             v1[tid] = (uint16_t)acc;
         }
@@ -383,7 +383,7 @@ __device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t
             for (int u = 0; u < F.nt; u++) {
                 const int i = tid - F.off[u];
                 if (i >= 0 && i < offmax)
-                    acc ^= gf_mul<M>(v1[t + i], F.c[u]);
+                    acc ^= gf_mul_im<M>(v1[t + i], F.c[u]);
             }
             pw[tid] = (uint16_t)acc;
         }
@@ -422,17 +422,17 @@ __device__ void genpoly_body(uint8_t *eb, uint8_t *smem, const KgDims &d, size_t
             A[c * W + x] = (uint16_t)acc;
         }
         __syncthreads();
-        const uint32_t inv = gf_inv<M>(A[c * W + c]);  // 0 when singular (then s_ok = 0)
+        const uint32_t inv = gf_inv<M, true>(A[c * W + c]);  // 0 when singular (then s_ok = 0)
         __syncthreads();
         if (tid >= c && tid <= t)
-            A[c * W + tid] = (uint16_t)gf_mul<M>(A[c * W + tid], inv);
+            A[c * W + tid] = (uint16_t)gf_mul_im<M>(A[c * W + tid], inv);
         if (tid < t)
             col[tid] = tid == c ? 0 : A[tid * W + c];
         __syncthreads();
         for (int r = warp; r < t; r += GP_THREADS / 32) {
             const uint32_t k = col[r];
             for (int x = c + lane; x <= t; x += 32)
-                A[r * W + x] ^= (uint16_t)gf_mul<M>(A[c * W + x], k);
+                A[r * W + x] ^= (uint16_t)gf_mul_im<M>(A[c * W + x], k);
         }
         __syncthreads();
     }
