@@ -699,12 +699,22 @@ __global__ void __launch_bounds__(PANEL_THREADS) k_ge_panel(uint8_t *__restrict_
         used[s_src[tid]] = 1;
     }
     __syncthreads();
-    if (tid == 0) {
-        pi->npiv = npiv;
+    if (tid < 32) {
+        // the first row not yet used, 32 rows per ballot (rows past mt stop it)
         int z = pi->scan0;
-        while (z < d.mt && used[z])
-            z++;
-        pi->scan0 = z;
+        for (;;) {
+            const int r = z + lane;
+            const uint32_t free_rows = __ballot_sync(0xFFFFFFFFu, r >= d.mt || !used[r]);
+            if (free_rows) {
+                z += __ffs(free_rows) - 1;
+                break;
+            }
+            z += 32;
+        }
+        if (lane == 0) {
+            pi->npiv = npiv;
+            pi->scan0 = min(z, d.mt);
+        }
     }
     // copies of the chosen rows, 16-byte columns from word p & ~3 (the
     // update's layout), four loads in flight per thread
