@@ -66,6 +66,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--keygen-only", action="store_true",
                     help="run only the key-generation leg and print its JSON (for profiling)")
     ap.add_argument("--keygen-count", type=int, default=64, help="seeds in the key-generation batch")
+    ap.add_argument("--no-reference-check", action="store_true",
+                    help="skip comparing every mixed-batch and serving row with the reference CPU decoder")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the all-sets (2^20 each) and mixed-batch (2^18) measurements")
     return ap.parse_args()
@@ -157,13 +159,17 @@ SERVER_CONFIG = {"max_batch": 8192, "slots": 8, "max_wait_us": 150, "fused_thres
 
 
 def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: int = 16384,
-                server_config: dict | None = None) -> dict:
+                server_config: dict | None = None, reference_check: bool = True) -> dict:
     """Serving workload: Poisson arrivals over `nkeys` seeded keys drawn from
     the five sets weighted 30/15/20/20/15, 5% malformed ciphertexts, keys
     device-resident, continuous batching.  Returns per-rate p50/p99 latency and
-    sustained decaps/s; valid requests are checked against their planted
-    error vectors."""
+    sustained decaps/s.  Every result row a rate wrote, valid and malformed,
+    is compared with the reference's own CPU decoder (oracle/_ref, decoded
+    once for the request pool), the valid ones also with their planted
+    vectors."""
     import concurrent.futures as cf
+
+    from oracle import oracle as o
     golden = {s: open(os.path.join(REPO, "tests", "golden", "kem", f"sk_{s}.bin"), "rb").read() for s in SERVE_SETS}
     counts = [round(nkeys * w / 100) for w in SERVE_WEIGHTS]
     counts[0] += nkeys - sum(counts)
@@ -191,6 +197,11 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
         planted[idx, : e.shape[1]] = e
         valid[idx] = v
     out = {"keys": len(keys), "keygen_s": keygen_s, "malformed_fraction": float(1 - valid.mean()), "points": []}
+    ref = None
+    if reference_check:
+        t0 = time.perf_counter()
+        ref, kind = o.reference_decrypt_rows([(s, sk) for s, sk, _ in keys], key_of, cts)
+        out["reference_check"] = {"checker": kind, "pool_rows": pool, "seconds": time.perf_counter() - t0}
     cfg = dict(SERVER_CONFIG, **(server_config or {}))
     out["server_config"] = cfg
     with cmd.Server(eng, record_completions=False, **cfg) as srv:
@@ -201,19 +212,26 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
         for rate in rates:
             err_pool[:] = 0
             st = srv.loadgen(ids[key_of], cts, err_pool, rate=rate, seconds=seconds)
-            # loadgen request i writes row i % pool: check the valid rows written
-            written = np.nonzero(valid[: min(int(st["completed"]), pool)])[0][:4000]
-            ok = bool(written.size > 0 and all(np.array_equal(err_pool[i, :1024], planted[i]) for i in written))
-            out["points"].append({"offered_per_s": st["offered_per_s"], "decaps_per_s": st["decaps_per_s"],
-                                  "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
-                                  "max_ms": st["max_us"] / 1e3, "mean_batch": st["mean_batch"],
-                                  "batches": st["batches"], "fused_batches": st["fused_batches"],
-                                  "refused": st["refused"], "results_match_planted": ok,
-                                  "gpu_batch_p50_ms": st["gpu_p50_us"] / 1e3,
-                                  "gpu_batch_p99_ms": st["gpu_p99_us"] / 1e3,
-                                  "wait_p50_ms": st["wait_p50_us"] / 1e3, "wait_p99_ms": st["wait_p99_us"] / 1e3,
-                                  "dispatch_busy": st["dispatch_busy"], "complete_busy": st["complete_busy"],
-                                  "mean_inflight": st["mean_inflight"]})
+            # loadgen request i writes row i % pool
+            written = min(int(st["completed"]), pool)
+            vrows = np.nonzero(valid[:written])[0]
+            ok = bool(vrows.size > 0 and np.array_equal(err_pool[vrows], planted[vrows]))
+            pt = {"offered_per_s": st["offered_per_s"], "decaps_per_s": st["decaps_per_s"],
+                  "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                  "max_ms": st["max_us"] / 1e3, "mean_batch": st["mean_batch"],
+                  "batches": st["batches"], "fused_batches": st["fused_batches"],
+                  "refused": st["refused"], "results_match_planted": ok,
+                  "gpu_batch_p50_ms": st["gpu_p50_us"] / 1e3,
+                  "gpu_batch_p99_ms": st["gpu_p99_us"] / 1e3,
+                  "wait_p50_ms": st["wait_p50_us"] / 1e3, "wait_p99_ms": st["wait_p99_us"] / 1e3,
+                  "dispatch_busy": st["dispatch_busy"], "complete_busy": st["complete_busy"],
+                  "mean_inflight": st["mean_inflight"]}
+            if ref is not None:
+                same = (err_pool[:written] == ref[:written]).all(axis=1)
+                pt["rows_checked_vs_reference"] = written
+                pt["malformed_rows_checked"] = int((valid[:written] == 0).sum())
+                pt["bit_exact_vs_reference"] = bool(same.all() and st["refused"] == 0)
+            out["points"].append(pt)
     under = [p for p in out["points"] if p["p99_ms"] < 1.0]
     out["max_decaps_per_s_p99_under_1ms"] = max((p["decaps_per_s"] for p in under), default=None)
     return out
@@ -357,13 +375,16 @@ def keygen_leg(cmd, eng, set_id: int = 6960119, count: int = 64, cpu_seconds: fl
     return out
 
 
-def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3) -> dict:
+def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: int = 3,
+                 reference_check: bool = True) -> dict:
     """Mixed batch: 64 seeded keys spread 13/13/13/13/12 over the five
     sets, `count` ciphertexts with the set drawn uniformly per ciphertext (key
     uniform within the set), 10% uniformly random mt-bit strings, all in one
-    cmd_decrypt_mixed_device launch.  Valid ciphertexts are checked against
-    their planted vectors; malformed ones must not decode to weight t."""
+    cmd_decrypt_mixed_device launch.  Every row, valid and malformed, is
+    compared with the reference's own CPU decoder (oracle/_ref, all host
+    threads), and the valid ones also with their planted vectors."""
     import torch
+    from oracle import oracle as o
     golden = {s: open(os.path.join(REPO, "tests", "golden", "kem", f"sk_{s}.bin"), "rb").read() for s in SERVE_SETS}
     per_set = [nkeys // 5 + (1 if i < nkeys % 5 else 0) for i in range(5)]
     ring = [(s, cmd.synth_key(s, golden[s], 0xC0FFEE + 97 * i + j)) for i, s in enumerate(SERVE_SETS)
@@ -395,52 +416,104 @@ def config_mixed(cmd, eng, stream, nkeys: int = 64, count: int = 1 << 18, reps: 
                                                        err_off, d_w.data_ptr(), sp), stream, reps, 2)
     E = d_err.cpu().numpy().astype("<u4").view(np.uint8).reshape(count, 1024)
     W = d_w.cpu().numpy().view(np.uint16)
+    for k in keys:
+        k.free()
     ok = True
     t_of = np.array([cmd.set_info(s).t for s, _ in ring])[key_idx]
     for i, s in enumerate(SERVE_SETS):
         rows = np.nonzero((valid == 1) & (set_of == i))[0]
         nb = cmd.set_info(s).err_bytes
         ok = ok and bool(np.array_equal(E[rows, :nb], planted[rows, :nb]) and (W[rows] == t_of[rows]).all())
-    bad = np.nonzero(valid == 0)[0]
-    for k in keys:
-        k.free()
-    return {"keys": len(keys), "ciphertexts": count, "malformed_fraction": float(1 - valid.mean()),
-            "ms_per_launch": ms, "decaps_per_s": count / (ms * 1e-3),
-            "valid_match_planted": ok, "malformed_below_weight_t": bool((W[bad] < t_of[bad]).all()),
-            "timed": "whole cmd_decrypt_mixed_device call: host round planning, plan upload and the fused kernel"}
+    out = {"keys": len(keys), "ciphertexts": count, "malformed_fraction": float(1 - valid.mean()),
+           "ms_per_launch": ms, "decaps_per_s": count / (ms * 1e-3), "valid_match_planted": ok,
+           "timed": "whole cmd_decrypt_mixed_device call: host round planning, plan upload and the fused kernel"}
+    if reference_check:
+        t0 = time.perf_counter()
+        ref, kind = o.reference_decrypt_rows(ring, key_idx, buf)
+        weights = np.unpackbits(ref, axis=1).sum(axis=1)
+        same = (E == ref).all(axis=1) & (W == weights)
+        out["reference_check"] = {
+            "checker": kind, "rows": int(count), "rows_equal": int(same.sum()),
+            "malformed_rows_equal": int(same[valid == 0].sum()), "malformed_rows": int((valid == 0).sum()),
+            "seconds": time.perf_counter() - t0, "threads": os.cpu_count() or 1}
+        out["bit_exact_vs_reference"] = bool(same.all())
+    return out
+
+
+ERR_WORDS = 218  # u32 words of a mceliece6960119 error row (n = 6960 bits)
+CT_BYTES = 194
+
+
+def rotating_buffers(count: int) -> tuple[int, int]:
+    """Device buffer sets the GPU arm rotates through so that no step finds
+    its inputs or outputs in L2: (sets, bytes per set)."""
+    per_set = count * (CT_BYTES + 4 * ERR_WORDS + 2)
+    return max(2, math.ceil(2 * L2_BYTES / per_set)), per_set
+
+
+def workload_config(count: int, world: int) -> dict:
+    """The workload both arms name (the reference arm times a bounded sample
+    of the same batch on the host cores)."""
+    nbuf, per_set = rotating_buffers(count)
+    return {"workload": "mceliece6960119 decrypt, 1 seeded key (reference kem/ key), "
+                        f"{count} ciphertexts/step/GPU, uniform weight-119 errors",
+            "set": SET, "ciphertexts_per_step": count, "parallelism": f"replicas x{world}",
+            "l2": f"inputs larger than L2: the GPU arm rotates {nbuf} device-resident buffer sets "
+                  f"({nbuf * per_set / 2**20:.0f} MiB > 2x L2)"}
 
 
 def run_reference(args) -> None:
+    """The reference's own CPU decoder (CPU/ sources compiled unmodified into
+    oracle/_ref by oracle/Makefile; the oracle restatement if that build is
+    absent) on all host cores.  Its inputs come from the oracle alone: the
+    public key of the kem/ key regenerated from the seed stored in it
+    (crypto_kem_keypair), weight-119 error vectors and their encryptions
+    (encrypt.c's syndrome rule).  Each step decodes a bounded sample of the
+    workload's batch, sized so that the whole run stays within minutes, and
+    every decoded vector is checked against the one encrypted."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    import cm_decrypt__b200 as cmd
     from oracle import oracle as o
     sk = open(KEM_SK, "rb").read()
-    pk = cmd.PubKey(SET, sk)
+    orc = o.Oracle(SET)
+    pk, sk_again, _ = orc.keypair(sk[:32])
+    if sk_again != sk:
+        raise SystemExit("reference arm: the kem/ key does not regenerate from its seed")
     cores = os.cpu_count() or 1
     kind = "reference" if o.RefLib.available(SET) else "port"
-    dec = o.RefLib(SET) if kind == "reference" else o.Oracle(SET)
-    per_step = max(cores, 8) * 4
-    cts, planted, _ = pk.ciphertexts(seed=1, count=per_step)
+    dec = o.RefLib(SET) if kind == "reference" else orc
+    probe_e = orc.random_errors(seed=rank_seed(0) + 7, count=2 * cores)
+    probe = orc.encrypt(pk, probe_e)
+    t0 = time.perf_counter()
+    dec.decrypt(sk, probe, nthreads=cores)
+    rate = probe.shape[0] / (time.perf_counter() - t0)
+    # about 1.5 s of decoding per step, whole rounds of `cores` ciphertexts
+    per_step = int(min(args.count, max(cores, round(1.5 * rate / cores) * cores)))
+    planted = orc.random_errors(seed=rank_seed(0), count=per_step)
+    cts = orc.encrypt(pk, planted)
     for _ in range(args.warmup):
         dec.decrypt(sk, cts, nthreads=cores)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         got = dec.decrypt(sk, cts, nthreads=cores)
     dt = time.perf_counter() - t0
-    assert np.array_equal(got, planted)
+    if not np.array_equal(got, planted):
+        raise SystemExit("reference arm: decoded vectors differ from the encrypted ones")
     v = per_step * args.steps / dt
+    sample = (f"{per_step} of the {args.count} mceliece6960119 ciphertexts of a step, decoded on {cores} "
+              f"host threads, every step")
     line = {
-        "impl": "reference", "metric": "decaps/s", "value": v, "unit": "decaps/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": "decaps/s", "value": v, "unit": "decaps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16/u32 GF(2^13)",
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16 GF(2^13)",
         "data": "synthetic",
-        "config": {"workload": "mceliece6960119 decrypt, 1 seeded key, uniform weight-119 errors",
-                   "sample_per_step": per_step},
-        "cpu_baseline": {"value": v, "unit": "decaps/s", "cores": cores, "kind": kind,
-                         "sample": f"{per_step} ciphertexts per step, {cores} threads"},
+        "config": workload_config(args.count, world),
+        "sample": sample,
+        "cpu_baseline": {"value": v, "unit": "decaps/s", "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": "decaps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "results_match_planted": True,
     }
     print(json.dumps(line), flush=True)
 
@@ -480,8 +553,8 @@ def main() -> None:
 
     # Rotating device buffer sets, together larger than 2x L2, so no step
     # reads inputs or writes outputs the previous step left in L2.
-    per_set = count * (info.ct_bytes + 4 * info.err_words + 2)
-    nbuf = max(2, math.ceil(2 * L2_BYTES / per_set))
+    assert info.ct_bytes == CT_BYTES and info.err_words == ERR_WORDS
+    nbuf, per_set = rotating_buffers(count)
     d_cts = [torch.from_numpy(cts).cuda() for _ in range(nbuf)]
     d_err = [torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda") for _ in range(nbuf)]
     d_w = [torch.zeros(count, dtype=torch.int16, device="cuda") for _ in range(nbuf)]
@@ -607,9 +680,15 @@ def main() -> None:
     w = work_per_decap(SET)
     achieved = per_rank * w["total"]
     hbm = per_rank * hbm_bytes_per_decap(SET)
-    traffic = None
+    traffic, traffic_detail = None, None
     if os.path.exists(TRAFFIC_FILE):
-        traffic = json.load(open(TRAFFIC_FILE)).get("dram_bytes_per_launch_scaled")
+        # dram__bytes_read.sum + dram__bytes_write.sum of one captured launch,
+        # per launch of this batch, with how the capture was scaled
+        tr = json.load(open(TRAFFIC_FILE))
+        traffic = tr.get("dram_bytes_per_launch")
+        traffic_detail = {k: tr[k] for k in ("dram_read_bytes_per_launch", "dram_write_bytes_per_launch",
+                                             "algorithmic_bytes_per_launch", "captured_cts", "scaling",
+                                             "source") if k in tr}
     peaks = {}
     pk_path = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(pk_path):
@@ -620,10 +699,7 @@ def main() -> None:
         "metric": "decaps/s", "value": value, "unit": "decaps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u32 bitsliced GF(2^13)", "data": "synthetic",
-        "config": {"workload": "mceliece6960119 fused decrypt, 1 seeded key (reference kem/ key), "
-                               f"{count} ciphertexts/step/GPU, uniform weight-119 errors",
-                   "set": SET, "ciphertexts_per_step": count, "parallelism": f"replicas x{world}",
-                   "l2": f"rotating {nbuf} resident buffer sets ({nbuf * per_set / 2**20:.0f} MiB > 2x L2)"},
+        "config": workload_config(count, world),
         "gpu_launches": launches,
         "plain": None if ms_plain is None else {
             "value": job_rate(world, count * min(args.steps, 3), ms_plain * 1e-3),
@@ -647,7 +723,7 @@ def main() -> None:
                                            "equivalent lane-ops/s at this decap rate",
                                    "equivalent": per_rank * w["yardstick_total"] / 1e12,
                                    "x_peak": per_rank * w["yardstick_total"] / int_peak},
-                     "traffic": traffic,
+                     "traffic": traffic, "traffic_detail": traffic_detail,
                      "hbm": {"achieved_gbs": hbm / 1e9, "peak_gbs": hbm_peak, "frac": hbm / 1e9 / hbm_peak,
                              "bytes_per_decap": hbm_bytes_per_decap(SET)}},
         "clocks": clocks,
@@ -657,7 +733,8 @@ def main() -> None:
         line["cpu_baseline"] = cpu_reference(sk, cts)
     if world == 1 and not args.no_configs:
         line["configs"] = {"all_sets_2^20": config_all_sets(cmd, eng, stream),
-                           "mixed_64keys_2^18": config_mixed(cmd, eng, stream)}
+                           "mixed_64keys_2^18": config_mixed(cmd, eng, stream,
+                                                             reference_check=not args.no_reference_check)}
     for g_ in graphs:
         g_.close()
     if world == 1 and not args.no_keygen:
@@ -665,7 +742,8 @@ def main() -> None:
     if world == 1 and not args.no_serve:
         fused_rate = value
         rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, round(0.5 * fused_rate, -5)})
-        line["serving"] = serving_leg(cmd, eng, args.serve_keys, rates, args.serve_seconds)
+        line["serving"] = serving_leg(cmd, eng, args.serve_keys, rates, args.serve_seconds,
+                                      reference_check=not args.no_reference_check)
         line["serving"]["fused_batch_decaps_per_s"] = fused_rate
         best = line["serving"]["max_decaps_per_s_p99_under_1ms"]
         line["serving"]["frac_of_fused_at_p99_under_1ms"] = None if best is None else best / fused_rate

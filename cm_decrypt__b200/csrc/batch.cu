@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -83,14 +84,19 @@ int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
     const int wpb = eng->fcfg[set].wpb;
-    if (round_cts % 32 != 0 || round_cts > (uint32_t)wpb * 32)
+    if (round_cts % 32 != 0 || round_cts > (uint32_t)wpb * 32) {
+        set_last_error("fused round of " + std::to_string(round_cts) +
+                       " ciphertexts: must be a multiple of 32 and at most " + std::to_string(wpb * 32));
         return CMD_E_ARG;
+    }
     const uint32_t round = round_cts ? round_cts
                                      : round_size(eng, set, wpb, count,
                                                   balanced < 0 ? eng->fcfg[set].balanced : balanced != 0);
     const uint64_t rounds = (count + round - 1) / round;
-    if (rounds > 0xFFFFFFFFull)
+    if (rounds > 0xFFFFFFFFull) {
+        set_last_error("batch needs more than 2^32 fused rounds");
         return CMD_E_ARG;
+    }
     FusedArgs a;
     memset(&a, 0, sizeof a);
     a.tiles = nullptr;
@@ -190,17 +196,24 @@ extern "C" int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *k
         return CMD_E_ARG;
     if (count == 0)
         return CMD_OK;
-    if (count > 0xFFFFFFFFull || nkeys > 0xFFFFFFFFull)
+    if (count > 0xFFFFFFFFull || nkeys > 0xFFFFFFFFull) {
+        set_last_error("mixed batch: more than 2^32 ciphertexts or keys");
         return CMD_E_ARG;
+    }
     for (size_t k = 0; k < nkeys; k++)
-        if (!keys[k] || keys[k]->eng != eng)
+        if (!keys[k] || keys[k]->eng != eng) {
+            set_last_error("mixed batch: key " + std::to_string(k) + " is null or belongs to another engine");
             return CMD_E_ARG;
+        }
     cudaSetDevice(eng->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : eng->stream;
 
     for (size_t c = 0; c < count; c++)
-        if (h_key_idx[c] >= nkeys)
+        if (h_key_idx[c] >= nkeys) {
+            set_last_error("mixed batch: ciphertext " + std::to_string(c) + " names key " +
+                           std::to_string(h_key_idx[c]) + " of " + std::to_string(nkeys));
             return CMD_E_ARG;
+        }
     std::vector<int> kset(nkeys);
     for (size_t k = 0; k < nkeys; k++)
         kset[k] = keys[k]->dev.set;

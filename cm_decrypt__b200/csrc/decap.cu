@@ -216,10 +216,10 @@ int cmd_key_prepare_decap(cmd_engine *eng, cmd_key *key)
 {
     if (!eng || !key || key->eng != eng)
         return CMD_E_ARG;
-    // one preparation at a time, so that two first calls for a key derive
-    // its columns once
-    static std::mutex prep_mu;
-    std::lock_guard<std::mutex> lk(prep_mu);
+    // one preparation at a time per key, so that two first calls for a key
+    // derive its columns once (keys of other engines and devices prepare in
+    // parallel); taken before eng->mu, which kg_pubkey_columns takes
+    std::lock_guard<std::mutex> lk(key->prep_mu);
     if (key->pk)
         return CMD_OK;
     const int set = key->dev.set;

@@ -172,6 +172,11 @@ int cmd_engine_create(int device, size_t hbm_budget_bytes, cmd_engine **out)
         return cuda_fail(e, "cudaStreamCreate");
     }
     snprintf(eng->gpu_name, sizeof eng->gpu_name, "%s", prop.name);
+    if (int rc = noalloc_setup(device)) {
+        cudaStreamDestroy(eng->stream);
+        delete eng;
+        return rc;
+    }
     if (int rc = upload_fft_plans(eng)) {
         cudaStreamDestroy(eng->stream);
         delete eng;

@@ -73,6 +73,10 @@ void plan_mixed(const int *key_set, size_t nkeys, const uint32_t *key_idx, size_
                 std::vector<uint32_t> &order, std::vector<FusedTile> &tiles);
 // Root-search tables (fft_plan.cpp): uploaded once per engine, budget-charged.
 int upload_fft_plans(cmd_engine *eng);
+// No-allocation path (noalloc.cu): with `device` current, looks up the
+// scratch array's device address and loads the plain kernels, so that
+// cmd_decrypt_plain_noalloc itself loads and allocates nothing.
+int noalloc_setup(int device);
 void release_fft_plans(cmd_engine *eng);
 inline FusedKeyRef key_ref(const KeyDev &k) { return FusedKeyRef{k.set, 0, k.tab, k.Lbs, k.bctl}; }
 
@@ -116,4 +120,5 @@ struct cmd_key {
     size_t bytes = 0;
     uint32_t *pk = nullptr;  // decapsulation: T block of the public key, column-major
     size_t pk_bytes = 0;
+    std::mutex prep_mu;      // cmd_key_prepare_decap, per key (before eng->mu)
 };

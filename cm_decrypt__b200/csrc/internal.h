@@ -55,6 +55,7 @@ cudaError_t launch_root_plain(const KeyDev &k, const uint16_t *d_loc, size_t cou
                               LaunchCounter lc, int num_sms);
 cudaError_t launch_root_images(const KeyDev &k, const uint16_t *d_loc, size_t count,
                                uint16_t *d_images, cudaStream_t s, LaunchCounter lc);
+cudaError_t preload_plain_kernels();
 
 // Fused path: one work item = up to 32 ciphertexts of one key.
 struct FusedTile {

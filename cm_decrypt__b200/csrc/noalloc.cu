@@ -11,13 +11,15 @@
 // every GPU that loads the library holds the array until the process exits.
 //
 // Host code cannot use the array's name as a device address (it names a host
-// shadow), so the first call on each device, with that device current, asks
-// the runtime for the array's device address with cudaGetSymbolAddress and
-// caches it.  That first call should therefore be made before any stream
-// capture begins.  Calls share the array and it keeps the previous call's
-// contents; the kernels overwrite every syndrome and locator entry they later
-// read, so nothing needs clearing, but calls that overlap on the GPU (other
-// streams or threads at the same time) race on it.
+// shadow), so cmd_engine_create, with the engine's device current, asks the
+// runtime for the array's device address with cudaGetSymbolAddress and
+// caches it per device.  With lazy module loading (the CUDA 12 default) that
+// lookup is also what loads the array onto the device, and engine creation
+// loads the plain kernels the same way, so the entry point itself neither
+// loads a module nor allocates.  Calls share the array and it keeps the
+// previous call's contents; the kernels overwrite every syndrome and locator
+// entry they later read, so nothing needs clearing, but calls that overlap
+// on the GPU (other streams or threads at the same time) race on it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -39,8 +41,9 @@ constexpr int NA_MAX_DEVICES = 64;
 static std::mutex g_na_mu;
 static void *g_na_ptr[NA_MAX_DEVICES];
 
-// Device address of the scratch array on `device` (set up once per device).
-static int noalloc_scratch(int device, uint8_t **out)
+// Called by cmd_engine_create with `device` current: the scratch array's
+// device address (once per device) and the plain kernels' module.
+int noalloc_setup(int device)
 {
     if (device < 0 || device >= NA_MAX_DEVICES) {
         set_last_error("device index out of range for the no-alloc path");
@@ -48,20 +51,23 @@ static int noalloc_scratch(int device, uint8_t **out)
     }
     std::lock_guard<std::mutex> lk(g_na_mu);
     if (!g_na_ptr[device]) {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        cudaError_t e = cudaSetDevice(device);
         void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e == cudaSuccess)
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (cur >= 0 && cur != device)
-            cudaSetDevice(cur);
+            e = preload_plain_kernels();
         if (e != cudaSuccess)
-            return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+            return cuda_fail(e, "no-alloc scratch set-up");
         g_na_ptr[device] = p;
     }
-    *out = static_cast<uint8_t *>(g_na_ptr[device]);
     return CMD_OK;
+}
+
+static uint8_t *noalloc_scratch(int device)
+{
+    if (device < 0 || device >= NA_MAX_DEVICES)
+        return nullptr;
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    return static_cast<uint8_t *>(g_na_ptr[device]);
 }
 
 }  // namespace cmd
@@ -81,19 +87,27 @@ extern "C" int cmd_decrypt_plain_noalloc(const cmd_key *key, const uint8_t *d_ct
     if (count == 0)
         return CMD_OK;
     cmd_engine *eng = key->eng;
-    uint8_t *base = nullptr;
-    int rc = noalloc_scratch(eng->device, &base);
-    if (rc)
-        return rc;
-    cudaSetDevice(eng->device);
+    uint8_t *base = noalloc_scratch(eng->device);
+    if (!base) {
+        set_last_error("no-alloc scratch not set up on this device (cmd_engine_create does it)");
+        return CMD_E_ARG;
+    }
+    // the caller's current device is put back before returning
+    int caller_dev = -1;
+    cudaGetDevice(&caller_dev);
+    if (caller_dev != eng->device)
+        cudaSetDevice(eng->device);
     cudaStream_t s = stream ? (cudaStream_t)stream : eng->stream;
     uint32_t *synd = reinterpret_cast<uint32_t *>(base);
     uint16_t *loc = reinterpret_cast<uint16_t *>(base + NA_SYND_BYTES);
     LaunchCounter lc{&eng->launches};
     cudaError_t e;
+    int rc = CMD_OK;
     if ((e = launch_synd_plain(key->dev, d_cts, count, synd, s, lc)) != cudaSuccess ||
         (e = launch_bm_plain(key->dev.set, reinterpret_cast<uint16_t *>(synd), count, loc, s, lc)) != cudaSuccess ||
         (e = launch_root_plain(key->dev, loc, count, d_err, d_weight, s, lc, eng->num_sms)) != cudaSuccess)
-        return cuda_fail(e, "no-alloc plain path launch");
-    return CMD_OK;
+        rc = cuda_fail(e, "no-alloc plain path launch");
+    if (caller_dev >= 0 && caller_dev != eng->device)
+        cudaSetDevice(caller_dev);
+    return rc;
 }

@@ -292,6 +292,27 @@ cudaError_t launch_root_plain(const KeyDev &k, const uint16_t *d_loc, size_t cou
     });
 }
 
+// Loads the plain kernels' module on the current device now (with lazy
+// module loading, the default, a kernel's module is otherwise loaded, and its
+// memory allocated, by its first launch).
+cudaError_t preload_plain_kernels()
+{
+    cudaError_t e = cudaSuccess;
+    auto one = [&](const void *f) {
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess)
+            e = cudaFuncGetAttributes(&fa, f);
+    };
+    for (int set = 0; set < NSETS; set++)
+        dispatch_set(set, [&]<int S>() {
+            one((const void *)k_synd_plain<S>);
+            one((const void *)k_bm_plain<S>);
+            one((const void *)k_root_plain<S>);
+            return 0;
+        });
+    return e;
+}
+
 cudaError_t launch_root_images(const KeyDev &k, const uint16_t *d_loc, size_t count, uint16_t *d_images,
                                cudaStream_t s, LaunchCounter lc)
 {

@@ -143,11 +143,12 @@ int cmd_decrypt_mixed_device(cmd_engine *eng, const cmd_key *const *keys,
  * every GPU that loads the library until the process exits).  The caller
  * passes the expanded key, device ciphertexts (count * ct_bytes) and device
  * outputs (count rows of err_words words; weights may be NULL).  count above
- * the maximum returns CMD_E_ARG.  The first call on a device looks up the
- * array's device address, so make that first call before any stream
- * capture begins.  Calls share the array: calls that overlap on the GPU
- * (concurrent streams or threads) race, so serialise them.  Asynchronous on
- * `stream` (NULL = the key's engine stream). */
+ * the maximum returns CMD_E_ARG.  cmd_engine_create looks up the array's
+ * device address and loads the array and the plain kernels onto the device,
+ * so the call itself loads and allocates nothing.  Calls share the array:
+ * calls that overlap on the GPU (concurrent streams or threads) race, so
+ * serialise them.  The caller's current device is left as it was.
+ * Asynchronous on `stream` (NULL = the key's engine stream). */
 #define CMD_NOALLOC_MAX_CTS 4096
 int cmd_decrypt_plain_noalloc(const cmd_key *key, const uint8_t *d_cts,
                               size_t count, uint32_t *d_err,

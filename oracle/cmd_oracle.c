@@ -676,3 +676,81 @@ void o_kg_controlbits(int m, const int16_t *pi, uint8_t *out)
     cb_rec(out, 0, 1, pi, m, n, ws);
     free(ws);
 }
+
+/* Niederreiter encryption of given error vectors with a public key: the
+ * syndrome rule of kem/common/core/encrypt.c:87-120, where row i of H is the
+ * pk row i placed in the last (n-mt+7)/8 bytes of an n-bit row with identity
+ * bit i set, and ciphertext bit i = <row i, e>.  Computed column-wise: the
+ * ciphertext is the XOR of the columns of H at the set bits of e. */
+int o_encrypt_batch(const o_params *p, const uint8_t *pk, const uint8_t *errs, size_t count, uint8_t *cts)
+{
+    const int m = p->m, n = p->n, mt = m * p->t, nbytes = n / 8, row_b = (n - mt + 7) / 8;
+    const int first = 8 * (nbytes - row_b), cb = p->ct_bytes;
+    uint8_t *cols = (uint8_t *)calloc((size_t)(n - first) * (size_t)cb, 1);
+    if (!cols)
+        return -1;
+    for (int i = 0; i < mt; i++) {
+        const uint8_t *row = pk + (size_t)i * row_b;
+        for (int j = first; j < n; j++) {
+            const int b = j - first;
+            int bit = (row[b >> 3] >> (b & 7)) & 1;
+            if (j == i)
+                bit = 1;
+            if (bit)
+                cols[(size_t)(j - first) * cb + (i >> 3)] |= (uint8_t)(1u << (i & 7));
+        }
+    }
+    for (size_t c = 0; c < count; c++) {
+        const uint8_t *e = errs + c * (size_t)nbytes;
+        uint8_t *ct = cts + c * (size_t)cb;
+        memset(ct, 0, (size_t)cb);
+        for (int j = 0; j < n; j++) {
+            if (!((e[j >> 3] >> (j & 7)) & 1))
+                continue;
+            if (j >= first) {
+                const uint8_t *col = cols + (size_t)(j - first) * cb;
+                for (int b = 0; b < cb; b++)
+                    ct[b] ^= col[b];
+            } else if (j < mt) {
+                ct[j >> 3] ^= (uint8_t)(1u << (j & 7));
+            }
+        }
+    }
+    free(cols);
+    return 0;
+}
+
+static uint64_t o_splitmix(uint64_t *s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+/* Error vectors of weight exactly t, uniform over [0, n): a partial
+ * Fisher-Yates shuffle per vector from a splitmix64 stream seeded by `seed`
+ * (test inputs; the reference's own generator, encrypt.c:40-85, draws m-bit
+ * indices without rejecting those >= n). */
+void o_random_errors(const o_params *p, uint64_t seed, size_t count, uint8_t *errs)
+{
+    const int n = p->n, t = p->t, nbytes = n / 8;
+    uint16_t *perm = (uint16_t *)malloc((size_t)n * sizeof(uint16_t));
+    if (!perm)
+        return;
+    uint64_t st = seed;
+    for (size_t c = 0; c < count; c++) {
+        uint8_t *e = errs + c * (size_t)nbytes;
+        memset(e, 0, (size_t)nbytes);
+        for (int i = 0; i < n; i++)
+            perm[i] = (uint16_t)i;
+        for (int i = 0; i < t; i++) {
+            const int j = i + (int)(o_splitmix(&st) % (uint64_t)(n - i));
+            const uint16_t x = perm[i];
+            perm[i] = perm[j];
+            perm[j] = x;
+            e[perm[i] >> 3] |= (uint8_t)(1u << (perm[i] & 7));
+        }
+    }
+    free(perm);
+}

@@ -89,6 +89,17 @@ int o_kg_pk_gen(const o_params *p, const uint16_t *irr, const uint32_t *perm,
                 uint8_t *pk, int16_t *pi);
 void o_kg_controlbits(int m, const int16_t *pi, uint8_t *out);
 
+
+/* Test inputs for the reference-only bench arm and CPU tests.
+ *  o_encrypt_batch: ciphertexts (ct_bytes each) of `count` error vectors
+ *    (n/8 bytes each) under a public key, by encrypt.c:87-120's syndrome rule.
+ *  o_random_errors: `count` error vectors of weight exactly t, uniform over
+ *    [0, n), from a seeded stream. */
+int o_encrypt_batch(const o_params *p, const uint8_t *pk, const uint8_t *errs,
+                    size_t count, uint8_t *cts);
+void o_random_errors(const o_params *p, uint64_t seed, size_t count,
+                     uint8_t *errs);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,11 +29,26 @@ class Params(ctypes.Structure):
                 ("set_id", "m", "n", "t", "ct_bytes", "sk_bytes", "sb", "cond_bytes")]
 
 
-def build(with_reference: bool | None = None) -> None:
-    """Compile liboracle.so and, when the reference tree is mounted, _ref/."""
-    ref_dir = os.environ.get("CMD_REFERENCE_DIR", "/root/reference")
+def reference_dir() -> str:
+    """The reference tree: $CMD_REFERENCE_DIR, else a checkout named
+    `reference` beside this repository; "" when neither exists."""
+    env = os.environ.get("CMD_REFERENCE_DIR", "")
+    if env:
+        return env
+    beside = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+    return beside if os.path.isdir(os.path.join(beside, "CPU")) else ""
+
+
+def build(with_reference: bool | None = None, ref_dir: str | None = None) -> None:
+    """Compile liboracle.so and, when the reference tree is present
+    (`ref_dir`, else reference_dir()), _ref/.  with_reference=True requires
+    it."""
+    ref_dir = ref_dir or reference_dir()
     targets = ["oracle"]
-    if with_reference or (with_reference is None and os.path.isdir(os.path.join(ref_dir, "CPU"))):
+    have = bool(ref_dir) and os.path.isdir(os.path.join(ref_dir, "CPU"))
+    if with_reference and not have:
+        raise FileNotFoundError("the reference tree: pass ref_dir or set CMD_REFERENCE_DIR")
+    if with_reference or (with_reference is None and have):
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}", *targets], check=True)
 
@@ -179,6 +194,25 @@ class Oracle:
         randombytes() yielding `seed`; see keypair_from_seed."""
         return keypair_from_seed(self, seed, max_attempts)
 
+    def encrypt(self, pk: bytes, errs: np.ndarray) -> np.ndarray:
+        """Ciphertexts [count, ct_bytes] of error vectors [count, n/8] under a
+        public key (kem/common/core/encrypt.c:87-120's syndrome rule)."""
+        errs = np.ascontiguousarray(errs, np.uint8).reshape(-1, self.n // 8)
+        pkb = np.frombuffer(bytes(pk), np.uint8).copy()
+        out = np.zeros((errs.shape[0], self.ct_bytes), np.uint8)
+        if self.lib.o_encrypt_batch(ctypes.byref(self.p), _ptr(pkb, _u8p), _ptr(errs, _u8p),
+                                    ctypes.c_size_t(errs.shape[0]), _ptr(out, _u8p)):
+            raise MemoryError
+        return out
+
+    def random_errors(self, seed: int, count: int) -> np.ndarray:
+        """`count` error vectors [count, n/8] of weight exactly t, uniform
+        over [0, n), from a seeded stream."""
+        out = np.zeros((count, self.n // 8), np.uint8)
+        self.lib.o_random_errors(ctypes.byref(self.p), ctypes.c_uint64(seed & (2 ** 64 - 1)),
+                                 ctypes.c_size_t(count), _ptr(out, _u8p))
+        return out
+
     def errorstream(self, err: np.ndarray) -> bytes:
         err = np.ascontiguousarray(err, np.uint8).reshape(-1, self.n // 8)
         cap = err.shape[0] * (1 + 6 * self.n // 8 * 8) + 16
@@ -260,6 +294,35 @@ class RefKeygen:
 
     def keypair(self, seed: bytes, max_attempts: int = 256):
         return keypair_from_seed(self, seed, max_attempts)
+
+
+def reference_decrypt_rows(keys: list[tuple[int, bytes]], key_idx: np.ndarray, cts: np.ndarray,
+                           nthreads: int = 0, row_bytes: int = 1024) -> tuple[np.ndarray, str]:
+    """Decodes a batch that mixes keys and parameter sets with the reference's
+    own CPU decoder (RefLib; the restatement where the reference build is
+    absent).  keys[k] = (set id, secret key); row r is ciphertext cts[r] (its
+    first ct_bytes bytes) under keys[key_idx[r]].  Returns (error rows
+    [rows, row_bytes], zero past each set's n/8 bytes; the checker's kind:
+    "reference" or "port")."""
+    nthreads = nthreads or (os.cpu_count() or 1)
+    key_idx = np.asarray(key_idx)
+    out = np.zeros((key_idx.size, row_bytes), np.uint8)
+    decs: dict[int, object] = {}
+    kinds = set()
+    order = np.argsort(key_idx, kind="stable")
+    bounds = np.searchsorted(key_idx[order], np.arange(len(keys) + 1))
+    for k, (s, sk) in enumerate(keys):
+        rows = order[bounds[k]: bounds[k + 1]]
+        if rows.size == 0:
+            continue
+        if s not in decs:
+            decs[s] = RefLib(s) if RefLib.available(s) else Oracle(s)
+            kinds.add("reference" if isinstance(decs[s], RefLib) else "port")
+        d = decs[s]
+        ctb = d.ct_bytes if hasattr(d, "ct_bytes") else d.p.ct_bytes
+        e = d.decrypt(sk, np.ascontiguousarray(cts[rows, :ctb]), nthreads=min(nthreads, rows.size))
+        out[rows, : e.shape[1]] = e
+    return out, ("reference" if kinds == {"reference"} else "port" if kinds == {"port"} else "mixed")
 
 
 class RefLib:

@@ -11,11 +11,15 @@
 # controlbits path); the script fails otherwise.
 #
 # Usage: tests/golden/gen_kem_vectors.sh [CT_PER_SK] [REFERENCE_DIR]
-# Needs the reference tree (read-only) and oracle/_ref/bin/decrypt_<set>
-# (make -C oracle ref).
+# Needs the reference tree (read-only: the second argument, else
+# $CMD_REFERENCE_DIR) and oracle/_ref/bin/decrypt_<set> (make -C oracle ref).
 set -eu
 CT_PER_SK="${1:-5}"
-REF="${2:-/root/reference}"
+REF="${2:-${CMD_REFERENCE_DIR:-}}"
+if [ -z "$REF" ] || [ ! -d "$REF/kem" ]; then
+    echo "gen_kem_vectors.sh: give the reference tree as the second argument or in CMD_REFERENCE_DIR" >&2
+    exit 2
+fi
 HERE="$(CDPATH= cd -- "$(dirname -- "$0")" && pwd)"
 REPO="$(CDPATH= cd -- "$HERE/../.." && pwd)"
 OUT="$HERE/kem"

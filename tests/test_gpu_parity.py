@@ -189,6 +189,49 @@ def test_mixed_batch(oracle_mod, engine):
             k.free()
 
 
+def test_mixed_64_keys_every_row_vs_reference(oracle_mod, engine):
+    """The mixed-batch workload at 2^14 ciphertexts: 64 seeded keys spread
+    13/13/13/13/12 over the five sets, the set drawn uniformly per ciphertext,
+    10% uniformly random mt-bit strings, one cmd_decrypt_mixed_device launch.
+    Every row, malformed ones included, equals the reference's own CPU
+    decoder's output (oracle/_ref; CPU/param/param<set>/src/decrypt.c), and
+    every weight its popcount."""
+    g = rng(0x5EED4)
+    per_set = [13, 13, 13, 13, 12]
+    ring = [(s, cmd.synth_key(s, golden_sk(s), 0xC0FFEE + 97 * i + j)) for i, s in enumerate(SETS)
+            for j in range(per_set[i])]
+    ks = [cmd.Key(engine, s, sk) for s, sk in ring]
+    try:
+        count = 1 << 14
+        set_of = g.integers(0, 5, count)
+        first = np.cumsum([0] + per_set[:-1])
+        key_idx = (first[set_of] + (g.random(count) * np.array(per_set)[set_of]).astype(np.int64)).astype(np.uint32)
+        buf = np.zeros((count, 208), np.uint8)
+        valid = np.zeros(count, np.uint8)
+        for k in range(len(ks)):
+            idx = np.nonzero(key_idx == k)[0]
+            if idx.size:
+                c, _, v = cmd.PubKey(*ring[k]).ciphertexts(seed=1000 + k, count=idx.size, malformed_permille=100)
+                buf[idx, : c.shape[1]] = c
+                valid[idx] = v
+        assert 0.05 < 1 - valid.mean() < 0.15
+        d_ct = dev(buf.reshape(-1))
+        d_err = torch.zeros(count * 256, dtype=torch.int32, device="cuda")
+        d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+        cmd.decrypt_mixed_device(engine, ks, key_idx, d_ct.data_ptr(), np.arange(count, dtype=np.uint64) * 208,
+                                 d_err.data_ptr(), np.arange(count, dtype=np.uint64) * 256, d_w.data_ptr())
+        torch.cuda.synchronize()
+        E = d_err.cpu().numpy().astype("<u4").view(np.uint8).reshape(count, 1024)
+        W = d_w.cpu().numpy().view(np.uint16)
+    finally:
+        for k in ks:
+            k.free()
+    ref, _ = oracle_mod.reference_decrypt_rows(ring, key_idx, buf)
+    bad = np.nonzero(~(E == ref).all(axis=1))[0]
+    assert bad.size == 0, (bad[:10], int((valid[bad] == 0).sum()))
+    assert np.array_equal(W, np.unpackbits(ref, axis=1).sum(axis=1))
+
+
 @pytest.mark.parametrize("path", ["plain", "fused"])
 def test_full_size_properties(engine, keys, path):
     """Full-size batch at 6960119 (65,536 ciphertexts): every valid

@@ -117,3 +117,36 @@ def test_oracle_pk_gen_rejects_repeated_words(oracle_mod):
     assert o.kg_pk_gen(irr, perm) is None
     if oracle_mod.RefKeygen.available(s):
         assert oracle_mod.RefKeygen(s).kg_pk_gen(irr, perm) is None
+
+
+@pytest.mark.parametrize("s", SETS)
+def test_oracle_encrypt_matches_syndrome_rule_and_reference_decoder(oracle_mod, s):
+    """o_encrypt_batch (the reference-only bench arm's input generator) equals
+    the row-wise syndrome rule, re-encrypts the shipped ciphertexts, and its
+    weight-t ciphertexts decode to their error vectors in the reference's own
+    decoder."""
+    o = oracle_mod.Oracle(s)
+    sk = golden_sk(s)
+    pk, _, _ = o.keypair(sk[:32])
+    e = o.random_errors(seed=11 + s, count=6)
+    bits = np.unpackbits(e, axis=1, bitorder="little")
+    assert (bits.sum(axis=1) == o.t).all()
+    assert not np.array_equal(e[0], e[1])
+    cts = o.encrypt(pk, e)
+    assert np.array_equal(cts, pk_syndromes(pk, o.m, o.n, o.t, bits))
+    dec = (oracle_mod.RefLib(s) if oracle_mod.RefLib.available(s) else o).decrypt(sk, cts)
+    assert np.array_equal(dec, e)
+    # the shipped kem/ ciphertexts from their decoded vectors (zero-element
+    # flag dropped when fewer than t errors were sent)
+    _, L, _ = o.expand(sk)
+    zero = int(np.nonzero(L == 0)[0][0])
+    es = errors_from_stream(golden_errorstream(s), o.n)
+    shipped = np.frombuffer(golden_ct(s), np.uint8).reshape(-1, o.ct_bytes)
+    for i in range(es.shape[0]):
+        ei = es[i].copy()
+        if ei.sum() < o.t + 1 and ei[zero]:
+            alt = ei.copy()
+            alt[zero] = 0
+            if np.array_equal(o.encrypt(pk, np.packbits(alt, bitorder="little")[None])[0], shipped[i]):
+                continue
+        assert np.array_equal(o.encrypt(pk, np.packbits(ei, bitorder="little")[None])[0], shipped[i]), (s, i)
