@@ -31,7 +31,7 @@ SET_INDEX = {s: i for i, s in enumerate(SETS)}
 # Status codes (include/cmd_b200.h); 0/-1/-4 are the reference's KAT_* codes.
 CMD_OK, CMD_E_FILE, CMD_E_ARG, CMD_E_CUDA = 0, -1, -4, -5
 CMD_E_NOMEM, CMD_E_BUDGET, CMD_E_BUSY, CMD_E_TIMEOUT, CMD_E_NODEVICE = -6, -7, -8, -9, -10
-PATHS = {"auto": 0, "plain": 1, "fused": 2}
+PATHS = {"auto": 0, "plain": 1, "fused": 2, "tile": 3}
 
 
 class CmdError(RuntimeError):
@@ -113,6 +113,7 @@ def lib() -> ctypes.CDLL:
         "cmd_decrypt_mixed_device": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp]),
         "cmd_decrypt_plain_noalloc": (_i32, [_vp, _vp, _sz, _vp, _vp, _vp]),
         "cmd_stage_synd": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
+        "cmd_stage_synd_fft": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
         "cmd_stage_bm": (_i32, [_vp, _i32, _vp, _sz, _vp, _vp]),
         "cmd_stage_root": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp, _vp]),
         "cmd_stage_root_images": (_i32, [_vp, _vp, _vp, _sz, _vp, _vp]),
@@ -411,6 +412,11 @@ class Server:
 # ---- per-stage hooks (device pointers) -----------------------------------
 def synd(engine: Engine, key: Key, d_cts: int, count: int, d_synd: int, stream: int = 0) -> None:
     _check(lib().cmd_stage_synd(engine.handle, key.handle, d_cts, count, d_synd, stream or None), "synd")
+
+
+def synd_fft(engine: Engine, key: Key, d_cts: int, count: int, d_synd: int, stream: int = 0) -> None:
+    """synd() by the serving path's transposed additive FFT (no syndrome table)."""
+    _check(lib().cmd_stage_synd_fft(engine.handle, key.handle, d_cts, count, d_synd, stream or None), "synd_fft")
 
 
 def bm(engine: Engine, set_id: int, d_synd: int, count: int, d_loc: int, stream: int = 0) -> None:

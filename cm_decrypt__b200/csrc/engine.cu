@@ -12,6 +12,8 @@
 #include "engine.h"
 
 namespace cmd {
+static int run_tile(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                    uint16_t *d_weight, uint16_t *d_synd, cudaStream_t s);
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string &msg) { g_last_error = msg; }
@@ -237,7 +239,7 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
     }
     const size_t bytes = carve_size({(size_t)si.n * 2, (size_t)(si.t + 1) * 2, (size_t)si.n * 2,
                                      (size_t)si.sb * si.twp() * 4, (size_t)si.m * si.nw * 4,
-                                     benes_mask_words(si) * 4, (size_t)si.sk});
+                                     benes_mask_words(si) * 4, fft_weight_words(si) * 4, (size_t)si.sk});
     if (!budget_take(eng, bytes)) {
         set_last_error("key does not fit the engine HBM budget");
         return CMD_E_BUDGET;
@@ -264,6 +266,7 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
     key->dev.tab = cv.take<uint32_t>((size_t)si.sb * si.twp());
     key->dev.Lbs = cv.take<uint32_t>((size_t)si.m * si.nw);
     key->dev.bctl = cv.take<uint32_t>(benes_mask_words(si));
+    key->dev.wfft = cv.take<uint32_t>(fft_weight_words(si));
     key->dev.sk = cv.take<uint8_t>(si.sk);
     std::lock_guard<std::mutex> lk(eng->mu);
     if ((e = cudaMemcpyAsync(key->dev.sk, h_sk, si.sk, cudaMemcpyHostToDevice, eng->stream)) != cudaSuccess ||
@@ -348,6 +351,18 @@ int cmd_stage_synd(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, si
     return e == cudaSuccess ? CMD_OK : cuda_fail(e, "synd kernel");
 }
 
+int cmd_stage_synd_fft(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint16_t *d_synd,
+                       void *stream)
+{
+    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_synd)))
+        return CMD_E_ARG;
+    if (count == 0)
+        return CMD_OK;
+    cudaSetDevice(eng->device);
+    std::lock_guard<std::mutex> lk(eng->mu);
+    return run_tile(eng, key, d_cts, count, nullptr, nullptr, d_synd, stream ? (cudaStream_t)stream : eng->stream);
+}
+
 int cmd_stage_bm(cmd_engine *eng, cmd_set set, const uint16_t *d_synd, size_t count, uint16_t *d_loc, void *stream)
 {
     if (!eng || !valid_set(set) || (count && (!d_synd || !d_loc)))
@@ -420,6 +435,32 @@ static int run_plain(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
     return CMD_OK;
 }
 
+// The serving tile kernels over one key's batch, in chunks whose byte and
+// word offsets fit the tile items' 32-bit fields.  With d_synd: syndromes
+// only.  Caller holds eng->mu.
+static int run_tile(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
+                    uint16_t *d_weight, uint16_t *d_synd, cudaStream_t s)
+{
+    const SetInfo si = set_info(key->dev.set);
+    const size_t chunk = std::min<size_t>(count, (size_t)1 << 22);
+    int rc = eng->scratch.reserve(eng, tile_single_scratch_words(chunk) * 4);
+    if (rc)
+        return rc;
+    FftPlans plans;
+    for (int st = 0; st < NSETS; st++)
+        plans.p[st] = eng->fft[st];
+    for (size_t c0 = 0; c0 < count; c0 += chunk) {
+        const size_t n = std::min(chunk, count - c0);
+        const cudaError_t e = launch_tile_single(
+            key->dev, d_cts + c0 * si.ct, n, static_cast<uint32_t *>(eng->scratch.ptr),
+            d_err ? d_err + c0 * si.nw : nullptr, d_weight ? d_weight + c0 : nullptr,
+            d_synd ? d_synd + c0 * 2 * si.t : nullptr, plans, s, LaunchCounter{&eng->launches});
+        if (e != cudaSuccess)
+            return cuda_fail(e, "tile path launch");
+    }
+    return CMD_OK;
+}
+
 int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
                uint32_t *d_err, uint16_t *d_weight, cudaStream_t s)
 {
@@ -427,6 +468,8 @@ int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t
         return CMD_OK;
     if (path == CMD_PATH_PLAIN)
         return run_plain(eng, key, d_cts, count, d_err, d_weight, s);
+    if (path == CMD_PATH_TILE)
+        return run_tile(eng, key, d_cts, count, d_err, d_weight, nullptr, s);
     return run_fused_single(eng, key, d_cts, count, d_err, d_weight, s);
 }
 
@@ -437,7 +480,7 @@ extern "C" {
 int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
                        uint32_t *d_err, uint16_t *d_weight, void *stream)
 {
-    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_err)) || path < 0 || path > 2)
+    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_err)) || path < 0 || path > 3)
         return CMD_E_ARG;
     cudaSetDevice(eng->device);
     std::lock_guard<std::mutex> lk(eng->mu);
@@ -447,7 +490,7 @@ int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const
 int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *h_cts, size_t count,
                       uint8_t *h_err, uint16_t *h_weight)
 {
-    if (!eng || !key || key->eng != eng || (count && (!h_cts || !h_err)) || path < 0 || path > 2)
+    if (!eng || !key || key->eng != eng || (count && (!h_cts || !h_err)) || path < 0 || path > 3)
         return CMD_E_ARG;
     if (count == 0)
         return CMD_OK;
@@ -469,7 +512,7 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
     // Large fused batches go as BATCH_STREAMS pieces on their own streams
     // (each with its own work counter, full rounds): one piece's copies run
     // while the others compute, and the pieces' kernels share the SMs.
-    const bool pieces = path != CMD_PATH_PLAIN && chunk >= (size_t)BATCH_STREAMS * 8192;
+    const bool pieces = path != CMD_PATH_PLAIN && path != CMD_PATH_TILE && chunk >= (size_t)BATCH_STREAMS * 8192;
     if (pieces) {
         if ((rc = ensure_counter(eng)))
             return rc;

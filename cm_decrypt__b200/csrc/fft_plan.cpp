@@ -13,8 +13,15 @@
 // the evaluation point; the kernel keeps output q at position bitrev_m(q), so
 // every butterfly pairs whole 32-bit words of the bitsliced array.
 //
-// Per depth d < D this file computes
-//   * scalpow[d][i] = b_d^i (i < 2^(D-d)), b_d the first basis element at
+// The same recursion, transposed, gives the serving path's syndromes: the
+// power sums sum_a u_a a^j (j < 2t) of values u_a at all 2^m elements (see
+// latency.cu).  That needs 2t coefficients, depth D' with 2^D' >= 2t, one
+// level more than the root search for t = 96 and 119; the tables below go to
+// depth D' (the root search reads the first D levels, whose entries do not
+// depend on how deep the tables go).
+//
+// Per depth d < D' this file computes
+//   * scalpow[d][i] = b_d^i (i < 2^(D'-d)), b_d the first basis element at
 //     depth d -- the scaling g(x) = f(b_d x) of the radix conversion;
 //   * the twiddles: the butterfly of depth d pairs positions Y and
 //     Y + 2^(m-d-1); its multiplier a(Y) depends on r = Y mod 2^(m-d-1):
@@ -63,7 +70,7 @@ FftPlanHost make_fft_plan(int set)
     const SetInfo si = set_info(set);
     const int m = si.m;
     FftPlanHost p;
-    p.D = fft_depth(si.t);
+    p.D = synd_depth(si.t);
     p.scalpow.assign(8 * 256, 0);
     std::vector<uint32_t> B(m);
     for (int j = 0; j < m; j++)

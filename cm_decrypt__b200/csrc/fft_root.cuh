@@ -89,6 +89,97 @@ __device__ __forceinline__ void fft_convert(uint32_t *cv, const uint16_t *__rest
     }
 }
 
+// Transpose of the radix conversion at depth D' = synd_depth(t) (2^D' >= 2t
+// entries), for the serving path's syndromes: every elementary step of
+// fft_convert (x_a ^= x_b, a scaling) is replaced by its transpose (x_b ^=
+// x_a, the same scaling) and the steps run in the opposite order.  In:
+// cv[s * CVS + k], the depth-D' constants' dual (sums over the FFT groups);
+// out: entry x = the power sum of index x.
+template <int S, int CVS, int NT, class Sync>
+__device__ __forceinline__ void fft_convert_t(uint32_t *cv, const uint16_t *__restrict__ scalpow, int tid, Sync sync)
+{
+    constexpr int M = Set<S>::M, D = synd_depth(Set<S>::T), NX = 1 << D;
+#pragma unroll 1
+    for (int d = D - 1; d >= 0; d--) {
+#pragma unroll 1
+        for (int kb = 2; kb <= D - d; kb++) {
+            const int Q = 1 << (kb - 2);
+#pragma unroll 1
+            for (int h = 1; h <= 2; h++) {  // h = 1: third ^= second; h = 2: fourth ^= third
+                for (int u = tid; u < (NX / 4) * M; u += NT) {
+                    const int e = u / M, k = u - e * M;
+                    const int sub = e & ((1 << d) - 1), rest = e >> d;
+                    const int i = (rest >> (kb - 2)) * 4 * Q + h * Q + (rest & (Q - 1));
+                    cv[(((i + Q) << d) + sub) * CVS + k] ^= cv[((i << d) + sub) * CVS + k];
+                }
+                sync();
+            }
+        }
+        if (d > 0) {
+            for (int x = tid; x < NX; x += NT) {
+                const uint32_t c = __ldg(scalpow + d * 256 + (x >> d));
+                uint32_t v[M], cm[M], p[2 * M - 1];
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    v[k] = cv[x * CVS + k];
+                    cm[k] = 0u - ((c >> k) & 1u);
+                }
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    p[k] = 0;
+                bs_mul_acc<M>(p, v, cm);
+                bs_reduce<M>(p);
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    cv[x * CVS + k] = p[k];
+            }
+            sync();
+        }
+    }
+}
+
+// Layer l of the key's support network over a 2^m-bit array held by one
+// warp (word w = lane + 32j in z[j]): every pair (p, p + 2^e) whose mask bit
+// (the lower element's) is set exchanges its two bits; e = l for l < m, else
+// 2m-2-l.  A layer is its own inverse.
+template <int S>
+__device__ __forceinline__ void swap_layer(uint32_t *z, const uint32_t *__restrict__ bctl, int l, int lane)
+{
+    using F = FftDims<S>;
+    constexpr int M = F::M, NWD = F::NWD, R = F::R;
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    const int e = l < M ? l : 2 * M - 2 - l;
+    const uint32_t *ml = bctl + l * NWD;
+    if (e < 5) {  // pairs inside a word
+        const int sh = 1 << e;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const uint32_t mk = __ldg(ml + lane + 32 * j);
+            const uint32_t t = ((z[j] >> sh) ^ z[j]) & mk;
+            z[j] ^= t ^ (t << sh);
+        }
+    } else if (e < 10) {  // pairs across lanes
+        const int ls = 1 << (e - 5);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const uint32_t other = __shfl_xor_sync(FULL, z[j], ls);
+            const uint32_t mk = __ldg(ml + ((lane & ~ls) + 32 * j));
+            z[j] ^= (z[j] ^ other) & mk;
+        }
+    } else {  // pairs inside a lane
+        const int js = 1 << (e - 10);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (!(j & js)) {
+                const uint32_t mk = __ldg(ml + lane + 32 * j);
+                const uint32_t t = (z[j] ^ z[j | js]) & mk;
+                z[j] ^= t;
+                z[j | js] ^= t;
+            }
+        }
+    }
+}
+
 // One warp: error row (and weight) of locator q from the converted array cv
 // (bitsliced, cv[s * CVS + k]).  fa: this warp's FA_WORDS words of shared
 // memory.  erow: NW words, or null.  prow: null, or t+1 u16 that receive the
@@ -200,38 +291,8 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
     }
     __syncwarp();  // fa may be refilled right after this call
 #pragma unroll
-    for (int l = 0; l < 2 * M - 1; l++) {
-        const int e = l < M ? l : 2 * M - 2 - l;
-        const uint32_t *ml = bctl + l * NWD;
-        if (e < 5) {  // pairs inside a word
-            const int sh = 1 << e;
-#pragma unroll
-            for (int j = 0; j < R; j++) {
-                const uint32_t mk = __ldg(ml + lane + 32 * j);
-                const uint32_t t = ((z[j] >> sh) ^ z[j]) & mk;
-                z[j] ^= t ^ (t << sh);
-            }
-        } else if (e < 10) {  // pairs across lanes
-            const int ls = 1 << (e - 5);
-#pragma unroll
-            for (int j = 0; j < R; j++) {
-                const uint32_t other = __shfl_xor_sync(FULL, z[j], ls);
-                const uint32_t mk = __ldg(ml + ((lane & ~ls) + 32 * j));
-                z[j] ^= (z[j] ^ other) & mk;
-            }
-        } else {  // pairs inside a lane
-            const int js = 1 << (e - 10);
-#pragma unroll
-            for (int j = 0; j < R; j++) {
-                if (!(j & js)) {
-                    const uint32_t mk = __ldg(ml + lane + 32 * j);
-                    const uint32_t t = (z[j] ^ z[j | js]) & mk;
-                    z[j] ^= t;
-                    z[j | js] ^= t;
-                }
-            }
-        }
-    }
+    for (int l = 0; l < 2 * M - 1; l++)
+        swap_layer<S>(z, bctl, l, lane);
     uint32_t v[R];
     int cnt = 0;
 #pragma unroll

@@ -29,6 +29,10 @@ struct KeyDev {
                                 // bit b of bctl[l*2^(m-5)+w] set when layer l
                                 // exchanges position 32w+b (the pair's lower
                                 // element) with its partner
+    uint32_t *wfft = nullptr;   // 1/g(a)^2 at every field element a in the
+                                // additive FFT's position order, bitsliced
+                                // plane-major [m][2^(m-5)]: bit b of word w is
+                                // the element a = bitrev_m(32w + b)
     uint8_t *sk = nullptr;      // device copy of the secret key bytes
 };
 
@@ -45,6 +49,8 @@ struct LaunchCounter {
 cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc);
 // Words of KeyDev::bctl for one set.
 inline size_t benes_mask_words(const SetInfo &si) { return (size_t)(2 * si.m - 1) << (si.m - 5); }
+// Words of KeyDev::wfft for one set.
+inline size_t fft_weight_words(const SetInfo &si) { return (size_t)si.m << (si.m - 5); }
 
 cudaError_t launch_synd_plain(const KeyDev &k, const uint8_t *d_cts, size_t count,
                               uint32_t *d_synd, cudaStream_t s, LaunchCounter lc);
@@ -109,7 +115,7 @@ cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cuda
 
 // Latency path (serving loop; latency.cu): one work item per ciphertext.
 struct LatItem {
-    const uint32_t *tab;  // key's syndrome table
+    const uint32_t *wfft; // key's syndrome weights in FFT order (KeyDev::wfft)
     const uint32_t *bctl; // key's support-network swap masks
     uint32_t ct_off;      // byte offset of the ciphertext in the batch
     uint32_t err_off;     // word offset of the error row in the batch
@@ -119,17 +125,23 @@ struct LatItem {
 // Tile path: ntiles tiles of 32 item slots (LatItem.pad = tile count, padding
 // slots set -1).  d_scratch holds ntiles * TILE_SCRATCH_WORDS words: each
 // tile's radix-converted locators (bitsliced, 16 words per entry), then the
-// partial syndromes (SYN_PARTS rows of SYN_ROWW words per item slot).
+// transposed-FFT sums of its ciphertexts (2^D' u16 entries x 32 slots).
 constexpr int TILE_LOC_WORDS = 256 * 16;
-constexpr int SYN_PARTS = 4;
-constexpr int SYN_ROWW = 128;
-constexpr int TILE_SCRATCH_WORDS = TILE_LOC_WORDS + 32 * SYN_PARTS * SYN_ROWW;
+constexpr int TILE_SUM_WORDS = 256 * 32 / 2;
+constexpr int TILE_SCRATCH_WORDS = TILE_LOC_WORDS + TILE_SUM_WORDS;
 struct FftPlans {
     FftPlanDev p[NSETS];
 };
 cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_scratch,
                              uint32_t *d_err, uint16_t *d_weight, const FftPlans &plans, cudaStream_t s,
                              LaunchCounter lc);
+// The tile path over one key's batch (ciphertexts at the set's ct stride,
+// error rows at its nw stride); with d_synd, only the syndromes (rows of 2t
+// u16).  d_scratch: tile_single_scratch_words(count) words.
+cudaError_t launch_tile_single(const KeyDev &k, const uint8_t *d_cts, size_t count, uint32_t *d_scratch,
+                               uint32_t *d_err, uint16_t *d_weight, uint16_t *d_synd, const FftPlans &plans,
+                               cudaStream_t s, LaunchCounter lc);
+size_t tile_single_scratch_words(size_t count);
 
 void set_last_error(const std::string &msg);
 

@@ -136,6 +136,34 @@ template <int S> __global__ void __launch_bounds__(256) k_benes_masks(KeyDev k)
     k.bctl[idx] = mask;
 }
 
+// Syndrome weights in the additive FFT's position order, for the serving
+// syndrome kernel (the transposed FFT): bit b of wfft[k * 2^(m-5) + w] = bit k
+// of 1/g(a)^2 at the field element a = bitrev_m(32w + b), for all 2^m
+// elements (the same values as compute_inverses' e_inv, util.c:86-100, there
+// indexed by support position).  Thread per element, warp per word.
+template <int S> __global__ void __launch_bounds__(256) k_fft_weights(KeyDev k)
+{
+    using P = Set<S>;
+    constexpr int M = P::M, T = P::T, NWD = 1 << (M - 5);
+    __shared__ uint16_t g[T + 1];
+    for (int i = threadIdx.x; i <= T; i += blockDim.x)
+        g[i] = k.g[i];
+    __syncthreads();
+    const uint32_t y = blockIdx.x * blockDim.x + threadIdx.x;  // grid covers 2^m exactly
+    const uint32_t a = __brev(y) >> (32 - M);
+    uint32_t v = g[T];
+    for (int j = T - 1; j >= 0; j--)
+        v = gf_mul_im<M>(v, a) ^ g[j];
+    const uint32_t inv = gf_inv<M, true>(gf_mul_im<M>(v, v));
+    const int lane = threadIdx.x & 31, w = (int)(y >> 5);
+#pragma unroll
+    for (int b = 0; b < M; b++) {
+        const uint32_t plane = __ballot_sync(0xFFFFFFFFu, (inv >> b) & 1u);
+        if (lane == 0)
+            k.wfft[b * NWD + w] = plane;
+    }
+}
+
 cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc)
 {
     return dispatch_set(k.set, [&]<int S>() -> cudaError_t {
@@ -144,7 +172,8 @@ cudaError_t launch_key_expand(const KeyDev &k, cudaStream_t s, LaunchCounter lc)
         k_key_tables<S><<<(P::N + 255) / 256, 256, 0, s>>>(k);
         k_bitslice_support<S><<<(P::NW * 32 + 255) / 256, 256, 0, s>>>(k);
         k_benes_masks<S><<<((2 * P::M - 1) * (1 << (P::M - 5)) + 255) / 256, 256, 0, s>>>(k);
-        lc.bump(4);
+        k_fft_weights<S><<<(1 << P::M) / 256, 256, 0, s>>>(k);
+        lc.bump(5);
         return cudaGetLastError();
     });
 }

@@ -1,16 +1,48 @@
 // Latency-oriented decrypt path for the serving loop: tiles of up to 32
-// ciphertexts of one parameter set, each ciphertext with its own key, in two
+// ciphertexts of one parameter set, each ciphertext with its own key, in three
 // launches per batch (any mix of sets: one tile per 32 ciphertexts of a set).
 //
-// Scaled Berlekamp-Massey.  bm() (CPU/src/common/bm.c:12-68) updates
-// C <- C + (d/b) x B, which needs b^-1 every iteration: a chain of ~16
-// dependent field operations per step.  Here C <- b C + d x B instead, with
-// the same decisions (d != 0, N >= 2L), the same truncation to t+1
-// coefficients and the same B/b/L updates.  By induction C_here = lambda *
-// C_ref with lambda a product of earlier (nonzero) b values, so the returned
-// polynomial is a nonzero multiple of bm()'s output: it has exactly the same
-// roots and the decrypt flags exactly the same positions, decode failures
-// included.  (The per-stage hook cmd_stage_bm keeps bm()'s exact output.)
+//  k_tile_tsynd  warp per ciphertext: the 2t syndromes (util.c:102-114) by the
+//                transposed additive FFT, with no per-key syndrome table;
+//  k_tile_bm     CTA per tile: the syndromes' last stage, Berlekamp-Massey
+//                (bm.c:12-68) bitsliced across the tile, the locators' radix
+//                conversion;
+//  k_root_tile   warp per ciphertext: additive-FFT root search and the key's
+//                support network (root_13.c:216-240).
+//
+// Syndromes.  synd() sums, over the ciphertext bits b < sb that are set, the
+// table row L_b^j / g(L_b)^2 (j < 2t).  Written over the field: s_j =
+// sum_a u_a a^j, with u_a = 1/g(a)^2 at the element a = L_b of every set bit
+// and 0 elsewhere.  That is the transpose of evaluating a polynomial of 2^D'
+// coefficients (2^D' >= 2t) at all 2^m elements, which the root search does
+// with the additive FFT; so the syndromes come from the FFT run backwards:
+//   1. the ciphertext bits, in support order, go through the key's support
+//      network in reverse (the network maps FFT positions to support
+//      positions; each layer is its own inverse), and select the key's
+//      weights 1/g(a)^2 stored in FFT position order (KeyDev::wfft);
+//   2. D' transposed butterfly levels, depth 0 first: A <- A + B,
+//      B <- B + w*A (the transpose of A' = A + w*B, B' = A' + B);
+//   3. each group of positions that shares its top D' bits is one word; the
+//      word's parity per plane is the dual of the depth-D' constant of
+//      sub-problem bitrev(word);
+//   4. (in k_tile_bm, bitsliced across the tile) the transposed radix
+//      conversion turns those 2^D' values into the power sums s_0 .. s_{2t-1}.
+// All of it is exact GF(2^m) arithmetic, so the syndromes equal synd()'s.
+// Per key it reads the support-network masks and the weights (about 39 KB
+// for m = 13) instead of a 745 KB table, so the keys of a large serving set
+// stay in L2.
+//
+// Scaled Berlekamp-Massey.  bm() updates C <- C + (d/b) x B, which needs
+// b^-1 every iteration: a chain of ~16 dependent field operations per step.
+// Here C <- b C + d x B instead, with the same decisions (d != 0, N >= 2L),
+// the same truncation to t+1 coefficients and the same B/b/L updates.  By
+// induction C_here = lambda * C_ref with lambda a product of earlier
+// (nonzero) b values, so the returned polynomial is a nonzero multiple of
+// bm()'s output: it has exactly the same roots and the decrypt flags exactly
+// the same positions, decode failures included.  (The per-stage hook
+// cmd_stage_bm keeps bm()'s exact output.)  Coefficients above the largest
+// L of the tile are zero (deg C <= L), so they are neither multiplied into
+// the discrepancy nor updated.
 #include <algorithm>
 
 #include "fft_root.cuh"
@@ -25,304 +57,356 @@ constexpr uint32_t FULL = 0xFFFFFFFFu;
 
 static_assert(sizeof(LatItem) == 32, "LatItem layout");
 
-// ---------------------------------------------------------------- tile path
-// Tiles of up to 32 ciphertexts of one set, each with its own key.  Item slot
-// 32*t + q is ciphertext q of tile t (LatItem.pad = the tile's count, padding
-// slots have set -1).
-//
-// k_tile_synd: SYN_PARTS CTAs per ciphertext, each over a contiguous quarter
-//   of the syndrome-table rows of the ciphertext's own key (util.c:102-114):
-//   warp w takes rows w, w+8, ...; lane l owns table words 4l..4l+3 (one
-//   128-bit load per row), every row masked by the ciphertext bit; the eight
-//   warps' sums meet in shared memory and the CTA writes one partial
-//   syndrome row.  A batch's tables stream through every SM at once instead
-//   of through one SM per tile.
-// k_tile_bm: one CTA of 8 warps per tile.
-//   1. syndromes: XOR of each ciphertext's SYN_PARTS partial rows;
-//   2. ballot transpose to bitsliced syndromes (bit q = ciphertext q);
-//   3. scaled Berlekamp-Massey bitsliced across the 32 ciphertexts with thread
-//      i owning coefficient i, so one step costs about one bitsliced multiply
-//      per thread: partial discrepancies meet in shared memory, B lives in a
-//      shared ring buffer whose rotation is the x*B shift;
-//   4. radix conversion of the 32 locators by the whole CTA (fft_root.cuh);
-//      the converted array (2^D entries x 16 words) goes to global.
-// k_root_tile: 8 warps per CTA, four CTAs per tile, warp = one ciphertext:
-// additive-FFT evaluation and the ciphertext's own key's support network.
-
-template <int S>
-__device__ __forceinline__ void tile_synd(const LatItem &it, const uint8_t *cts, int part, uint32_t *out,
-                                          uint32_t (*red)[SYN_ROWW], uint8_t *ct)
-{
-    using P = Set<S>;
-    constexpr int TWP = P::TWP, RPP = (P::SB + SYN_PARTS - 1) / SYN_PARTS;
-    static_assert(TWP <= SYN_ROWW, "partial syndrome row");
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    for (int v = tid; v < P::CT; v += blockDim.x)
-        ct[v] = cts[it.ct_off + v];
-    __syncthreads();
-    const int b0 = part * RPP, b1 = b0 + RPP < P::SB ? b0 + RPP : P::SB;
-    const bool live = 4 * lane < TWP;
-    const uint4 *tab = reinterpret_cast<const uint4 *>(it.tab) + lane;
-    uint4 acc = make_uint4(0, 0, 0, 0);
-    // Rows whose ciphertext bit is clear are skipped (the bit is the same for
-    // the whole warp, so the branch does not diverge): about half the table
-    // is read.  The ciphertext is public, so which rows are read reveals
-    // nothing about the key or the error vector.
-#pragma unroll 8
-    for (int b = b0 + warp; b < b1; b += 8) {
-        if (live && ((ct[b >> 3] >> (b & 7)) & 1u)) {
-            const uint4 x = __ldg(tab + (size_t)b * (TWP / 4));
-            acc.x ^= x.x;
-            acc.y ^= x.y;
-            acc.z ^= x.z;
-            acc.w ^= x.w;
-        }
-    }
-    if (live)
-        *reinterpret_cast<uint4 *>(&red[warp][4 * lane]) = acc;
-    __syncthreads();
-    for (int w = tid; w < TWP; w += blockDim.x) {
-        uint32_t v = 0;
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-            v ^= red[k][w];
-        out[w] = v;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_tile_synd(const LatItem *__restrict__ items, const uint8_t *__restrict__ cts,
-                                                   uint32_t *__restrict__ synp)
-{
-    __shared__ __align__(16) uint32_t red[8][SYN_ROWW];
-    __shared__ uint8_t ct[208];
-    const int slot = blockIdx.x / SYN_PARTS, part = blockIdx.x % SYN_PARTS, t = slot >> 5, q = slot & 31;
-    const LatItem it = items[slot];
-    if (it.set < 0 || q >= (int)items[(size_t)t * 32].pad)
-        return;  // whole CTA
-    uint32_t *out = synp + ((size_t)slot * SYN_PARTS + part) * SYN_ROWW;
-    switch (it.set) {
-    case S348864: tile_synd<S348864>(it, cts, part, out, red, ct); break;
-    case S460896: tile_synd<S460896>(it, cts, part, out, red, ct); break;
-    case S6688128: tile_synd<S6688128>(it, cts, part, out, red, ct); break;
-    case S6960119: tile_synd<S6960119>(it, cts, part, out, red, ct); break;
-    default: tile_synd<S8192128>(it, cts, part, out, red, ct); break;
-    }
-}
-
-template <int S> struct TileSmem {
-    using P = Set<S>;
-    static constexpr int SYN_STRIDE = P::TW | 1;  // odd stride: conflict-free column reads
-    uint32_t syn[32 * SYN_STRIDE];
-    uint32_t S_[2 * P::T * P::M];
-    uint32_t ring[(P::T + 2) * P::M];
-    uint32_t cs[(P::T + 1) * P::M];       // C after each update, for the discrepancy warps
-    alignas(16) uint32_t part[2][8][16];  // per-warp partial discrepancies, double-buffered by step parity
+template <int S> struct TsDims {
+    using F = FftDims<S>;
+    static constexpr int M = F::M, T = F::T, NWD = F::NWD, R = F::R;
+    static constexpr int DS = synd_depth(T);  // transposed-FFT depth, 2^DS >= 2t
+    static constexpr int NS = 1 << DS;        // group sums per ciphertext
+    static_assert(DS == M - 5, "the last transposed level pairs adjacent words: one group per word");
+    static_assert(NS * 32 / 2 <= TILE_SUM_WORDS, "tile sums");
 };
 
-// Threads of k_tile_bm: two roles of up to five warps each (t+1 <= 129
-// coefficients per role).  The kernel is bounded to 96 registers a thread
-// so that two tiles share an SM: one tile keeps an SM's ALUs about half busy
-// (its steps are a chain of dependent multiplies and barriers).
-constexpr int TILE_THREADS = 320;
+constexpr int TS_WARPS = 8;                  // ciphertexts per k_tile_tsynd CTA
+constexpr size_t TS_FA_WORDS = 13 * 256;     // per-warp 2^m-element array, largest set
 
-template <int S> __device__ __forceinline__ void tile_bm(int count, const uint32_t *synp, uint32_t *loc_bs,
-                                                         const uint16_t *scalpow, uint8_t *smem_raw)
+// One warp: the transposed FFT of ciphertext q of its tile; writes the
+// group sums sums[s * 32 + q] (bit k = plane k), s < 2^D'.
+template <int S>
+__device__ __forceinline__ void tsynd_one(const LatItem &it, const uint8_t *__restrict__ cts,
+                                          const uint32_t *__restrict__ tw, uint32_t *fa, uint16_t *sums, int q,
+                                          int lane)
 {
+    using Z = TsDims<S>;
     using P = Set<S>;
-    using Sm = TileSmem<S>;
-    constexpr int M = P::M, T = P::T, TW = P::TW, R = T + 2;
-    constexpr int NWB = (T + 1 + 31) / 32;  // warps that own coefficients
-    constexpr int SYN = Sm::SYN_STRIDE;
-    Sm &sm = *reinterpret_cast<Sm *>(smem_raw);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    // ---- 1. syndromes: XOR of the partial rows from k_tile_synd ------------
-    for (int v = tid; v < 32 * TW; v += blockDim.x) {
-        const int q = v / TW, w = v - q * TW;
-        uint32_t x = 0;
-        if (q < count) {
-            const uint32_t *src = synp + (size_t)q * SYN_PARTS * SYN_ROWW + w;
+    constexpr int M = Z::M, NWD = Z::NWD, R = Z::R, DS = Z::DS, SB = P::SB, CTW = P::CTW;
+    static_assert(Z::NWD * M <= (int)TS_FA_WORDS, "transposed-FFT array");
+    // 1. ciphertext bits in support order (word w = lane + 32j: positions
+    //    32w .. 32w+31; bits >= sb are zero), then the network in reverse
+    // (byte loads: a ciphertext may start at any byte; sb = 8 * ct bytes)
+    static_assert(SB == 8 * P::CT, "synd() reads exactly the ciphertext's bytes");
+    const uint8_t *c = cts + it.ct_off;
+    uint32_t z[R];
 #pragma unroll
-            for (int p = 0; p < SYN_PARTS; p++)
-                x ^= src[p * SYN_ROWW];
+    for (int j = 0; j < R; j++) {
+        const int w = lane + 32 * j;
+        uint32_t v = 0;
+        if (w < CTW) {
+#pragma unroll
+            for (int b = 0; b < 4; b++)
+                if (4 * w + b < P::CT)
+                    v |= (uint32_t)__ldg(c + 4 * w + b) << (8 * b);
         }
-        sm.syn[q * SYN + w] = x;
+        z[j] = v;
     }
-    __syncthreads();
-
-    // ---- 2. transpose: S_[j*M + k] bit q = bit k of syndrome j of ct q ----
-    for (int w = warp; w < TW; w += TILE_THREADS / 32) {
-        const uint32_t v = sm.syn[lane * SYN + w];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int j = 2 * w + h;
+    for (int l = 2 * M - 2; l >= 0; l--)
+        swap_layer<S>(z, it.bctl, l, lane);
+    // 2a. depth 0 on u = bit * 1/g(a)^2: the pair (w, w + 2^(m-6)) is this
+    //     lane's (z[j], z[j + R/2])
+    const uint32_t *wf = it.wfft;
 #pragma unroll
-            for (int k = 0; k < M; k++) {
-                const uint32_t bal = __ballot_sync(FULL, (v >> (16 * h + k)) & 1u);
-                if (lane == ((j * M + k) & 31))
-                    sm.S_[j * M + k] = bal;
-            }
+    for (int j = 0; j < R / 2; j++) {
+        const int wa = lane + 32 * j, wb = wa + NWD / 2;
+        const uint32_t *g = tw + (size_t)wa * 16;
+        uint32_t A[M], B[M], G[M], p[2 * M - 1];
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+            B[k] = z[j + R / 2] & __ldg(wf + k * NWD + wb);
+            A[k] = (z[j] & __ldg(wf + k * NWD + wa)) ^ B[k];
+            G[k] = __ldg(g + k);
         }
-    }
-    for (int v = tid; v < R * M; v += blockDim.x)
-        sm.ring[v] = (v == M) ? FULL : 0u;  // B = x
-    __syncthreads();
-
-    // ---- 3. scaled Berlekamp-Massey, two warps per 32 coefficients ---------
-    // Warps [NWB, 2 NWB) own the coefficients (thread i of the role owns C_i
-    // and its B ring slot) and do the update C <- b*C + d*x*B; warps
-    // [0, NWB) compute the shares C_i * S_{N-i} of the next discrepancy.
-    // Per step: (A) update: d*x*B, the one product that needs this step's
-    // discrepancy (b*C was formed in the previous step); barrier; (B) the
-    // discrepancy warps multiply the new C by the syndromes while the
-    // update warps form b*C for the next step; barrier.  Two warps per
-    // scheduler share the work and hide each other's latency.
-    const bool dsc = warp < NWB;
-    const bool upd = warp >= NWB && warp < 2 * NWB;
-    const int i = upd ? tid - 32 * NWB : tid;
-    uint32_t C[M], bb[M], q1[2 * M - 1];
-#pragma unroll
-    for (int k = 0; k < M; k++) {
-        C[k] = (i == 0 && k == 0) ? FULL : 0u;
-        bb[k] = k == 0 ? FULL : 0u;
-    }
-#pragma unroll
-    for (int k = 0; k < 2 * M - 1; k++)
-        q1[k] = k < M ? C[k] : 0u;  // b*C with b = 1
-    int Lq = 0;  // L of ciphertext `lane` (update warps)
-    // discrepancy warps: share of discrepancy N, C_i * S_{N-i} for
-    // i <= min(N, t), XOR-reduced over the warp into part[N & 1][warp]
-    auto partial = [&](int N) {
-        const int lim = N < T ? N : T;
-        uint32_t p[2 * M - 1];
 #pragma unroll
         for (int k = 0; k < 2 * M - 1; k++)
             p[k] = 0;
-        if (i <= lim) {
-            uint32_t s[M];
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                s[k] = sm.S_[(N - i) * M + k];
-            bs_mul_acc<M>(p, C, s);
-            bs_reduce<M>(p);
-        }
+        bs_mul_acc<M>(p, G, A);
+        bs_reduce<M>(p);
 #pragma unroll
         for (int k = 0; k < M; k++) {
-            const uint32_t v = __reduce_xor_sync(FULL, p[k]);
-            if (lane == 0)
-                sm.part[N & 1][warp][k] = v;
-        }
-    };
-    if (dsc)
-        partial(0);
-    __syncthreads();
-#pragma unroll 1
-    for (int N = 0; N < 2 * T; N++) {
-        if (upd) {
-            // (A) the discrepancy, then the update
-            uint32_t dd[16];
-#pragma unroll
-            for (int k = 0; k < 16; k++)
-                dd[k] = 0;
-#pragma unroll
-            for (int w = 0; w < NWB; w++) {
-                const uint4 *pr = reinterpret_cast<const uint4 *>(sm.part[N & 1][w]);
-#pragma unroll
-                for (int v = 0; v < 4; v++) {
-                    const uint4 x = pr[v];
-                    dd[4 * v] ^= x.x;
-                    dd[4 * v + 1] ^= x.y;
-                    dd[4 * v + 2] ^= x.z;
-                    dd[4 * v + 3] ^= x.w;
-                }
-            }
-            uint32_t d[M], mne = 0;
-#pragma unroll
-            for (int k = 0; k < M; k++) {
-                d[k] = dd[k];
-                mne |= dd[k];
-            }
-            const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
-            const uint32_t mle = __ballot_sync(FULL, my_mle);
-            Lq = my_mle ? N + 1 - Lq : Lq;
-            // Coefficients above N + 1 of C and x*B are still zero (their
-            // ring entries were never written): whole warps past that skip.
-            if (i <= T && i <= N + 1) {
-                int slot = i + (R - (N % R)) % R;
-                slot = slot >= R ? slot - R : slot;
-                uint32_t *bp = sm.ring + slot * M;
-                uint32_t bv[M];
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    bv[k] = bp[k];
-                bs_mul_acc<M>(q1, d, bv);
-                bs_reduce<M>(q1);
-#pragma unroll
-                for (int k = 0; k < M; k++) {
-                    bp[k] = (bv[k] & ~mle) | (C[k] & mle);
-                    C[k] = q1[k];
-                    sm.cs[i * M + k] = q1[k];
-                }
-            }
-            const int freeslot = (R - ((N + 1) % R)) % R;
-            if (i < M)
-                sm.ring[freeslot * M + i] = 0;
-#pragma unroll
-            for (int k = 0; k < M; k++)
-                bb[k] = (bb[k] & ~mle) | (d[k] & mle);
-        }
-        __syncthreads();
-        if (N + 1 < 2 * T) {
-            // (B) next discrepancy shares; b*C for the next update
-            if (dsc) {
-                const int lim = N + 1 < T ? N + 1 : T;
-                if (i <= lim)
-#pragma unroll
-                    for (int k = 0; k < M; k++)
-                        C[k] = sm.cs[i * M + k];
-                partial(N + 1);
-            } else if (upd && i <= T && i <= N + 2) {
-#pragma unroll
-                for (int k = 0; k < 2 * M - 1; k++)
-                    q1[k] = 0;
-                bs_mul_acc<M>(q1, bb, C);
-            }
-            __syncthreads();
+            fa[k * NWD + wa] = A[k];
+            fa[k * NWD + wb] = B[k] ^ p[k];
         }
     }
-    // ---- 4. radix conversion, converted locators out -----------------------
-    // Entry x of the conversion array is C[T-x] (bm.c:62-65 reverses the
-    // locator before root() evaluates it), zero for T < x < 2^D; S_ is free.
-    using F = FftDims<S>;
-    static_assert(F::NX * M <= 2 * T * M && F::NX * 16 <= TILE_LOC_WORDS, "conversion array size");
-    if (upd && i <= T)
+    __syncwarp();
+    // 2b. depths 1 .. D'-2: pairs (wa, wa + Sw), Sw = 2^(m-d-6) words
+#pragma unroll 1
+    for (int d = 1; d < DS - 1; d++) {
+        const int sbit = M - d - 6, Sw = 1 << sbit;
+        const uint32_t *twd = tw + (size_t)(NWD - (NWD >> d)) * 16;
+#pragma unroll 1
+        for (int j = 0; j < R / 2; j++) {
+            const int P2 = lane + 32 * j;
+            const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
+            const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+            uint32_t A[M], B[M], G[M], p[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                B[k] = fa[k * NWD + wa + Sw];
+                A[k] = fa[k * NWD + wa] ^ B[k];
+                G[k] = __ldg(g + k);
+            }
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            bs_mul_acc<M>(p, G, A);
+            bs_reduce<M>(p);
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                fa[k * NWD + wa] = A[k];
+                fa[k * NWD + wa + Sw] = B[k] ^ p[k];
+            }
+        }
+        __syncwarp();
+    }
+    // 2c/3. depth D'-1 pairs adjacent words (one twiddle word); each word is
+    //       a group: its parity per plane goes out as the sum of sub-problem
+    //       bitrev_D'(word)
+    {
+        const uint32_t *g = tw + (size_t)(NWD - (NWD >> (DS - 1))) * 16;
+        uint32_t G[M];
 #pragma unroll
         for (int k = 0; k < M; k++)
-            sm.S_[(T - i) * M + k] = C[k];
-    for (int v = tid; v < (F::NX - T - 1) * M; v += blockDim.x)
-        sm.S_[(T + 1) * M + v] = 0u;
-    __syncthreads();
-    fft_convert<S, M, TILE_THREADS>(sm.S_, scalpow, tid, [] { __syncthreads(); });
-    for (int v = tid; v < F::NX * M; v += blockDim.x) {
-        const int x = v / M, k = v - x * M;
-        loc_bs[x * 16 + k] = sm.S_[v];
+            G[k] = __ldg(g + k);
+#pragma unroll 1
+        for (int j = 0; j < R / 2; j++) {
+            const int wa = 2 * (lane + 32 * j);
+            uint32_t A[M], B[M], p[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                B[k] = fa[k * NWD + wa + 1];
+                A[k] = fa[k * NWD + wa] ^ B[k];
+            }
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            bs_mul_acc<M>(p, G, A);
+            bs_reduce<M>(p);
+            uint32_t pa = 0, pb = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                pa |= (uint32_t)(__popc(A[k]) & 1) << k;
+                pb |= (uint32_t)(__popc(B[k] ^ p[k]) & 1) << k;
+            }
+            const int sa = (int)(__brev((uint32_t)wa) >> (32 - DS));
+            const int sb = (int)(__brev((uint32_t)(wa + 1)) >> (32 - DS));
+            sums[sa * 32 + q] = (uint16_t)pa;
+            sums[sb * 32 + q] = (uint16_t)pb;
+        }
+    }
+    __syncwarp();  // fa is refilled by this warp's next ciphertext, if any
+}
+
+// Four CTAs per tile; warp w of CTA c handles ciphertext 8c + w of the tile.
+__global__ void __launch_bounds__(TS_WARPS * 32) k_tile_tsynd(const LatItem *__restrict__ items,
+                                                              const uint8_t *__restrict__ cts,
+                                                              uint32_t *__restrict__ scratch, FftPlans plans)
+{
+    extern __shared__ __align__(16) uint32_t smem_ts[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x >> 2, q = TS_WARPS * (blockIdx.x & 3) + warp, slot = 32 * t + q;
+    const LatItem it = items[slot];
+    if (it.set < 0 || q >= (int)items[(size_t)t * 32].pad)
+        return;  // whole warp: no block-wide barrier follows
+    uint16_t *sums = reinterpret_cast<uint16_t *>(scratch + (size_t)t * TILE_SCRATCH_WORDS + TILE_LOC_WORDS);
+    uint32_t *fa = smem_ts + (size_t)warp * TS_FA_WORDS;
+    switch (it.set) {
+    case S348864: tsynd_one<S348864>(it, cts, plans.p[S348864].tw, fa, sums, q, lane); break;
+    case S460896: tsynd_one<S460896>(it, cts, plans.p[S460896].tw, fa, sums, q, lane); break;
+    case S6688128: tsynd_one<S6688128>(it, cts, plans.p[S6688128].tw, fa, sums, q, lane); break;
+    case S6960119: tsynd_one<S6960119>(it, cts, plans.p[S6960119].tw, fa, sums, q, lane); break;
+    default: tsynd_one<S8192128>(it, cts, plans.p[S8192128].tw, fa, sums, q, lane); break;
     }
 }
 
-__global__ void __launch_bounds__(TILE_THREADS, 2) k_tile_bm(const LatItem *__restrict__ items, const uint32_t *__restrict__ synp,
-                                                 uint32_t *__restrict__ loc_bs, FftPlans plans)
+// Threads of k_tile_bm: thread i owns locator coefficient i (t+1 <= 129).
+constexpr int BM_WARPS = 5;
+constexpr int BM_THREADS = BM_WARPS * 32;
+
+template <int S> struct TileSmem {
+    using Z = TsDims<S>;
+    static constexpr int SS = Z::M | 1;  // odd plane stride: per-coefficient rows meet no bank conflicts
+    uint32_t sx[Z::NS * SS];             // group sums -> syndromes -> converted locators
+    uint32_t ring[(Z::T + 2) * SS];      // B, rotated one slot per step (the x*B shift)
+    alignas(16) uint32_t part[2][BM_WARPS][16];  // per-warp discrepancy shares, by step parity
+};
+
+// Steps 1-2 of k_tile_bm, by the whole CTA: gather the tile's group sums
+// (sx[s][k] bit q = plane k of sum s of ciphertext q; zero for q >= count),
+// then the transposed radix conversion: sx[j] = syndrome j, bitsliced.
+template <int S>
+__device__ __forceinline__ void tile_syndromes(int count, const uint32_t *tile_scratch, TileSmem<S> &sm,
+                                               const uint16_t *scalpow)
+{
+    using Z = TsDims<S>;
+    constexpr int M = Z::M, NS = Z::NS, SS = TileSmem<S>::SS;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const uint16_t *sums = reinterpret_cast<const uint16_t *>(tile_scratch + TILE_LOC_WORDS);
+    for (int s = warp; s < NS; s += BM_WARPS) {
+        const uint32_t v = lane < count ? (uint32_t)sums[s * 32 + lane] : 0u;
+        uint32_t mine = 0;
+#pragma unroll
+        for (int k = 0; k < M; k++) {
+            const uint32_t b = __ballot_sync(FULL, (v >> k) & 1u);
+            if (lane == k)
+                mine = b;
+        }
+        if (lane < M)
+            sm.sx[s * SS + lane] = mine;
+    }
+    __syncthreads();
+    fft_convert_t<S, SS, BM_THREADS>(sm.sx, scalpow, tid, [] { __syncthreads(); });
+}
+
+template <int S>
+__device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch, uint32_t *loc_bs,
+                                        const uint16_t *scalpow, uint8_t *smem_raw)
+{
+    using Z = TsDims<S>;
+    using Sm = TileSmem<S>;
+    constexpr int M = Z::M, T = Z::T, NS = Z::NS, SS = Sm::SS, R = T + 2;
+    static_assert(T + 1 <= BM_THREADS, "one thread per locator coefficient");
+    Sm &sm = *reinterpret_cast<Sm *>(smem_raw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    // ---- 1-2. syndromes, bitsliced across the tile ------------------------
+    for (int v = tid; v < R * SS; v += BM_THREADS)
+        sm.ring[v] = (v == SS) ? FULL : 0u;  // B = x
+    tile_syndromes<S>(count, tile_scratch, sm, scalpow);
+
+    // ---- 3. scaled Berlekamp-Massey, thread i owns C_i -------------------
+    // Per step: (1) warps holding coefficients i <= min(N, t, max L) form
+    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp;
+    // barrier; (2) every thread sums the shares (d, per ciphertext), every
+    // warp derives the same decisions, and the owners of i <= new max L form
+    // C_i <- b*C_i + d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in
+    // the ring slot of coefficient i.  Ring entries above that, up to the
+    // largest possible degree of B, only take the swap (C_i = 0 there).
+    const int i = tid;
+    uint32_t C[M], bb[M];
+#pragma unroll
+    for (int k = 0; k < M; k++) {
+        C[k] = (i == 0 && k == 0) ? FULL : 0u;
+        bb[k] = k == 0 ? FULL : 0u;  // b = 1
+    }
+    int Lq = 0, Bd = 1;    // lane q: L and a bound on deg B of ciphertext q
+    int Lmax = 0, Bmax = 1;
+#pragma unroll 1
+    for (int N = 0; N < 2 * T; N++) {
+        const int lim = min(N, min(T, Lmax));
+        if (32 * warp <= lim) {
+            uint32_t p[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                p[k] = 0;
+            if (i <= lim) {
+                uint32_t sv[M];
+                const uint32_t *src = sm.sx + (N - i) * SS;
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    sv[k] = src[k];
+                bs_mul_acc<M>(p, C, sv);
+                bs_reduce<M>(p);
+            }
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                const uint32_t v = __reduce_xor_sync(FULL, p[k]);
+                if (lane == 0)
+                    sm.part[N & 1][warp][k] = v;
+            }
+        }
+        __syncthreads();
+        uint32_t d[M], mne = 0;
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            d[k] = 0;
+        for (int w = 0; 32 * w <= lim; w++) {
+            const uint4 *pr = reinterpret_cast<const uint4 *>(sm.part[N & 1][w]);
+#pragma unroll
+            for (int v = 0; v < (M + 3) / 4; v++) {
+                const uint4 x = pr[v];
+                if (4 * v + 0 < M) d[4 * v + 0] ^= x.x;
+                if (4 * v + 1 < M) d[4 * v + 1] ^= x.y;
+                if (4 * v + 2 < M) d[4 * v + 2] ^= x.z;
+                if (4 * v + 3 < M) d[4 * v + 3] ^= x.w;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            mne |= d[k];
+        const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
+        const uint32_t mle = __ballot_sync(FULL, my_mle);
+        const int Lnew = my_mle ? N + 1 - Lq : Lq;
+        const int Bdnew = min(min(my_mle ? Lq : Bd, T) + 1, T);
+        const int Lb = min(__reduce_max_sync(FULL, (unsigned)Lnew), (unsigned)T);
+        int slot = i - N % R;
+        slot = slot < 0 ? slot + R : slot;
+        uint32_t *bp = sm.ring + slot * SS;
+        if (i <= Lb) {
+            uint32_t bv[M], q1[2 * M - 1];
+#pragma unroll
+            for (int k = 0; k < 2 * M - 1; k++)
+                q1[k] = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bv[k] = bp[k];
+            bs_mul_acc<M>(q1, bb, C);
+            bs_mul_acc<M>(q1, d, bv);
+            bs_reduce<M>(q1);
+#pragma unroll
+            for (int k = 0; k < M; k++) {
+                bp[k] = (bv[k] & ~mle) | (C[k] & mle);
+                C[k] = q1[k];
+            }
+        } else if (i <= min(Bmax, T)) {
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bp[k] &= ~mle;
+        }
+        // the slot that becomes coefficient 0 of x*B at step N+1
+        const int freeslot = (R - (N + 1) % R) % R;
+        if (tid < M)
+            sm.ring[freeslot * SS + tid] = 0;
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            bb[k] = (bb[k] & ~mle) | (d[k] & mle);
+        Lq = Lnew;
+        Bd = Bdnew;
+        Lmax = Lb;
+        // (slots past `count` never take the swap: their syndromes are zero)
+        Bmax = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)Bdnew : 0u);
+    }
+    __syncthreads();
+    // ---- 4. radix conversion of the reversed locators, out ---------------
+    // Entry x of the conversion array is C[T-x] (bm.c:62-65 reverses the
+    // locator before root() evaluates it), zero for T < x < 2^D.
+    using F = FftDims<S>;
+    static_assert(F::NX <= NS && F::NX * 16 <= TILE_LOC_WORDS, "conversion array size");
+    if (i <= T)
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            sm.sx[(T - i) * SS + k] = C[k];
+    for (int v = tid; v < (F::NX - T - 1) * SS; v += BM_THREADS)
+        sm.sx[(T + 1) * SS + v] = 0u;
+    __syncthreads();
+    fft_convert<S, SS, BM_THREADS>(sm.sx, scalpow, tid, [] { __syncthreads(); });
+    for (int v = tid; v < F::NX * M; v += BM_THREADS) {
+        const int x = v / M, k = v - x * M;
+        loc_bs[x * 16 + k] = sm.sx[x * SS + k];
+    }
+}
+
+__global__ void __launch_bounds__(BM_THREADS) k_tile_bm(const LatItem *__restrict__ items,
+                                                        uint32_t *__restrict__ scratch, FftPlans plans)
 {
     extern __shared__ __align__(16) uint8_t smem_tile[];
     const LatItem *ti = items + (size_t)blockIdx.x * 32;
     const int count = (int)ti[0].pad;
-    const uint32_t *sp = synp + (size_t)blockIdx.x * 32 * SYN_PARTS * SYN_ROWW;
-    uint32_t *out = loc_bs + (size_t)blockIdx.x * TILE_LOC_WORDS;
+    uint32_t *tsc = scratch + (size_t)blockIdx.x * TILE_SCRATCH_WORDS;
     switch (ti[0].set) {
-    case S348864: tile_bm<S348864>(count, sp, out, plans.p[S348864].scalpow, smem_tile); break;
-    case S460896: tile_bm<S460896>(count, sp, out, plans.p[S460896].scalpow, smem_tile); break;
-    case S6688128: tile_bm<S6688128>(count, sp, out, plans.p[S6688128].scalpow, smem_tile); break;
-    case S6960119: tile_bm<S6960119>(count, sp, out, plans.p[S6960119].scalpow, smem_tile); break;
-    default: tile_bm<S8192128>(count, sp, out, plans.p[S8192128].scalpow, smem_tile); break;
+    case S348864: tile_bm<S348864>(count, tsc, tsc, plans.p[S348864].scalpow, smem_tile); break;
+    case S460896: tile_bm<S460896>(count, tsc, tsc, plans.p[S460896].scalpow, smem_tile); break;
+    case S6688128: tile_bm<S6688128>(count, tsc, tsc, plans.p[S6688128].scalpow, smem_tile); break;
+    case S6960119: tile_bm<S6960119>(count, tsc, tsc, plans.p[S6960119].scalpow, smem_tile); break;
+    default: tile_bm<S8192128>(count, tsc, tsc, plans.p[S8192128].scalpow, smem_tile); break;
     }
 }
 
@@ -352,7 +436,7 @@ __global__ void __launch_bounds__(ROOT_WARPS * 32) k_root_tile(const LatItem *__
     const LatItem it = items[slot];
     if (it.set < 0 || q >= (int)items[(size_t)t * 32].pad)
         return;  // whole warp: no block-wide barrier follows
-    const uint32_t *cv = loc_bs + (size_t)t * TILE_LOC_WORDS;
+    const uint32_t *cv = loc_bs + (size_t)t * TILE_SCRATCH_WORDS;
     uint32_t *fa = smem_root + (size_t)warp * ROOT_FA_WORDS;
     uint16_t *wp = weight ? weight + slot : nullptr;
     switch (it.set) {
@@ -375,6 +459,122 @@ size_t tile_smem_bytes()
     return m;
 }
 
+// Items of a single-key batch of `count` ciphertexts at a ct_bytes stride;
+// error rows at an nw-word stride, row c = ciphertext c.
+__global__ void k_tile_items(LatItem *__restrict__ items, uint32_t count, const uint32_t *wfft,
+                             const uint32_t *bctl, uint32_t ct_bytes, uint32_t nw, int set, uint32_t nslots)
+{
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= nslots)
+        return;
+    const uint32_t t = slot >> 5, q = slot & 31, left = count - 32 * t;
+    const uint32_t cnt = left < 32 ? left : 32;
+    items[slot] = LatItem{wfft, bctl, slot * ct_bytes, slot * nw, q < cnt ? set : -1, (int32_t)cnt};
+}
+
+// The syndromes of every ciphertext of a tile as rows of 2t u16 (the
+// per-stage hook's layout): steps 1-2 of k_tile_bm, then a transpose out.
+template <int S>
+__device__ __forceinline__ void synd_out(int count, const uint32_t *tsc, uint16_t *synd, const uint16_t *scalpow,
+                                         uint8_t *smem_raw)
+{
+    using Sm = TileSmem<S>;
+    constexpr int M = Set<S>::M, T = Set<S>::T;
+    Sm &sm = *reinterpret_cast<Sm *>(smem_raw);
+    tile_syndromes<S>(count, tsc, sm, scalpow);
+    for (int v = threadIdx.x; v < count * 2 * T; v += BM_THREADS) {
+        const int q = v / (2 * T), j = v - q * 2 * T;
+        uint32_t x = 0;
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            x |= ((sm.sx[j * Sm::SS + k] >> q) & 1u) << k;
+        synd[((size_t)blockIdx.x * 32 + q) * 2 * T + j] = (uint16_t)x;
+    }
+}
+
+__global__ void __launch_bounds__(BM_THREADS) k_tile_synd_out(const LatItem *__restrict__ items,
+                                                              const uint32_t *__restrict__ scratch,
+                                                              uint16_t *__restrict__ synd, FftPlans plans)
+{
+    extern __shared__ __align__(16) uint8_t smem_tile[];
+    const LatItem *ti = items + (size_t)blockIdx.x * 32;
+    const int count = (int)ti[0].pad;
+    const uint32_t *tsc = scratch + (size_t)blockIdx.x * TILE_SCRATCH_WORDS;
+    switch (ti[0].set) {
+    case S348864: synd_out<S348864>(count, tsc, synd, plans.p[S348864].scalpow, smem_tile); break;
+    case S460896: synd_out<S460896>(count, tsc, synd, plans.p[S460896].scalpow, smem_tile); break;
+    case S6688128: synd_out<S6688128>(count, tsc, synd, plans.p[S6688128].scalpow, smem_tile); break;
+    case S6960119: synd_out<S6960119>(count, tsc, synd, plans.p[S6960119].scalpow, smem_tile); break;
+    default: synd_out<S8192128>(count, tsc, synd, plans.p[S8192128].scalpow, smem_tile); break;
+    }
+}
+
+cudaError_t tile_prepare(int dev, size_t smem, size_t ts_smem, size_t root_smem);
+
+// The tile path over one key's batch (d_scratch: tile_single_scratch_words).
+cudaError_t launch_tile_single(const KeyDev &k, const uint8_t *d_cts, size_t count, uint32_t *d_scratch,
+                               uint32_t *d_err, uint16_t *d_weight, uint16_t *d_synd, const FftPlans &plans,
+                               cudaStream_t s, LaunchCounter lc)
+{
+    if (count == 0)
+        return cudaSuccess;
+    const SetInfo si = set_info(k.set);
+    const uint32_t ntiles = (uint32_t)((count + 31) / 32);
+    LatItem *items = reinterpret_cast<LatItem *>(d_scratch);
+    uint32_t *tiles = d_scratch + (size_t)ntiles * 32 * sizeof(LatItem) / 4;
+    k_tile_items<<<(ntiles * 32 + 255) / 256, 256, 0, s>>>(items, (uint32_t)count, k.wfft, k.bctl, (uint32_t)si.ct,
+                                                          (uint32_t)si.nw, k.set, ntiles * 32);
+    lc.bump();
+    if (d_synd) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        const size_t smem = tile_smem_bytes();
+        cudaError_t e = tile_prepare(dev, smem, TS_WARPS * TS_FA_WORDS * 4, ROOT_WARPS * ROOT_FA_WORDS * 4);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_tile_synd_out, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+            return e;
+        k_tile_tsynd<<<ntiles * (32 / TS_WARPS), TS_WARPS * 32, TS_WARPS * TS_FA_WORDS * 4, s>>>(items, d_cts, tiles,
+                                                                                                plans);
+        k_tile_synd_out<<<ntiles, BM_THREADS, smem, s>>>(items, tiles, d_synd, plans);
+        lc.bump(2);
+        return cudaGetLastError();
+    }
+    return launch_tile_path(items, d_cts, ntiles, tiles, d_err, d_weight, plans, s, lc);
+}
+
+size_t tile_single_scratch_words(size_t count)
+{
+    const size_t ntiles = (count + 31) / 32;
+    return ntiles * 32 * sizeof(LatItem) / 4 + ntiles * TILE_SCRATCH_WORDS;
+}
+
+// Raises the tile kernels' shared-memory limits once per device.
+cudaError_t tile_prepare(int dev, size_t smem, size_t ts_smem, size_t root_smem)
+{
+    static size_t attr[64] = {};
+    size_t &set_to = attr[dev & 63];
+    if (set_to >= smem)
+        return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_tsynd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts_smem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)root_smem);
+    // One shared-memory split for all three kernels, so that CTAs of
+    // concurrent batches' kernels can share an SM without it draining to
+    // change its split.
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_tsynd, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e == cudaSuccess)
+        set_to = smem;
+    return e;
+}
+
 // ntiles tiles of 32 item slots; weights are indexed by item slot.
 cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t ntiles, uint32_t *d_scratch,
                              uint32_t *d_err, uint16_t *d_weight, const FftPlans &plans, cudaStream_t s,
@@ -382,36 +582,18 @@ cudaError_t launch_tile_path(const void *d_items, const uint8_t *d_cts, uint32_t
 {
     if (ntiles == 0)
         return cudaSuccess;
-    // the opt-in is per device: remember what each device has been given
-    static size_t attr[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
-    size_t &set_to = attr[dev & 63];
     const size_t smem = tile_smem_bytes();
+    const size_t ts_smem = TS_WARPS * TS_FA_WORDS * 4;
     const size_t root_smem = ROOT_WARPS * ROOT_FA_WORDS * 4;
-    if (set_to < smem) {
-        cudaError_t e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)root_smem);
-        // One shared-memory split for all three kernels, so that CTAs of
-        // concurrent batches' kernels can share an SM without it draining to
-        // change its split (two k_tile_bm or two k_root_tile CTAs per SM).
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_tile_synd, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_tile_bm, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_root_tile, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-        if (e != cudaSuccess)
-            return e;
-        set_to = smem;
-    }
+    if (cudaError_t e = tile_prepare(dev, smem, ts_smem, root_smem); e != cudaSuccess)
+        return e;
     const LatItem *items = static_cast<const LatItem *>(d_items);
-    uint32_t *d_loc_bs = d_scratch;
-    uint32_t *d_synp = d_scratch + (size_t)ntiles * TILE_LOC_WORDS;
-    k_tile_synd<<<ntiles * 32 * SYN_PARTS, 256, 0, s>>>(items, d_cts, d_synp);
-    k_tile_bm<<<ntiles, TILE_THREADS, smem, s>>>(items, d_synp, d_loc_bs, plans);
-    k_root_tile<<<ntiles * 4, ROOT_WARPS * 32, root_smem, s>>>(items, d_loc_bs, d_err, d_weight, plans);
+    k_tile_tsynd<<<ntiles * (32 / TS_WARPS), TS_WARPS * 32, ts_smem, s>>>(items, d_cts, d_scratch, plans);
+    k_tile_bm<<<ntiles, BM_THREADS, smem, s>>>(items, d_scratch, plans);
+    k_root_tile<<<ntiles * (32 / ROOT_WARPS), ROOT_WARPS * 32, root_smem, s>>>(items, d_scratch, d_err, d_weight,
+                                                                             plans);
     lc.bump(3);
     return cudaGetLastError();
 }

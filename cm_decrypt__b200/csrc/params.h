@@ -27,6 +27,10 @@ constexpr CMD_HD int fft_depth(int t)
         d++;
     return d;
 }
+// Depth of the transposed additive FFT that forms the 2t syndromes: the
+// smallest D' with 2^D' >= 2t (7 for t = 64, 8 for t = 96, 119, 128; m - 5 for
+// every set).
+constexpr CMD_HD int synd_depth(int t) { return fft_depth(2 * t - 1); }
 // M: GFBITS, N: SYS_N, T: SYS_T, CT: ciphertext = SYND_BYTES, SK: secret key.
 #define CMD_DEFINE_SET(ID, ID_NUM, M_, N_, T_, CT_, SK_)                               \
     template <> struct Set<ID> {                                                       \

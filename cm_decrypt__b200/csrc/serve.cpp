@@ -374,10 +374,12 @@ int cmd_server::launch(Slot &sl)
     }
     FusedKeyRef *krefs = reinterpret_cast<FusedKeyRef *>(sl.h_in + lay.keys);
     std::vector<int> kset(kid.size());
+    std::vector<const uint32_t *> kwfft(kid.size());
     for (size_t k = 0; k < kid.size(); k++) {
         const cmd_key *key = keys[kid[k]].key;
         krefs[k] = key_ref(key->dev);
         kset[k] = key->dev.set;
+        kwfft[k] = key->dev.wfft;
     }
     LaunchCounter lc{&eng->launches};
     cudaStream_t s = sl.stream;
@@ -414,10 +416,11 @@ int cmd_server::launch(Slot &sl)
                 if (q < cnt) {
                     const uint32_t r = by_set[i + q];
                     const FusedKeyRef &kr = krefs[key_idx[r]];
-                    items[slot] = LatItem{kr.tab, kr.bctl, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE, kr.set, cnt};
+                    items[slot] = LatItem{kwfft[key_idx[r]], kr.bctl, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE,
+                                          kr.set, cnt};
                     sl.slot_of[r] = slot;
                 } else {
-                    items[slot] = LatItem{krefs[0].tab, krefs[0].bctl, 0, slot * ERR_STRIDE, -1, cnt};
+                    items[slot] = LatItem{kwfft[0], krefs[0].bctl, 0, slot * ERR_STRIDE, -1, cnt};
                 }
             }
             ntiles++;

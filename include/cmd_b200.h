@@ -101,8 +101,12 @@ int cmd_key_synd_table(const cmd_key *key, uint16_t *h_tab, size_t entries);
 /* ---- batched decrypt --------------------------------------------------- */
 /* Path selector: CMD_PATH_PLAIN runs the three per-stage kernels (syndrome,
  * Berlekamp-Massey, root search + pack); CMD_PATH_FUSED runs the fused
- * bitsliced kernel; CMD_PATH_AUTO lets the engine's tuner choose. */
-typedef enum { CMD_PATH_AUTO = 0, CMD_PATH_PLAIN = 1, CMD_PATH_FUSED = 2 } cmd_path;
+ * bitsliced kernel; CMD_PATH_TILE runs the serving loop's latency kernels
+ * (syndromes by the transposed additive FFT, a CTA per 32-ciphertext tile
+ * for Berlekamp-Massey, a warp per ciphertext for the root search);
+ * CMD_PATH_AUTO lets the engine's tuner choose.  Graph capture takes AUTO,
+ * PLAIN and FUSED. */
+typedef enum { CMD_PATH_AUTO = 0, CMD_PATH_PLAIN = 1, CMD_PATH_FUSED = 2, CMD_PATH_TILE = 3 } cmd_path;
 
 /* Replaces the per-ciphertext loop memcpy -> synd -> bm -> root ->
  * build_error_vector (CPU/param/param6960119/src/decrypt.c:163-177, 43-53).
@@ -159,6 +163,11 @@ int cmd_decrypt_plain_noalloc(const cmd_key *key, const uint8_t *d_cts,
  * util.c:102-114). */
 int cmd_stage_synd(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
                    size_t count, uint16_t *d_synd, void *stream);
+/* synd() by the serving path's method (the transposed additive FFT over the
+ * key's support network, no syndrome table): the same count rows of 2t u16
+ * (CPU/param/param6960119/src/util.c:102-114). */
+int cmd_stage_synd_fft(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
+                       size_t count, uint16_t *d_synd, void *stream);
 /* bm(): d_loc = count rows of t+1 u16, reversed as bm() writes them
  * (CPU/src/common/bm.c:12-68). */
 int cmd_stage_bm(cmd_engine *eng, cmd_set set, const uint16_t *d_synd,

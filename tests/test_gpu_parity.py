@@ -61,16 +61,19 @@ def test_stages(oracle_mod, engine, keys, s):
     n = cts.shape[0]
     d_ct = dev(cts)
     d_s = torch.zeros((n, 2 * info.t), dtype=torch.int16, device="cuda")
+    d_sf = torch.zeros((n, 2 * info.t), dtype=torch.int16, device="cuda")
     d_l = torch.zeros((n, info.t + 1), dtype=torch.int16, device="cuda")
     d_img = torch.zeros((n, info.n), dtype=torch.int16, device="cuda")
     d_e = torch.zeros((n, info.err_words), dtype=torch.int32, device="cuda")
     d_w = torch.zeros(n, dtype=torch.int16, device="cuda")
     cmd.synd(engine, k, d_ct.data_ptr(), n, d_s.data_ptr())
+    cmd.synd_fft(engine, k, d_ct.data_ptr(), n, d_sf.data_ptr())
     cmd.bm(engine, s, d_s.data_ptr(), n, d_l.data_ptr())
     cmd.root_images(engine, k, d_l.data_ptr(), n, d_img.data_ptr())
     cmd.root(engine, k, d_l.data_ptr(), n, d_e.data_ptr(), d_w.data_ptr())
     torch.cuda.synchronize()
     S = d_s.cpu().numpy().view(np.uint16)
+    SF = d_sf.cpu().numpy().view(np.uint16)
     Lc = d_l.cpu().numpy().view(np.uint16)
     IMG = d_img.cpu().numpy().view(np.uint16)
     E = words_to_bytes(d_e, info.n)
@@ -79,6 +82,7 @@ def test_stages(oracle_mod, engine, keys, s):
         ct = cts[i].tobytes()
         s_ref = o.synd(ct)
         assert np.array_equal(S[i], s_ref), ("synd", i)
+        assert np.array_equal(SF[i], s_ref), ("synd by the transposed FFT", i)
         l_ref = o.bm(s_ref)
         assert np.array_equal(Lc[i], l_ref), ("bm", i)
         img = o.root(l_ref)
@@ -94,7 +98,7 @@ def test_stages(oracle_mod, engine, keys, s):
         assert not tail.any()
 
 
-@pytest.mark.parametrize("path", ["plain", "fused"])
+@pytest.mark.parametrize("path", ["plain", "fused", "tile"])
 @pytest.mark.parametrize("s", SETS)
 def test_kem_fixture_errorstream(engine, keys, s, path):
     info = keys[s].info
@@ -103,7 +107,7 @@ def test_kem_fixture_errorstream(engine, keys, s, path):
     assert cmd.errorstream(s, err) == golden_errorstream(s)
 
 
-@pytest.mark.parametrize("path", ["plain", "fused"])
+@pytest.mark.parametrize("path", ["plain", "fused", "tile"])
 @pytest.mark.parametrize("s", SETS)
 def test_decrypt_vs_oracle(oracle_mod, engine, keys, s, path):
     o = oracle_mod.Oracle(s)
@@ -130,7 +134,7 @@ def test_derived_keys(oracle_mod, engine, s):
             assert np.array_equal(key.support(), L)
             pk = cmd.PubKey(s, sk)
             cts, planted, valid = pk.ciphertexts(seed=seed, count=70, malformed_permille=200)
-            for path in ("plain", "fused"):
+            for path in ("plain", "fused", "tile"):
                 err, _ = cmd.decrypt(engine, key, cts, path=path)
                 assert np.array_equal(err, o.decrypt(sk, cts, nthreads=8))
         finally:
@@ -232,7 +236,7 @@ def test_mixed_64_keys_every_row_vs_reference(oracle_mod, engine):
     assert np.array_equal(W, np.unpackbits(ref, axis=1).sum(axis=1))
 
 
-@pytest.mark.parametrize("path", ["plain", "fused"])
+@pytest.mark.parametrize("path", ["plain", "fused", "tile"])
 def test_full_size_properties(engine, keys, path):
     """Full-size batch at 6960119 (65,536 ciphertexts): every valid
     ciphertext decodes to exactly its planted weight-119 error vector."""
