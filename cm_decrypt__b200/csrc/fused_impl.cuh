@@ -22,7 +22,10 @@
 //     d*x*B instead of bm()'s C <- C + (d/b)*x*B: same decisions (d != 0,
 //     N >= 2L), same truncation, and by induction the result is lambda times
 //     bm()'s locator with lambda a product of nonzero b values -- the same
-//     roots, so the same flagged positions, with no inversion chain per step;
+//     roots, so the same flagged positions, with no inversion chain per step.
+//     deg C <= L for every ciphertext, so only coefficients up to the tile's
+//     largest L enter the discrepancy and the update (about half the slots
+//     of the reference loop bounds for weight-t errors, where L ~ N/2);
 //  5. root search (root_13.c:216-240 evaluates the locator at each support
 //     point): the locator is evaluated at all 2^m field elements by an
 //     additive FFT, then the key's support network (the Benes layers that
@@ -222,10 +225,14 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
         for (int k = 0; k < M; k++)
             bb[k] = k == 0 ? FULLMASK : 0u;       // b = 1
         int Lq = 0;                               // L of ciphertext `lane`
+        int Bd = 1;                               // bound on deg B of ciphertext `lane`
+        int Lmax = 0, Bmax = 1;                   // their maxima over the tile
         __syncwarp();
 #pragma unroll 1
         for (int N = 0; N < 2 * T; N++) {
-            const int lim = N < T ? N : T;
+            // deg C <= L for every ciphertext, so coefficients above the
+            // tile's largest L are zero: they take no part in the discrepancy
+            const int lim = min(N, min(T, Lmax));
             uint32_t p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
@@ -256,17 +263,28 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
             }
             const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
             const uint32_t mle = __ballot_sync(FULLMASK, my_mle);
+            const int Bdn = min(min(my_mle ? Lq : Bd, T) + 1, T);
             Lq = my_mle ? N + 1 - Lq : Lq;
+            const int Lb = min((int)__reduce_max_sync(FULLMASK, (unsigned)Lq), T);
+            const int Bm = min(Bmax, T);
             // Scaled update C <- b*C + d*x*B (see the note at the top of the
             // file): both products accumulate unreduced, one reduction.
-            // Before the update deg C <= N and deg x*B <= N + 1, so slots
-            // whose coefficients all exceed N + 1 hold zeros (their ring
-            // entries were never written) and are skipped.
+            // After the step deg C <= L, so coefficients above the tile's
+            // new largest L stay zero; B there only takes the swap (to C_i =
+            // 0) where its degree bound reaches, and is zero above that.
             int off = (R - (N % R)) % R;  // slot(i) = (i - N) mod R
+            const int hi = Lb > Bm ? Lb : Bm;
 #pragma unroll 1
-            for (int j = 0; j < NJ && 32 * j <= N + 1; j++) {
+            for (int j = 0; j < NJ && 32 * j <= hi; j++) {
                 const int i = lane + 32 * j;
-                if (i <= T) {
+                if (i > Lb && i <= Bm) {
+                    int slot = i + off;
+                    slot = slot >= R ? slot - R : slot;
+                    uint32_t *bp = ring + slot * M;
+#pragma unroll
+                    for (int k = 0; k < M; k++)
+                        bp[k] &= ~mle;
+                } else if (i <= Lb) {
                     int slot = i + off;
                     slot = slot >= R ? slot - R : slot;
                     uint32_t *bp = ring + slot * M;
@@ -296,6 +314,10 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
             const int freeslot = (R - ((N + 1) % R)) % R;
             if (lane < M)
                 ring[freeslot * M + lane] = 0;
+            Bd = Bdn;
+            Lmax = Lb;
+            // (lanes past the tile's count never take the swap: zero syndromes)
+            Bmax = (int)__reduce_max_sync(FULLMASK, lane < ntile ? (unsigned)Bd : 0u);
             __syncwarp();
         }
         // The reference's root search evaluates sum_x C[T-x] a^x
