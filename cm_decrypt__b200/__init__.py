@@ -146,6 +146,7 @@ def lib() -> ctypes.CDLL:
         "cmd_server_destroy": (None, [_vp]),
         "cmd_server_add_key": (_i32, [_vp, _i32, _vp, _sz, ctypes.POINTER(ctypes.c_uint32)]),
         "cmd_server_submit": (_i32, [_vp, ctypes.c_uint32, _vp, _vp, _u64]),
+        "cmd_server_submit_many": (_i32, [_vp, _sz, _vp, _vp, _sz, _vp, _sz, _vp, ctypes.POINTER(_sz)]),
         "cmd_server_poll": (_i32, [_vp, ctypes.POINTER(Completion), _sz, ctypes.POINTER(_sz), ctypes.c_uint32]),
         "cmd_server_drain": (_i32, [_vp, ctypes.c_uint32]),
         "cmd_server_stats_get": (_i32, [_vp, ctypes.POINTER(ServerStats), _i32]),
@@ -382,6 +383,22 @@ class Server:
         if rc not in (CMD_OK, CMD_E_BUSY):
             raise CmdError(rc, "cmd_server_submit")
         return rc
+
+    def submit_many(self, key_ids: np.ndarray, cts: np.ndarray, err_out: np.ndarray | None,
+                    tags: np.ndarray | None = None) -> int:
+        """Queues len(key_ids) requests under one lock (cts rows, err_out rows);
+        returns how many were accepted.  err_out must stay alive until completion."""
+        ki = np.ascontiguousarray(key_ids, np.uint32)
+        c = np.ascontiguousarray(cts, np.uint8)
+        tg = None if tags is None else np.ascontiguousarray(tags, np.uint64)
+        acc = _sz()
+        rc = lib().cmd_server_submit_many(self.handle, ki.size, _ptr(ki), _ptr(c), c.shape[1],
+                                          _ptr(err_out) if err_out is not None else None,
+                                          err_out.shape[1] if err_out is not None else 0,
+                                          _ptr(tg) if tg is not None else None, ctypes.byref(acc))
+        if rc not in (CMD_OK, CMD_E_BUSY):
+            raise CmdError(rc, "cmd_server_submit_many")
+        return acc.value
 
     def poll(self, max_n: int = 4096, timeout_us: int = 0) -> list[tuple[int, int, int, int]]:
         buf = (Completion * max_n)()

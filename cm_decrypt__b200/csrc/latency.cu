@@ -274,12 +274,13 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
 
     // ---- 3. scaled Berlekamp-Massey, thread i owns C_i -------------------
     // Per step: (1) warps holding coefficients i <= min(N, t, max L) form
-    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp;
-    // barrier; (2) every thread sums the shares (d, per ciphertext), every
-    // warp derives the same decisions, and the owners of i <= new max L form
-    // C_i <- b*C_i + d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in
-    // the ring slot of coefficient i.  Ring entries above that, up to the
-    // largest possible degree of B, only take the swap (C_i = 0 there).
+    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp,
+    // and the owners of i up to a bound on the new L form b*C_i; barrier;
+    // (2) every thread sums the shares (d, per ciphertext), every warp
+    // derives the same decisions, and the owners complete C_i <- b*C_i +
+    // d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in the ring slot
+    // of coefficient i.  Ring entries above the bound, up to the largest
+    // possible degree of B, only take the swap (C_i = 0 there).
     const int i = tid;
     uint32_t C[M], bb[M];
 #pragma unroll
@@ -289,11 +290,19 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
     }
     int Lq = 0, Bd = 1;    // lane q: L and a bound on deg B of ciphertext q
     int Lmax = 0, Bmax = 1;
+    int Lub = 1;           // bound on every ciphertext's L after this step
 #pragma unroll 1
     for (int N = 0; N < 2 * T; N++) {
         const int lim = min(N, min(T, Lmax));
+        const int ub = min(Lub, T);
+        // b*C_i does not depend on this step's discrepancy: it is formed
+        // before the barrier, while the discrepancy shares reduce
+        uint32_t q1[2 * M - 1];
+#pragma unroll
+        for (int k = 0; k < 2 * M - 1; k++)
+            q1[k] = 0;
         if (32 * warp <= lim) {
-            uint32_t p[2 * M - 1];
+            uint32_t p[2 * M - 1], red[M];
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
                 p[k] = 0;
@@ -307,11 +316,16 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
                 bs_reduce<M>(p);
             }
 #pragma unroll
-            for (int k = 0; k < M; k++) {
-                const uint32_t v = __reduce_xor_sync(FULL, p[k]);
-                if (lane == 0)
-                    sm.part[N & 1][warp][k] = v;
-            }
+            for (int k = 0; k < M; k++)
+                red[k] = __reduce_xor_sync(FULL, p[k]);
+            if (i <= ub)
+                bs_mul_acc<M>(q1, bb, C);
+            if (lane == 0)
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    sm.part[N & 1][warp][k] = red[k];
+        } else if (i <= ub) {
+            bs_mul_acc<M>(q1, bb, C);
         }
         __syncthreads();
         uint32_t d[M], mne = 0;
@@ -336,19 +350,17 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
         const uint32_t mle = __ballot_sync(FULL, my_mle);
         const int Lnew = my_mle ? N + 1 - Lq : Lq;
         const int Bdnew = min(min(my_mle ? Lq : Bd, T) + 1, T);
-        const int Lb = min(__reduce_max_sync(FULL, (unsigned)Lnew), (unsigned)T);
         int slot = i - N % R;
         slot = slot < 0 ? slot + R : slot;
         uint32_t *bp = sm.ring + slot * SS;
-        if (i <= Lb) {
-            uint32_t bv[M], q1[2 * M - 1];
-#pragma unroll
-            for (int k = 0; k < 2 * M - 1; k++)
-                q1[k] = 0;
+        // Coefficients up to the bound: C_i <- b*C_i + d*B_i (exactly zero
+        // above the new L), B_i takes the swap; above it C_i = 0, so B_i
+        // only takes the swap, where B can be nonzero.
+        if (i <= ub) {
+            uint32_t bv[M];
 #pragma unroll
             for (int k = 0; k < M; k++)
                 bv[k] = bp[k];
-            bs_mul_acc<M>(q1, bb, C);
             bs_mul_acc<M>(q1, d, bv);
             bs_reduce<M>(q1);
 #pragma unroll
@@ -370,8 +382,11 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
             bb[k] = (bb[k] & ~mle) | (d[k] & mle);
         Lq = Lnew;
         Bd = Bdnew;
-        Lmax = Lb;
-        // (slots past `count` never take the swap: their syndromes are zero)
+        // Maxima over the tile for the next step; slots past `count` never
+        // take the swap (their syndromes are zero), so they do not count.
+        Lmax = (int)__reduce_max_sync(FULL, (unsigned)Lnew);
+        const int nb = Lnew > N + 2 - Lnew ? Lnew : N + 2 - Lnew;
+        Lub = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)nb : 0u);
         Bmax = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)Bdnew : 0u);
     }
     __syncthreads();

@@ -650,6 +650,55 @@ void cmd_server::complete_loop()
     }
 }
 
+namespace {
+
+// Queues requests key_ids[i] / h_cts + i * ct_stride (results to h_err_base
+// + i * err_stride, or nowhere) under one lock, in order, until the queue is
+// full; arrival times t_arrive[i] (steady-clock ns), or now.  *accepted = how
+// many were queued; the rest are refused.
+int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8_t *h_cts, size_t ct_stride,
+                 uint8_t *h_err_base, size_t err_stride, const uint64_t *tags, const uint64_t *t_arrive,
+                 size_t *accepted)
+{
+    bool wake = false;
+    size_t k = 0;
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        if (srv->stop)
+            return CMD_E_ARG;
+        for (size_t i = 0; i < n; i++)
+            if (key_ids[i] >= srv->keys.size())
+                return CMD_E_ARG;
+        const size_t before = srv->pending.size();
+        const uint64_t now = t_arrive ? 0 : now_ns();
+        for (; k < n && srv->pending.size() < srv->cfg.queue_capacity; k++) {
+            Request r;
+            r.key_id = key_ids[k];
+            r.tag = tags ? tags[k] : k;
+            r.err_out = h_err_base ? h_err_base + k * err_stride : nullptr;
+            r.set = srv->keys[r.key_id].set;
+            const int ctb = set_info(r.set).ct;
+            memcpy(r.ct, h_cts + k * ct_stride, ctb);
+            memset(r.ct + ctb, 0, CT_STRIDE - ctb);
+            r.t_arrive = t_arrive ? t_arrive[k] : now;
+            if (srv->submitted++ == 0)
+                srv->t_first = r.t_arrive;
+            srv->pending.push_back(r);
+        }
+        srv->refused += n - k;
+        // The dispatcher waits for a first request or for a full batch: only
+        // those two transitions need a wake-up (not every submission).
+        const size_t np = srv->pending.size();
+        wake = k > 0 && (before == 0 || (before < srv->cfg.max_batch && np >= srv->cfg.max_batch));
+    }
+    if (wake)
+        srv->cv_dispatch.notify_one();
+    *accepted = k;
+    return CMD_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server **out)
@@ -774,37 +823,22 @@ int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uin
 {
     if (!srv || !h_ct)
         return CMD_E_ARG;
-    Request r;
-    r.key_id = key_id;
-    r.tag = tag;
-    r.err_out = h_err_out;
-    bool wake = false;
-    {
-        std::lock_guard<std::mutex> lk(srv->mu);
-        if (key_id >= srv->keys.size())
-            return CMD_E_ARG;
-        if (srv->stop)
-            return CMD_E_ARG;
-        if (srv->pending.size() >= srv->cfg.queue_capacity) {
-            srv->refused++;
-            return CMD_E_BUSY;
-        }
-        r.set = srv->keys[key_id].set;
-        const int ctb = set_info(r.set).ct;
-        memcpy(r.ct, h_ct, ctb);
-        memset(r.ct + ctb, 0, CT_STRIDE - ctb);
-        r.t_arrive = now_ns();
-        if (srv->submitted++ == 0)
-            srv->t_first = r.t_arrive;
-        srv->pending.push_back(r);
-        // The dispatcher waits for a first request or for a full batch: only
-        // those two transitions need a wake-up (not every submission).
-        const size_t np = srv->pending.size();
-        wake = np == 1 || np == srv->cfg.max_batch;
-    }
-    if (wake)
-        srv->cv_dispatch.notify_one();
-    return CMD_OK;
+    size_t accepted = 0;
+    const int rc = submit_group(srv, 1, &key_id, h_ct, 0, h_err_out, 0, &tag, nullptr, &accepted);
+    return rc ? rc : (accepted ? CMD_OK : CMD_E_BUSY);
+}
+
+int cmd_server_submit_many(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8_t *h_cts,
+                           size_t ct_stride, uint8_t *h_err_base, size_t err_stride, const uint64_t *tags,
+                           size_t *accepted)
+{
+    if (!srv || (n && (!key_ids || !h_cts || !ct_stride)) || (h_err_base && !err_stride))
+        return CMD_E_ARG;
+    size_t acc = 0;
+    const int rc = submit_group(srv, n, key_ids, h_cts, ct_stride, h_err_base, err_stride, tags, nullptr, &acc);
+    if (accepted)
+        *accepted = acc;
+    return rc ? rc : (acc == n ? CMD_OK : CMD_E_BUSY);
 }
 
 int cmd_server_poll(cmd_server *srv, cmd_completion *out, size_t max, size_t *n, uint32_t timeout_us)
@@ -897,10 +931,13 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
     return CMD_OK;
 }
 
-// Open-loop Poisson load: submits requests from a pool (request i uses key
-// key_ids[i % pool] and ciphertext i % pool; results land in err_pool rows)
-// at exponentially distributed inter-arrival times of mean 1/rate, for
-// `seconds`, then waits for every request to complete.
+// Open-loop Poisson load: request i uses key key_ids[i % pool] and
+// ciphertext i % pool, and its result lands in err_pool row i % pool.
+// Arrival times are a Poisson process of rate rate_per_s over `seconds`;
+// each request is queued with its scheduled arrival time, so latency counts
+// from when the request was due even if the generator queues it a little
+// later.  Every pass of the generator queues, under one lock, all requests
+// whose time has come.  Then it waits for every request to complete.
 int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *cts, size_t ct_stride,
                        uint8_t *err_pool, size_t err_stride, size_t pool, double rate_per_s, double seconds,
                        uint64_t seed, cmd_server_stats *out)
@@ -911,30 +948,54 @@ int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *
     cmd_server_stats_get(srv, &dummy, 1);
     std::mt19937_64 rng(seed);
     std::exponential_distribution<double> gap(rate_per_s);
+    constexpr size_t GROUP = 4096;
+    std::vector<uint32_t> g_key(GROUP);
+    std::vector<uint64_t> g_tag(GROUP), g_t(GROUP);
+    std::vector<uint8_t> g_ct(GROUP * CT_STRIDE);
+    std::vector<uint8_t *> g_err(GROUP);
     const uint64_t t0 = now_ns();
     const uint64_t t_end = t0 + (uint64_t)(seconds * 1e9);
-    double next = (double)t0;
+    double next = (double)t0 + gap(rng) * 1e9;
     size_t i = 0;
-    uint64_t busy = 0;
-    while (true) {
-        next += gap(rng) * 1e9;
-        if (next >= (double)t_end)
-            break;
-        while ((double)now_ns() < next) {
+    while (next < (double)t_end) {
+        const uint64_t now = now_ns();
+        if ((double)now < next)
+            continue;
+        // the requests due by now, queued together
+        size_t g = 0;
+        while (g < GROUP && next <= (double)now && next < (double)t_end) {
+            const size_t k = i % pool;
+            g_key[g] = key_ids[k];
+            g_tag[g] = i;
+            g_t[g] = (uint64_t)next;
+            memcpy(g_ct.data() + g * CT_STRIDE, cts + k * ct_stride, std::min<size_t>(ct_stride, CT_STRIDE));
+            g_err[g] = err_pool ? err_pool + k * err_stride : nullptr;
+            g++;
+            i++;
+            next += gap(rng) * 1e9;
         }
-        const size_t k = i % pool;
-        int rc = cmd_server_submit(srv, key_ids[k], cts + k * ct_stride, err_pool ? err_pool + k * err_stride : nullptr,
-                                   i);
-        if (rc == CMD_E_BUSY)
-            busy++;
-        else if (rc != CMD_OK)
-            return rc;
-        i++;
+        // one lock per group; outputs are scattered, so queue one by one
+        // inside it through the group call per request run of the pool
+        size_t acc = 0;
+        for (size_t a = 0; a < g;) {
+            // consecutive requests whose result rows are consecutive pool rows
+            size_t b = a + 1;
+            while (b < g && err_pool && g_err[b] == g_err[b - 1] + err_stride)
+                b++;
+            size_t got = 0;
+            const int rc = submit_group(srv, b - a, g_key.data() + a, g_ct.data() + a * CT_STRIDE, CT_STRIDE,
+                                        g_err[a], err_pool ? err_stride : 0, g_tag.data() + a, g_t.data() + a,
+                                        &got);
+            if (rc != CMD_OK)
+                return rc;
+            acc += got;
+            a = b;
+        }
+        (void)acc;
     }
     int rc = cmd_server_drain(srv, 60000);
     cmd_server_stats_get(srv, out, 0);
     out->offered_per_s = i / seconds;
-    (void)busy;
     return rc;
 }
 

@@ -285,7 +285,7 @@ typedef struct {
     int32_t status;      /* CMD_OK or the batch's error                   */
     uint16_t weight;     /* flagged positions                             */
     uint16_t reserved;
-    uint64_t latency_ns; /* submit -> result in the caller's buffer        */
+    uint64_t latency_ns; /* arrival -> result in the caller's buffer       */
 } cmd_completion;
 typedef struct {
     uint64_t submitted, completed, refused, batches, fused_batches, resident_keys;
@@ -310,6 +310,14 @@ int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t
  * CMD_E_BUSY when queue_capacity requests are waiting. */
 int cmd_server_submit(cmd_server *srv, uint32_t key_id, const uint8_t *h_ct, uint8_t *h_err_out,
                       uint64_t tag);
+/* Queues n requests under one lock, in order: request i is key_ids[i], the
+ * ciphertext at h_cts + i * ct_stride, its result (when h_err_base is not
+ * NULL) at h_err_base + i * err_stride, tag tags[i] (i when tags is NULL).
+ * *accepted = how many were queued before the queue filled; CMD_E_BUSY when
+ * that is fewer than n (the rest are refused and counted as such). */
+int cmd_server_submit_many(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8_t *h_cts,
+                           size_t ct_stride, uint8_t *h_err_base, size_t err_stride, const uint64_t *tags,
+                           size_t *accepted);
 /* Up to max completions (waits up to timeout_us for the first).  Returns the
  * server's sticky status (CMD_OK unless a batch failed). */
 int cmd_server_poll(cmd_server *srv, cmd_completion *out, size_t max, size_t *n, uint32_t timeout_us);
@@ -319,7 +327,9 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *out, int reset);
 /* Open-loop Poisson load for `seconds` at rate_per_s: request i uses
  * key_ids[i % pool] and ciphertext i % pool (ct_stride bytes apart) and writes
  * its result to err_pool row i % pool (err_stride bytes apart; may be NULL).
- * Statistics are reset first and returned in *out after a full drain. */
+ * Each request is queued with its scheduled arrival time, so its latency
+ * counts from when it was due; the generator queues all requests due at
+ * once.  Statistics are reset first and returned in *out after a full drain. */
 int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *cts, size_t ct_stride,
                        uint8_t *err_pool, size_t err_stride, size_t pool, double rate_per_s,
                        double seconds, uint64_t seed, cmd_server_stats *out);

@@ -121,6 +121,35 @@ def test_server_alone_equals_in_mix(engine, workload, fused_threshold):
         assert np.array_equal(a[:nb], expect[i])
 
 
+def test_server_submit_many(engine, workload):
+    """Requests queued in groups under one lock give the oracle's results,
+    with their tags, and a group larger than the queue is cut where it fills."""
+    ring, key_of, cts, expect = workload
+    n = cts.shape[0]
+    with cmd.Server(engine, max_batch=256, slots=3, max_wait_us=100, fused_threshold=0) as srv:
+        ids = np.array([srv.add_key(s, sk) for s, sk in ring], np.uint32)
+        outs = np.zeros((n, 1024), np.uint8)
+        for a in range(0, n, 300):
+            b = min(n, a + 300)
+            assert srv.submit_many(ids[key_of[a:b]], cts[a:b], outs[a:b], np.arange(a, b) + 7) == b - a
+        srv.drain()
+        comps = srv.poll(max_n=n + 10)
+        assert sorted(c[0] for c in comps) == list(range(7, n + 7))
+    for i in range(n):
+        s, _ = ring[key_of[i]]
+        nb = cmd.set_info(s).err_bytes
+        assert np.array_equal(outs[i, :nb], expect[i]), i
+    with cmd.Server(engine, max_batch=64, slots=1, max_wait_us=100000, queue_capacity=50,
+                    fused_threshold=0) as srv:
+        ids = np.array([srv.add_key(s, sk) for s, sk in ring], np.uint32)
+        # a first request keeps the one slot busy so that the group waits in the queue
+        assert srv.submit_many(ids[key_of[:1]], cts[:1], None) == 1
+        got = srv.submit_many(ids[key_of[:200]], cts[:200], None)
+        assert 0 < got <= 50
+        srv.drain()
+        assert srv.stats()["refused"] >= 200 - got
+
+
 def test_server_lru_eviction_under_budget(workload):
     ring, key_of, cts, expect = workload
     with cmd.Engine(0) as probe:
