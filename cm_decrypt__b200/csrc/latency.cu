@@ -332,17 +332,24 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
 #pragma unroll
         for (int k = 0; k < M; k++)
             d[k] = 0;
-        for (int w = 0; 32 * w <= lim; w++) {
-            const uint4 *pr = reinterpret_cast<const uint4 *>(sm.part[N & 1][w]);
+        // every warp's shares at once (independent loads; warps past `lim`
+        // contribute nothing this step)
+        uint4 xs[BM_WARPS][(M + 3) / 4];
+#pragma unroll
+        for (int w = 0; w < BM_WARPS; w++)
+#pragma unroll
+            for (int v = 0; v < (M + 3) / 4; v++)
+                xs[w][v] = 32 * w <= lim ? reinterpret_cast<const uint4 *>(sm.part[N & 1][w])[v]
+                                         : make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int w = 0; w < BM_WARPS; w++)
 #pragma unroll
             for (int v = 0; v < (M + 3) / 4; v++) {
-                const uint4 x = pr[v];
-                if (4 * v + 0 < M) d[4 * v + 0] ^= x.x;
-                if (4 * v + 1 < M) d[4 * v + 1] ^= x.y;
-                if (4 * v + 2 < M) d[4 * v + 2] ^= x.z;
-                if (4 * v + 3 < M) d[4 * v + 3] ^= x.w;
+                if (4 * v + 0 < M) d[4 * v + 0] ^= xs[w][v].x;
+                if (4 * v + 1 < M) d[4 * v + 1] ^= xs[w][v].y;
+                if (4 * v + 2 < M) d[4 * v + 2] ^= xs[w][v].z;
+                if (4 * v + 3 < M) d[4 * v + 3] ^= xs[w][v].w;
             }
-        }
 #pragma unroll
         for (int k = 0; k < M; k++)
             mne |= d[k];

@@ -112,26 +112,31 @@ template <int S> __global__ void __launch_bounds__(256) k_bm_plain(const uint16_
     }
     uint32_t b = 1, L = 0;
     for (int N = 0; N < 2 * T; N++) {
-        const int lim = N < T ? N : T;
+        // deg C <= L: coefficients above L are zero and add nothing to the
+        // discrepancy (bm.c sums i <= min(N, t); the terms above L vanish)
+        const int lim = min(N < T ? N : T, (int)L);
         uint32_t part = 0;
 #pragma unroll
         for (int j = 0; j < NJ; j++) {
             const int i = lane + 32 * j;
-            if (i <= lim)
+            if (32 * j <= lim && i <= lim)
                 part ^= gf_mul<M>(C[j], s[N - i]);
         }
         const uint32_t d = __reduce_xor_sync(FULL, part);
         const uint32_t mne = 0u - (uint32_t)(d != 0);
         const uint32_t mle = mne & (0u - (uint32_t)((uint32_t)N >= 2 * L));
         const uint32_t f = gf_frac<M>(b, d);
+        const uint32_t Ln = (L & ~mle) | ((N + 1 - L) & mle);
+        const int ub = min((int)Ln, T);  // the new C is zero above the new L
         uint32_t sel[NJ];
 #pragma unroll
         for (int j = 0; j < NJ; j++) {
             const uint32_t oc = C[j];
-            C[j] ^= gf_mul<M>(f, B[j]) & mne;
+            if (32 * j <= ub)
+                C[j] ^= gf_mul<M>(f, B[j]) & mne;
             sel[j] = (B[j] & ~mle) | (oc & mle);
         }
-        L = (L & ~mle) | ((N + 1 - L) & mle);
+        L = Ln;
         b = (b & ~mle) | (d & mle);
         uint32_t up[NJ];
 #pragma unroll

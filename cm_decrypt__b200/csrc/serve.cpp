@@ -11,8 +11,10 @@
 //    are admitted as soon as a slot frees, and the batches overlap on the
 //    device (copies and kernels of different slots run concurrently).
 //  * Expanded keys stay resident in HBM; a key is expanded on first use and
-//    the least recently used unpinned keys are evicted when the engine's HBM
-//    budget is full (admission by budget).
+//    the least recently used keys that no batch in flight uses are evicted
+//    when the engine's HBM budget is full (admission by budget).  Every batch
+//    stamps its keys with its generation; a key is in use while a batch of
+//    that generation or later is in flight.
 //  * Small batches run the latency kernels of latency.cu (any mix of keys and
 //    sets in three launches, a short pass per ciphertext); batches of
 //    fused_threshold or more run the fused kernel (highest throughput).
@@ -22,8 +24,10 @@
 //    arrival-to-completion latency for the p50/p99 statistics.
 //  * Host work per request is O(1): the queue is a vector whose buffers
 //    circulate between the queue and the slots (no allocation per request),
-//    keys get a batch-local index by generation stamp, and requests are
-//    grouped by set and key with a counting sort.
+//    keys are marked once per batch by generation stamp, and the tile path
+//    groups requests by set in one counting pass; only the ciphertexts and
+//    the tile items are copied to the device.  Requests can be queued in
+//    groups under one lock (cmd_server_submit_many).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -108,7 +112,6 @@ struct KeyEntry {
     std::vector<uint8_t> sk;
     cmd_key *key = nullptr;
     uint64_t last_use = 0;
-    int pins = 0;
     uint64_t batch_gen = 0;  // dispatcher only: generation of the batch that last indexed this key
     uint32_t batch_idx = 0;  // index within that batch's key table
 };
@@ -200,7 +203,7 @@ struct Slot {
     size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
     std::vector<Request> reqs;  // taken from the queue (a buffer swap when a batch takes it all)
-    std::vector<uint32_t> pinned;  // key ids pinned by this batch
+    uint64_t gen = 0;          // generation of the batch in this slot (its keys carry it)
     bool fused = false;
     // completer scratch, reused batch to batch
     std::vector<uint32_t> lats, waits;
@@ -245,7 +248,7 @@ struct cmd_server {
 
     void dispatch_loop();
     void complete_loop();
-    int ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys);
+    int ensure_key(uint32_t id);
     int launch(Slot &sl);
 };
 
@@ -278,7 +281,7 @@ struct InLayout {
 
 }  // namespace
 
-int cmd_server::ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys)
+int cmd_server::ensure_key(uint32_t id)
 {
     KeyEntry &ke = keys[id];
     ke.last_use = ++tick;
@@ -289,20 +292,24 @@ int cmd_server::ensure_key(uint32_t id, std::vector<uint32_t> &batch_keys)
         if (rc != CMD_E_BUDGET)
             return rc;
         // Evict the least recently used resident key that no batch in flight
-        // and not this batch uses.
+        // and not this batch uses: its generation stamp is older than every
+        // batch in flight and than this one.
+        uint64_t oldest = batch_gen;  // this batch's generation
+        const uint32_t fl = inflight.load();
+        for (size_t si = 0; si < slots.size(); si++)
+            if ((fl >> si) & 1u)
+                oldest = std::min(oldest, slots[si].gen);
         int victim = -1;
-        bool held = false;  // some resident key is pinned by a batch in flight
+        bool held = false;  // some resident key is in use by a batch in flight
         {
             std::lock_guard<std::mutex> lk(mu);
             for (size_t k = 0; k < keys.size(); k++) {
                 if (!keys[k].key || k == id)
                     continue;
-                if (keys[k].pins > 0) {
-                    held = true;
+                if (keys[k].batch_gen >= oldest) {
+                    held = held || keys[k].batch_gen < batch_gen;
                     continue;
                 }
-                if (std::find(batch_keys.begin(), batch_keys.end(), (uint32_t)k) != batch_keys.end())
-                    continue;
                 if (victim < 0 || keys[k].last_use < keys[victim].last_use)
                     victim = (int)k;
             }
@@ -336,51 +343,29 @@ int cmd_server::launch(Slot &sl)
     }
     std::vector<uint32_t> ready;
     for (uint32_t k : kid) {
-        int rc = ensure_key(k, ready);
+        int rc = ensure_key(k);
         if ((rc == CMD_E_BUDGET || rc == CMD_E_BUSY) && !ready.empty())
             break;
         if (rc)
             return rc;
         ready.push_back(k);
     }
-    {
+    if (ready.size() < kid.size()) {
         std::lock_guard<std::mutex> lk(mu);
+        gen = ++batch_gen;  // re-stamp: only the ready keys stay in this batch
         for (uint32_t k : ready)
-            keys[k].pins++;
-        if (ready.size() < kid.size()) {
-            gen = ++batch_gen;  // re-stamp: only the ready keys stay in this batch
-            for (uint32_t k : ready)
-                keys[k].batch_gen = gen;
-            std::vector<Request> keep, defer;
-            for (const Request &r : sl.reqs)
-                (keys[r.key_id].batch_gen == gen ? keep : defer).push_back(r);
-            pending.push_front(defer.begin(), defer.end());
-            sl.reqs.swap(keep);
-        }
+            keys[k].batch_gen = gen;
+        std::vector<Request> keep, defer;
+        for (const Request &r : sl.reqs)
+            (keys[r.key_id].batch_gen == gen ? keep : defer).push_back(r);
+        pending.push_front(defer.begin(), defer.end());
+        sl.reqs.swap(keep);
     }
-    sl.pinned = ready;
-    // Key table in set order, so that grouping requests by key index also
-    // groups them by set.
-    kid = ready;
-    std::stable_sort(kid.begin(), kid.end(), [&](uint32_t a, uint32_t b) { return keys[a].set < keys[b].set; });
-    for (size_t k = 0; k < kid.size(); k++)
-        keys[kid[k]].batch_idx = (uint32_t)k;
+    sl.gen = gen;  // the batch's keys stay in use while it is in flight
     const size_t B = sl.reqs.size();
     InLayout lay(B, B);
-    uint32_t *key_idx = reinterpret_cast<uint32_t *>(sl.h_in + lay.key_idx);
-    for (size_t i = 0; i < B; i++) {
-        key_idx[i] = keys[sl.reqs[i].key_id].batch_idx;
+    for (size_t i = 0; i < B; i++)
         memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
-    }
-    FusedKeyRef *krefs = reinterpret_cast<FusedKeyRef *>(sl.h_in + lay.keys);
-    std::vector<int> kset(kid.size());
-    std::vector<const uint32_t *> kwfft(kid.size());
-    for (size_t k = 0; k < kid.size(); k++) {
-        const cmd_key *key = keys[kid[k]].key;
-        krefs[k] = key_ref(key->dev);
-        kset[k] = key->dev.set;
-        kwfft[k] = key->dev.wfft;
-    }
     LaunchCounter lc{&eng->launches};
     cudaStream_t s = sl.stream;
     cudaError_t e;
@@ -390,44 +375,39 @@ int cmd_server::launch(Slot &sl)
     sl.fused = cfg.fused_threshold > 0 && B >= cfg.fused_threshold;
     sl.slot_of.resize(B);
     if (!sl.fused) {
-        // Tile path: requests grouped by set into tiles of up to 32 (any keys
-        // within a tile); item slot 32*t + q is request q of tile t.
+        // Tile path: requests grouped by set (a counting pass over the five
+        // sets) into tiles of up to 32, any keys within a tile; item slot
+        // 32*t + q is request q of tile t.  Only the ciphertexts and the
+        // items go to the device.
         LatItem *items = reinterpret_cast<LatItem *>(sl.h_in + lay.items);
-        // by set, then by key (counting sort on the set-ordered key index):
-        // requests of one key sit side by side, so their syndrome CTAs read
-        // the same table rows close together in time
-        std::vector<uint32_t> by_set(B), start(kid.size() + 1, 0);
+        uint32_t cnt[NSETS] = {}, tile0[NSETS], next[NSETS] = {};
         for (size_t i = 0; i < B; i++)
-            start[key_idx[i] + 1]++;
-        for (size_t k = 0; k < kid.size(); k++)
-            start[k + 1] += start[k];
-        for (size_t i = 0; i < B; i++)
-            by_set[start[key_idx[i]]++] = (uint32_t)i;
+            cnt[sl.reqs[i].set]++;
         uint32_t ntiles = 0;
-        size_t i = 0;
-        while (i < B) {
-            const int set = kset[key_idx[by_set[i]]];
-            size_t j = i;
-            while (j < B && kset[key_idx[by_set[j]]] == set && j - i < 32)
-                j++;
-            const uint32_t cnt = (uint32_t)(j - i);
-            for (uint32_t q = 0; q < 32; q++) {
-                const uint32_t slot = 32 * ntiles + q;
-                if (q < cnt) {
-                    const uint32_t r = by_set[i + q];
-                    const FusedKeyRef &kr = krefs[key_idx[r]];
-                    items[slot] = LatItem{kwfft[key_idx[r]], kr.bctl, (uint32_t)(r * CT_STRIDE), slot * ERR_STRIDE,
-                                          kr.set, cnt};
-                    sl.slot_of[r] = slot;
-                } else {
-                    items[slot] = LatItem{kwfft[0], krefs[0].bctl, 0, slot * ERR_STRIDE, -1, cnt};
-                }
-            }
-            ntiles++;
-            i = j;
+        for (int st = 0; st < NSETS; st++) {
+            tile0[st] = ntiles;
+            ntiles += (cnt[st] + 31) / 32;
         }
+        for (size_t i = 0; i < B; i++) {
+            const Request &r = sl.reqs[i];
+            const uint32_t pos = next[r.set]++;
+            const uint32_t slot = 32 * (tile0[r.set] + pos / 32) + pos % 32;
+            const uint32_t left = cnt[r.set] - pos / 32 * 32;
+            const KeyDev &kd = keys[r.key_id].key->dev;
+            items[slot] = LatItem{kd.wfft, kd.bctl, (uint32_t)(i * CT_STRIDE), slot * ERR_STRIDE, r.set,
+                                  (int32_t)(left < 32 ? left : 32)};
+            sl.slot_of[i] = slot;
+        }
+        for (int st = 0; st < NSETS; st++)
+            for (uint32_t pos = cnt[st]; pos % 32; pos++) {  // the set's last tile, past its count
+                const uint32_t slot = 32 * (tile0[st] + pos / 32) + pos % 32;
+                items[slot] = LatItem{nullptr, nullptr, 0, slot * ERR_STRIDE, -1, (int32_t)(cnt[st] % 32)};
+            }
         sl.rows_used = (size_t)ntiles * 32;
-        if ((e = cudaMemcpyAsync(sl.d_in, sl.h_in, lay.total, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        if ((e = cudaMemcpyAsync(sl.d_in + lay.cts, sl.h_in + lay.cts, B * CT_STRIDE, cudaMemcpyHostToDevice, s)) !=
+                cudaSuccess ||
+            (e = cudaMemcpyAsync(sl.d_in + lay.items, sl.h_in + lay.items, sl.rows_used * sizeof(LatItem),
+                                 cudaMemcpyHostToDevice, s)) != cudaSuccess)
             return cuda_fail(e, "server H2D");
         FftPlans plans;
         for (int st = 0; st < NSETS; st++)
@@ -436,6 +416,22 @@ int cmd_server::launch(Slot &sl)
         if (e != cudaSuccess)
             return cuda_fail(e, "server tile-path launch");
     } else {
+        // Fused path: a key table in set order, so that grouping requests by
+        // key index also groups them by set.
+        kid = ready;
+        std::stable_sort(kid.begin(), kid.end(), [&](uint32_t a, uint32_t b) { return keys[a].set < keys[b].set; });
+        for (size_t k = 0; k < kid.size(); k++)
+            keys[kid[k]].batch_idx = (uint32_t)k;
+        uint32_t *key_idx = reinterpret_cast<uint32_t *>(sl.h_in + lay.key_idx);
+        for (size_t i = 0; i < B; i++)
+            key_idx[i] = keys[sl.reqs[i].key_id].batch_idx;
+        FusedKeyRef *krefs = reinterpret_cast<FusedKeyRef *>(sl.h_in + lay.keys);
+        std::vector<int> kset(kid.size());
+        for (size_t k = 0; k < kid.size(); k++) {
+            const cmd_key *key = keys[kid[k]].key;
+            krefs[k] = key_ref(key->dev);
+            kset[k] = key->dev.set;
+        }
         uint64_t *ct_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.ct_off);
         uint64_t *err_off = reinterpret_cast<uint64_t *>(sl.h_in + lay.err_off);
         for (size_t i = 0; i < B; i++) {
@@ -538,9 +534,6 @@ void cmd_server::dispatch_loop()
                     completions.push_back(cmd_completion{r.tag, rc, 0, 0, t - r.t_arrive});
                 completed++;
             }
-            for (uint32_t k : sl.pinned)
-                keys[k].pins--;
-            sl.pinned.clear();
             sl.reqs.clear();
             free_slots.push_back(si);
             if (status == CMD_OK)
@@ -638,9 +631,6 @@ void cmd_server::complete_loop()
         completed += B;
         t_last = t;
         complete_ns += t_done - t;
-        for (uint32_t k : sl.pinned)
-            keys[k].pins--;
-        sl.pinned.clear();
         sl.reqs.clear();
         inflight.fetch_and(~(1u << si));
         free_slots.push_back(si);

@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import shutil
 import subprocess
 
 import numpy as np
@@ -50,6 +51,8 @@ def build(with_reference: bool | None = None, ref_dir: str | None = None) -> Non
         raise FileNotFoundError("the reference tree: pass ref_dir or set CMD_REFERENCE_DIR")
     if with_reference or (with_reference is None and have):
         targets.append("ref")
+        if shutil.which("nvcc") or os.path.exists("/usr/local/cuda/bin/nvcc"):
+            targets.append("gpu_optimised")  # the reference's GPU_Optimised decoder, sm_100a
     subprocess.run(["make", "-s", "-C", HERE, f"REF={ref_dir}", *targets], check=True)
 
 
