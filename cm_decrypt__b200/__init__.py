@@ -138,6 +138,7 @@ def lib() -> ctypes.CDLL:
         "cmd_tune": (_i32, [_vp, _vp, _sz, _i32]),
         "cmd_engine_fused_config": (_i32, [_vp, _i32, ctypes.POINTER(_i32), ctypes.POINTER(_i32),
                                            ctypes.POINTER(ctypes.c_double)]),
+        "cmd_engine_tile_below": (_i32, [_vp, _i32, ctypes.POINTER(ctypes.c_uint32)]),
         "cmd_engine_set_fused_config": (_i32, [_vp, _i32, _i32, _i32]),
         "cmd_graph_capture": (_i32, [_vp, _vp, _i32, _vp, _sz, _vp, _vp, ctypes.POINTER(_vp)]),
         "cmd_graph_launch": (_i32, [_vp, _vp]),
@@ -319,7 +320,9 @@ def fused_config(engine: Engine, set_id: int) -> dict:
     wpb, bal, ns = _i32(), _i32(), ctypes.c_double()
     _check(lib().cmd_engine_fused_config(engine.handle, set_index(set_id), ctypes.byref(wpb), ctypes.byref(bal),
                                          ctypes.byref(ns)), "cmd_engine_fused_config")
-    return {"wpb": wpb.value, "balanced": bool(bal.value), "ns_per_ct": ns.value}
+    tb = ctypes.c_uint32()
+    _check(lib().cmd_engine_tile_below(engine.handle, set_index(set_id), ctypes.byref(tb)), "cmd_engine_tile_below")
+    return {"wpb": wpb.value, "balanced": bool(bal.value), "ns_per_ct": ns.value, "tile_below": tb.value}
 
 
 def set_fused_config(engine: Engine, set_id: int, wpb: int, balanced: bool = True) -> None:

@@ -238,7 +238,8 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
         return CMD_E_ARG;
     }
     const size_t bytes = carve_size({(size_t)si.n * 2, (size_t)(si.t + 1) * 2, (size_t)si.n * 2,
-                                     (size_t)si.sb * si.twp() * 4, (size_t)si.m * si.nw * 4,
+                                     (size_t)si.sb * si.twp() * 4, (size_t)si.sb * si.twd() * 4,
+                                     (size_t)si.m * si.nw * 4,
                                      benes_mask_words(si) * 4, fft_weight_words(si) * 4, (size_t)si.sk});
     if (!budget_take(eng, bytes)) {
         set_last_error("key does not fit the engine HBM budget");
@@ -264,6 +265,7 @@ int cmd_key_expand(cmd_engine *eng, cmd_set set, const uint8_t *h_sk, size_t sk_
     key->dev.g = cv.take<uint16_t>(si.t + 1);
     key->dev.ginv2 = cv.take<uint16_t>(si.n);
     key->dev.tab = cv.take<uint32_t>((size_t)si.sb * si.twp());
+    key->dev.tabd = cv.take<uint32_t>((size_t)si.sb * si.twd());
     key->dev.Lbs = cv.take<uint32_t>((size_t)si.m * si.nw);
     key->dev.bctl = cv.take<uint32_t>(benes_mask_words(si));
     key->dev.wfft = cv.take<uint32_t>(fft_weight_words(si));
@@ -468,7 +470,7 @@ int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t
         return CMD_OK;
     if (path == CMD_PATH_PLAIN)
         return run_plain(eng, key, d_cts, count, d_err, d_weight, s);
-    if (path == CMD_PATH_TILE)
+    if (path == CMD_PATH_TILE || (path == CMD_PATH_AUTO && count < eng->fcfg[key->dev.set].tile_below))
         return run_tile(eng, key, d_cts, count, d_err, d_weight, nullptr, s);
     return run_fused_single(eng, key, d_cts, count, d_err, d_weight, s);
 }

@@ -37,6 +37,11 @@ struct FusedConfig {
     bool balanced = true; // equal-share rounds (see round_size in batch.cu)
     bool tuned = false;
     double ns_per_ct = 0; // measured by the tuner
+    uint32_t tile_below = 0;  // CMD_PATH_AUTO: batches smaller than this take
+                              // the tile kernels (five warps per 32-ciphertext
+                              // tile for Berlekamp-Massey, one warp per
+                              // ciphertext for the FFTs) instead of the fused
+                              // kernel (one warp per tile); 0 = never
 };
 
 int cuda_fail(cudaError_t e, const char *what);
@@ -78,7 +83,7 @@ int upload_fft_plans(cmd_engine *eng);
 // cmd_decrypt_plain_noalloc itself loads and allocates nothing.
 int noalloc_setup(int device);
 void release_fft_plans(cmd_engine *eng);
-inline FusedKeyRef key_ref(const KeyDev &k) { return FusedKeyRef{k.set, 0, k.tab, k.Lbs, k.bctl}; }
+inline FusedKeyRef key_ref(const KeyDev &k) { return FusedKeyRef{k.set, 0, k.tabd, k.Lbs, k.bctl}; }
 
 }  // namespace cmd
 

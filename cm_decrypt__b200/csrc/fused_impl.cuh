@@ -9,10 +9,11 @@
 //
 //  1. stage its 32 ciphertexts in shared memory (128-bit loads when the round
 //     is one aligned slab);
-//  2. syndrome (util.c:102-114): lane q accumulates the packed 2t syndromes
-//     of ciphertext q; the key's syndrome table streams through shared memory
-//     in 16-row chunks (cp.async double buffer, shared by all warps) and each
-//     row is masked by the ciphertext bit, never branched on;
+//  2. syndrome (util.c:102-114): lane q accumulates the 2t syndromes of
+//     ciphertext q, m bits each back to back; the key's dense syndrome table
+//     streams through shared memory in 16-row chunks (cp.async double
+//     buffer, shared by all warps) and each row is masked by the ciphertext
+//     bit, never branched on;
 //  3. ballot-transpose the syndromes to bitsliced form (bit q = ciphertext q);
 //  4. Berlekamp-Massey (bm.c:12-68) bitsliced across the 32 ciphertexts: lane
 //     l owns locator coefficients l, l+32, ... (kept in shared memory, so the
@@ -56,7 +57,7 @@ __host__ __device__ constexpr int al16(int x) { return (x + 15) / 16 * 16; }
 template <int S> struct Fz {
     using P = Set<S>;
     static constexpr int M = P::M, T = P::T, NJ = (T + 1 + 31) / 32;
-    static constexpr int TWP = (T + 3) / 4 * 4;      // padded table row (words)
+    static constexpr int TWD = P::TWD;               // dense table row (words)
     static constexpr int RING = T + 2;               // B ring slots
     static constexpr int NX = FftDims<S>::NX;        // radix-conversion entries
     static constexpr int RAW_B = 32 * P::CT;
@@ -66,7 +67,7 @@ template <int S> struct Fz {
     static constexpr int A_B = al16(cmax(cmax(RAW_B + 16, RING_B + CM_B), FA_B));
     static constexpr int S_B = al16(2 * T * M * 4);  // bitsliced syndromes / locator
     static constexpr int WARP_B = A_B + S_B;
-    static constexpr int TAB_B = TAB_ROWS * TWP * 4;  // one chunk buffer
+    static constexpr int TAB_B = TAB_ROWS * TWD * 4;  // one chunk buffer
     static_assert(NX * M * 4 <= S_B, "conversion array must fit the syndrome region");
 };
 
@@ -108,7 +109,7 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
 {
     using Z = Fz<S>;
     using P = Set<S>;
-    constexpr int M = Z::M, T = Z::T, TWP = Z::TWP, NW = P::NW;
+    constexpr int M = Z::M, T = Z::T, TWD = Z::TWD, NW = P::NW;
     const FusedArgs &a = *rc.a;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int rem = (int)rc.tile.count - warp * 32;
@@ -148,12 +149,17 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     __syncwarp();
 
     // ---- 2. syndrome -----------------------------------------------------
-    uint32_t acc[T];
+    // The key's dense table: row b holds the 2t values L_b^j / g(L_b)^2 as m
+    // bits each, back to back (bit j*m + k = bit k of value j), so lane q's
+    // accumulator word w holds bits 32w .. 32w+31 of ciphertext q's 2t*m
+    // syndrome bits.
+    constexpr int NWU = (2 * T * M + 31) / 32;  // accumulator words in use
+    uint32_t acc[NWU];
 #pragma unroll
-    for (int w = 0; w < T; w++)
+    for (int w = 0; w < NWU; w++)
         acc[w] = 0;
     constexpr int NCHUNK = P::SB / TAB_ROWS;
-    constexpr int CHUNK_V = TAB_ROWS * TWP / 4;  // 16-byte pieces per chunk
+    constexpr int CHUNK_V = TAB_ROWS * TWD / 4;  // 16-byte pieces per chunk
     {
         const uint32_t *src = tab;
         for (int v = tid; v < CHUNK_V; v += WPB * 32)
@@ -164,8 +170,8 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     uint32_t ctw = 0;
     for (int c = 0; c < NCHUNK; c++) {
         if (c + 1 < NCHUNK) {
-            const uint32_t *src = tab + (size_t)(c + 1) * TAB_ROWS * TWP;
-            uint32_t *dst = tabbuf + ((c + 1) & 1) * TAB_ROWS * TWP;
+            const uint32_t *src = tab + (size_t)(c + 1) * TAB_ROWS * TWD;
+            uint32_t *dst = tabbuf + ((c + 1) & 1) * TAB_ROWS * TWD;
             for (int v = tid; v < CHUNK_V; v += WPB * 32)
                 cp_async16(dst + 4 * v, src + 4 * v);
             cp_async_commit();
@@ -174,21 +180,21 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
             cp_async_wait<0>();
         }
         __syncthreads();
-        const uint32_t *buf = tabbuf + (c & 1) * TAB_ROWS * TWP;
+        const uint32_t *buf = tabbuf + (c & 1) * TAB_ROWS * TWD;
 #pragma unroll 1
         for (int r = 0; r < TAB_ROWS; r++) {
             const int b = c * TAB_ROWS + r;
             if ((b & 31) == 0)
                 ctw = ld_u32_any(myct + (b >> 3));
             const uint32_t mask = (uint32_t)((int32_t)(ctw << (31 - (b & 31))) >> 31);
-            const uint4 *row = reinterpret_cast<const uint4 *>(buf + r * TWP);
+            const uint4 *row = reinterpret_cast<const uint4 *>(buf + r * TWD);
 #pragma unroll
-            for (int v = 0; v < TWP / 4; v++) {
+            for (int v = 0; v < TWD / 4; v++) {
                 const uint4 x = row[v];
-                if (4 * v + 0 < T) acc[4 * v + 0] ^= x.x & mask;
-                if (4 * v + 1 < T) acc[4 * v + 1] ^= x.y & mask;
-                if (4 * v + 2 < T) acc[4 * v + 2] ^= x.z & mask;
-                if (4 * v + 3 < T) acc[4 * v + 3] ^= x.w & mask;
+                if (4 * v + 0 < NWU) acc[4 * v + 0] ^= x.x & mask;
+                if (4 * v + 1 < NWU) acc[4 * v + 1] ^= x.y & mask;
+                if (4 * v + 2 < NWU) acc[4 * v + 2] ^= x.z & mask;
+                if (4 * v + 3 < NWU) acc[4 * v + 3] ^= x.w & mask;
             }
         }
         __syncthreads();
@@ -197,18 +203,18 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
         return;  // no work for this warp in this round (the CTA-wide part is done)
 
     // ---- 3. transpose: sS[j*M + k] bit q = bit k of syndrome j of ct q ----
+    // Syndrome bit x = j*M + k is bit x mod 32 of accumulator word x / 32: one
+    // ballot per bit, lane l keeps the ballot of bit l of the word.
 #pragma unroll
-    for (int w = 0; w < T; w++) {
+    for (int w = 0; w < NWU; w++) {
+        uint32_t mine = 0;
 #pragma unroll 1
-        for (int h = 0; h < 2; h++) {
-            const int j = 2 * w + h;
-#pragma unroll
-            for (int k = 0; k < M; k++) {
-                const uint32_t v = __ballot_sync(FULLMASK, (acc[w] >> (16 * h + k)) & 1u);
-                if (lane == ((j * M + k) & 31))
-                    sS[j * M + k] = v;
-            }
+        for (int b = 0; b < 32; b++) {
+            const uint32_t v = __ballot_sync(FULLMASK, (acc[w] >> b) & 1u);
+            mine = lane == b ? v : mine;
         }
+        if (32 * w + lane < 2 * T * M)
+            sS[32 * w + lane] = mine;
     }
     __syncwarp();
 

@@ -23,6 +23,9 @@ struct KeyDev {
                                 // 4) words; word w < t of row b packs
                                 // L_b^{2w}/g^2 (low) and L_b^{2w+1}/g^2 (high):
                                 // util.c:86-100 values, rows 16-byte aligned
+    uint32_t *tabd = nullptr;   // the same table, dense: sb rows of twd words,
+                                // bit j*m + k of row b = bit k of L_b^j/g^2
+                                // (the fused kernel's syndrome source)
     uint32_t *Lbs = nullptr;    // bitsliced support, plane-major [m][nw]:
                                 // bit p of Lbs[k*nw+w] = bit k of L[32w+p]
     uint32_t *bctl = nullptr;   // Benes network as swap masks, [2m-1][2^(m-5)]:

@@ -56,8 +56,9 @@ template <int S> __global__ void __launch_bounds__(1024) k_support(KeyDev k)
 
 // Per support point: g(L_i) by Horner (root_13.c:216-230), 1/g(L_i)^2, and for
 // i < sb the syndrome-table row L_i^j / g(L_i)^2, j < 2t (util.c:86-100),
-// packed two coefficients per 32-bit word.  Multiplies by integer multiplies
-// on operands with holes (gf_mul_im).
+// packed two coefficients per 32-bit word (tab) and densely, m bits per
+// coefficient (tabd).  Multiplies by integer multiplies on operands with holes
+// (gf_mul_im).
 template <int S> __global__ void __launch_bounds__(256) k_key_tables(KeyDev k)
 {
     using P = Set<S>;
@@ -78,15 +79,32 @@ template <int S> __global__ void __launch_bounds__(256) k_key_tables(KeyDev k)
     if (i < P::SB) {
         uint32_t x = inv;
         uint32_t *row = k.tab + (size_t)i * P::TWP;
+        uint32_t *drow = k.tabd + (size_t)i * P::TWD;
         for (int w = P::TW; w < P::TWP; w++)
             row[w] = 0;
+        // dense row: the 2t values' m bits back to back, little-endian
+        uint64_t acc = 0;
+        int nb = 0, dw = 0;
         for (int w = 0; w < P::TW; w++) {
             const uint32_t lo = x;
             x = gf_mul_im<M>(x, a);
             const uint32_t hi = x;
             x = gf_mul_im<M>(x, a);
             row[w] = lo | (hi << 16);
+            acc |= (uint64_t)lo << nb;
+            nb += M;
+            acc |= (uint64_t)hi << nb;
+            nb += M;
+            while (nb >= 32) {
+                drow[dw++] = (uint32_t)acc;
+                acc >>= 32;
+                nb -= 32;
+            }
         }
+        if (nb > 0)
+            drow[dw++] = (uint32_t)acc;
+        for (; dw < P::TWD; dw++)
+            drow[dw] = 0;
     }
 }
 

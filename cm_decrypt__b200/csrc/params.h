@@ -40,6 +40,7 @@ constexpr CMD_HD int synd_depth(int t) { return fft_depth(2 * t - 1); }
         static constexpr int NW = (N_ + 31) / 32;       /* error words per ct   */     \
         static constexpr int TW = T_;                   /* 2t u16 = t u32 words */     \
         static constexpr int TWP = (T_ + 3) / 4 * 4;    /* table row stride     */     \
+        static constexpr int TWD = (2 * T_ * M_ + 127) / 128 * 4; /* dense row    */     \
         static constexpr int COND = (1 << (M_ - 4)) * (2 * M_ - 1);                    \
         static constexpr int CTW = (CT_ + 3) / 4;       /* ct as u32 words      */     \
     };
@@ -53,6 +54,7 @@ CMD_DEFINE_SET(S8192128, 8192128, 13, 8192, 128, 208, 14120)
 struct SetInfo {
     int id, m, n, t, ct, sk, sb, nw, cond;
     CMD_HD int twp() const { return (t + 3) / 4 * 4; }  // syndrome-table row stride (words)
+    CMD_HD int twd() const { return (2 * t * m + 127) / 128 * 4; }  // dense-table row stride (words)
 };
 
 CMD_HD inline SetInfo set_info(int s)

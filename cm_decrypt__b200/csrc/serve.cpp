@@ -13,8 +13,8 @@
 //  * Expanded keys stay resident in HBM; a key is expanded on first use and
 //    the least recently used keys that no batch in flight uses are evicted
 //    when the engine's HBM budget is full (admission by budget).  Every batch
-//    stamps its keys with its generation; a key is in use while a batch of
-//    that generation or later is in flight.
+//    stamps the keys it made resident with its generation; a key is in use
+//    while a batch of that generation or later is in flight.
 //  * Small batches run the latency kernels of latency.cu (any mix of keys and
 //    sets in three launches, a short pass per ciphertext); batches of
 //    fused_threshold or more run the fused kernel (highest throughput).
@@ -112,7 +112,8 @@ struct KeyEntry {
     std::vector<uint8_t> sk;
     cmd_key *key = nullptr;
     uint64_t last_use = 0;
-    uint64_t batch_gen = 0;  // dispatcher only: generation of the batch that last indexed this key
+    uint64_t seen_gen = 0;   // dispatcher only: the batch that last listed this key
+    uint64_t batch_gen = 0;  // generation of the last batch this key was made resident for
     uint32_t batch_idx = 0;  // index within that batch's key table
 };
 
@@ -336,11 +337,13 @@ int cmd_server::launch(Slot &sl)
     uint64_t gen = ++batch_gen;
     for (const Request &r : sl.reqs) {
         KeyEntry &ke = keys[r.key_id];
-        if (ke.batch_gen != gen) {
-            ke.batch_gen = gen;
+        if (ke.seen_gen != gen) {
+            ke.seen_gen = gen;
             kid.push_back(r.key_id);
         }
     }
+    // A key made resident for this batch carries its generation, which keeps
+    // it from being evicted for the batch's later keys.
     std::vector<uint32_t> ready;
     for (uint32_t k : kid) {
         int rc = ensure_key(k);
@@ -348,6 +351,7 @@ int cmd_server::launch(Slot &sl)
             break;
         if (rc)
             return rc;
+        keys[k].batch_gen = gen;
         ready.push_back(k);
     }
     if (ready.size() < kid.size()) {

@@ -2,7 +2,10 @@
 //
 // Tuner: for one parameter set on one GPU it times the candidate launch
 // configurations (warps per CTA x round schedule) on a device batch and keeps
-// the fastest.  The decrypt kernels' instruction stream does not depend on
+// the fastest; then it times the fastest against the tile kernels (five warps
+// per 32-ciphertext tile for Berlekamp-Massey instead of one) at growing batch
+// sizes and records the size from which the fused kernel wins, below which
+// CMD_PATH_AUTO takes the tile kernels.  The decrypt kernels' instruction stream does not depend on
 // the ciphertext contents, so the sample is a constant byte pattern.  Choices
 // are cached per engine and persisted as JSON keyed by (GPU name, set) in
 // $CMD_TUNE_CACHE (default ~/.cache/cmd_b200/tune.json).
@@ -35,7 +38,9 @@ static std::string cache_path()
     return std::string(home ? home : "/tmp") + "/.cache/cmd_b200/tune.json";
 }
 
-// Minimal reader/writer for {"key": {"wpb": n, "balanced": b, "ns_per_ct": x}, ...}.
+// Minimal reader/writer for
+// {"key": {"wpb": n, "balanced": b, "ns_per_ct": x, "tile_below": c}, ...};
+// an entry without tile_below (an older tuner's) is tuned again.
 static std::map<std::string, FusedConfig> load_cache()
 {
     std::map<std::string, FusedConfig> out;
@@ -66,7 +71,10 @@ static std::map<std::string, FusedConfig> load_cache()
         const char *w = strstr(body.c_str(), "\"wpb\":");
         const char *b = strstr(body.c_str(), "\"balanced\":");
         const char *t = strstr(body.c_str(), "\"ns_per_ct\":");
-        if (w && sscanf(w + 6, "%d", &wpb) == 1 && (wpb == 4 || wpb == 8)) {
+        const char *tb = strstr(body.c_str(), "\"tile_below\":");
+        unsigned tbv = 0;
+        if (w && tb && sscanf(tb + 13, "%u", &tbv) == 1 && sscanf(w + 6, "%d", &wpb) == 1 && (wpb == 4 || wpb == 8)) {
+            c.tile_below = tbv;
             c.wpb = wpb;
             if (b)
                 sscanf(b + 11, "%d", &bal);
@@ -96,8 +104,9 @@ static void save_cache(const std::map<std::string, FusedConfig> &m)
     fprintf(f, "{\n");
     size_t i = 0;
     for (const auto &kv : m) {
-        fprintf(f, "  \"%s\": {\"wpb\": %d, \"balanced\": %d, \"ns_per_ct\": %.3f}%s\n", kv.first.c_str(),
-                kv.second.wpb, kv.second.balanced ? 1 : 0, kv.second.ns_per_ct, ++i < m.size() ? "," : "");
+        fprintf(f, "  \"%s\": {\"wpb\": %d, \"balanced\": %d, \"ns_per_ct\": %.3f, \"tile_below\": %u}%s\n",
+                kv.first.c_str(), kv.second.wpb, kv.second.balanced ? 1 : 0, kv.second.ns_per_ct,
+                kv.second.tile_below, ++i < m.size() ? "," : "");
     }
     fprintf(f, "}\n");
     fclose(f);
@@ -133,6 +142,14 @@ int cmd_engine_fused_config(cmd_engine *eng, cmd_set set, int *wpb, int *balance
         *balanced = c.balanced ? 1 : 0;
     if (ns_per_ct)
         *ns_per_ct = c.ns_per_ct;
+    return CMD_OK;
+}
+
+int cmd_engine_tile_below(cmd_engine *eng, cmd_set set, uint32_t *tile_below)
+{
+    if (!eng || !valid_set(set) || !tile_below)
+        return CMD_E_ARG;
+    *tile_below = eng->fcfg[set].tile_below;
     return CMD_OK;
 }
 
@@ -218,13 +235,48 @@ int cmd_tune(cmd_engine *eng, const cmd_key *key, size_t sample_count, int force
             }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
     if (best_ns >= 1e30) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
         eng->fcfg[set] = saved;
         set_last_error("tuner: no candidate configuration ran");
         return CMD_E_CUDA;
     }
+    eng->fcfg[set] = best;
+    // Fused kernel (one warp per tile) against the tile kernels at growing
+    // batch sizes: the tile kernels finish small batches sooner (their
+    // Berlekamp-Massey runs on five warps, their FFTs on a warp per
+    // ciphertext), the fused kernel does less work per ciphertext.
+    best.tile_below = 0;
+    const size_t sizes[] = {256, 1024, 4096, 16384, 65536};
+    for (size_t n : sizes) {
+        if (n > sample_count)
+            break;
+        auto timed = [&](bool tile) -> double {
+            float total = 0;
+            for (int rep = 0; rep < 3; rep++) {
+                cudaEventRecord(e0, s);
+                const int r = tile ? run_device(eng, key, CMD_PATH_TILE, d_cts, n, d_err, nullptr, s)
+                                   : run_fused_counter(eng, key, d_cts, n, d_err, nullptr, s, eng->tile_counter,
+                                                       nullptr, -1);
+                cudaEventRecord(e1, s);
+                if (r != CMD_OK || cudaEventSynchronize(e1) != cudaSuccess)
+                    return 1e30;
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (rep > 0)
+                    total += ms;
+            }
+            return total / 2;
+        };
+        const double tf = timed(false), tt = timed(true);
+        if (tt < tf)
+            best.tile_below = (uint32_t)(2 * n);  // the tile kernels still win here
+        else
+            break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
     best.tuned = true;
     best.ns_per_ct = best_ns;
     eng->fcfg[set] = best;

@@ -359,12 +359,18 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
 /* ---- fused-kernel tuning and graph replay (no reference counterpart) --- */
 /* Picks the fused kernel's launch configuration for key's set on this GPU
  * (warps per CTA 4|8, equal-share or full rounds) by timing the candidates on
- * sample_count ciphertexts (0 = about three waves).  Results are cached in the
- * engine and in $CMD_TUNE_CACHE (JSON keyed by GPU name and set); a cached
- * entry is reused unless force != 0. */
+ * sample_count ciphertexts (0 = about three waves), then the batch size below
+ * which CMD_PATH_AUTO takes the tile kernels instead (five warps per
+ * 32-ciphertext tile for Berlekamp-Massey rather than the fused kernel's
+ * one), from timings of both at 256 .. 65,536 ciphertexts.  Results are
+ * cached in the engine and in $CMD_TUNE_CACHE (JSON keyed by GPU name and
+ * set); a cached entry is reused unless force != 0. */
 int cmd_tune(cmd_engine *eng, const cmd_key *key, size_t sample_count, int force);
 int cmd_engine_fused_config(cmd_engine *eng, cmd_set set, int *wpb, int *balanced,
                             double *ns_per_ct);
+/* The tuned batch size below which CMD_PATH_AUTO runs the tile kernels (0:
+ * never). */
+int cmd_engine_tile_below(cmd_engine *eng, cmd_set set, uint32_t *tile_below);
 int cmd_engine_set_fused_config(cmd_engine *eng, cmd_set set, int wpb, int balanced);
 
 /* A decrypt over fixed device buffers captured as a CUDA graph and replayed

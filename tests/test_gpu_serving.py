@@ -26,9 +26,18 @@ def test_tune_and_graph_replay(engine):
         cfg = cmd.tune(engine, key, force=True)
         assert cfg["wpb"] in (4, 8) and cfg["ns_per_ct"] > 0
         cached = cmd.tune(engine, key)  # served from the cache
-        assert (cached["wpb"], cached["balanced"]) == (cfg["wpb"], cfg["balanced"])
+        assert (cached["wpb"], cached["balanced"], cached["tile_below"]) == \
+            (cfg["wpb"], cfg["balanced"], cfg["tile_below"])
         assert cached["ns_per_ct"] == pytest.approx(cfg["ns_per_ct"], rel=1e-3)
+        # the tuned crossover: small batches take the tile kernels under
+        # CMD_PATH_AUTO (the tile path wins on a batch of a few tiles)
+        assert cfg["tile_below"] >= 512
         pk = cmd.PubKey(s, golden_sk(s))
+        small, small_e, _ = pk.ciphertexts(seed=8, count=100, malformed_permille=100)
+        launches = engine.launch_count()
+        err, _ = cmd.decrypt(engine, key, small, path="auto")
+        assert engine.launch_count() - launches == 4  # tile items + the three tile kernels
+        assert np.array_equal(err, cmd.decrypt(engine, key, small, path="fused")[0])
         cts, planted, _ = pk.ciphertexts(seed=4, count=5000)
         d_ct = torch.from_numpy(cts).cuda()
         for path in ("fused", "plain"):
