@@ -110,7 +110,10 @@ template <int S> __global__ void __launch_bounds__(256) k_bm_plain(const uint16_
         C[j] = (i == 0);
         B[j] = (i == 1);
     }
-    uint32_t b = 1, L = 0;
+    // f = d/b = d * b^-1 (gf_frac's value): b changes only when L does, so
+    // b^-1 is kept and inverted again only then, off the next discrepancy's
+    // path (bm.c recomputes gf_frac(b, d) every step).
+    uint32_t b = 1, binv = 1, L = 0;
     for (int N = 0; N < 2 * T; N++) {
         // deg C <= L: coefficients above L are zero and add nothing to the
         // discrepancy (bm.c sums i <= min(N, t); the terms above L vanish)
@@ -125,7 +128,7 @@ template <int S> __global__ void __launch_bounds__(256) k_bm_plain(const uint16_
         const uint32_t d = __reduce_xor_sync(FULL, part);
         const uint32_t mne = 0u - (uint32_t)(d != 0);
         const uint32_t mle = mne & (0u - (uint32_t)((uint32_t)N >= 2 * L));
-        const uint32_t f = gf_frac<M>(b, d);
+        const uint32_t f = gf_mul<M>(d, binv);
         const uint32_t Ln = (L & ~mle) | ((N + 1 - L) & mle);
         const int ub = min((int)Ln, T);  // the new C is zero above the new L
         uint32_t sel[NJ];
@@ -138,6 +141,8 @@ template <int S> __global__ void __launch_bounds__(256) k_bm_plain(const uint16_
         }
         L = Ln;
         b = (b & ~mle) | (d & mle);
+        if (mle)  // the same for the whole warp: one ciphertext
+            binv = gf_inv<M>(d);
         uint32_t up[NJ];
 #pragma unroll
         for (int j = 0; j < NJ; j++)

@@ -211,6 +211,54 @@ struct Slot {
     std::vector<cmd_completion> comps;
 };
 
+// Latency histogram with no allocation after construction: 1 us buckets up to
+// 20 ms, 100 us buckets up to 2 s, one overflow bucket.  Quantiles are exact
+// to the bucket (1 us below 20 ms); the maximum and the sum are kept exactly.
+class LatencyHist {
+public:
+    LatencyHist() : fine_(FINE, 0), coarse_(COARSE + 1, 0) {}
+    void add(uint64_t ns)
+    {
+        const uint64_t us = ns / 1000;
+        if (us < FINE)
+            fine_[us]++;
+        else
+            coarse_[std::min<uint64_t>((us - FINE) / 100, COARSE)]++;
+        n_++;
+        sum_ += ns;
+        max_ = std::max(max_, ns);
+    }
+    void clear()
+    {
+        std::fill(fine_.begin(), fine_.end(), 0);
+        std::fill(coarse_.begin(), coarse_.end(), 0);
+        n_ = sum_ = max_ = 0;
+    }
+    uint64_t count() const { return n_; }
+    double mean_us() const { return n_ ? sum_ / 1e3 / n_ : 0; }
+    double max_us() const { return max_ / 1e3; }
+    // the bucket holding the sample of rank f * (n - 1), as its lower edge in us
+    double quantile_us(double f) const
+    {
+        if (!n_)
+            return 0;
+        const uint64_t rank = (uint64_t)(f * (n_ - 1));
+        uint64_t seen = 0;
+        for (uint64_t b = 0; b < FINE; b++)
+            if ((seen += fine_[b]) > rank)
+                return (double)b;
+        for (uint64_t b = 0; b <= COARSE; b++)
+            if ((seen += coarse_[b]) > rank)
+                return (double)(FINE + 100 * b);
+        return max_us();
+    }
+
+private:
+    static constexpr uint64_t FINE = 20000, COARSE = 19800;
+    std::vector<uint64_t> fine_, coarse_;
+    uint64_t n_ = 0, sum_ = 0, max_ = 0;
+};
+
 }  // namespace cmd
 
 using namespace cmd;
@@ -238,9 +286,9 @@ struct cmd_server {
     int status = CMD_OK;
     uint64_t batch_gen = 0;  // dispatcher only
     // statistics
-    std::vector<uint32_t> lat_ns;
-    std::vector<uint32_t> gpu_ns;   // per batch
-    std::vector<uint32_t> wait_ns;  // per request: arrival -> launch
+    LatencyHist lat;   // per request: arrival -> result delivered
+    LatencyHist gpu;   // per batch: device time, input copy to result copy
+    LatencyHist wait;  // per request: arrival -> batch launch
     uint64_t submitted = 0, completed = 0, refused = 0, batches = 0, fused_batches = 0, batched_cts = 0;
     uint64_t t_first = 0, t_last = 0;
     uint64_t dispatch_ns = 0, complete_ns = 0, inflight_sum = 0;  // host time in launch / result handling
@@ -629,9 +677,11 @@ void cmd_server::complete_loop()
         }
         if (cfg.record_completions)
             completions.insert(completions.end(), sl.comps.begin(), sl.comps.end());
-        lat_ns.insert(lat_ns.end(), sl.lats.begin(), sl.lats.end());
-        wait_ns.insert(wait_ns.end(), sl.waits.begin(), sl.waits.end());
-        gpu_ns.push_back((uint32_t)(gpu_ms * 1e6f));
+        for (size_t i = 0; i < B; i++) {
+            lat.add(sl.lats[i]);
+            wait.add(sl.waits[i]);
+        }
+        gpu.add((uint64_t)(gpu_ms * 1e6f));
         completed += B;
         t_last = t;
         complete_ns += t_done - t;
@@ -879,31 +929,15 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
     st->resident_keys = 0;
     for (const auto &k : srv->keys)
         st->resident_keys += k.key != nullptr;
-    auto quantile = [](std::vector<uint32_t> v, double f) {
-        if (v.empty())
-            return 0.0;
-        size_t i = (size_t)(f * (v.size() - 1));
-        std::nth_element(v.begin(), v.begin() + i, v.end());
-        return v[i] / 1e3;
-    };
-    st->gpu_p50_us = quantile(srv->gpu_ns, 0.50);
-    st->gpu_p99_us = quantile(srv->gpu_ns, 0.99);
-    st->wait_p50_us = quantile(srv->wait_ns, 0.50);
-    st->wait_p99_us = quantile(srv->wait_ns, 0.99);
-    if (!srv->lat_ns.empty()) {
-        std::vector<uint32_t> v = srv->lat_ns;
-        auto q = [&](double f) {
-            size_t i = (size_t)(f * (v.size() - 1));
-            std::nth_element(v.begin(), v.begin() + i, v.end());
-            return v[i] / 1e3;
-        };
-        st->p50_us = q(0.50);
-        st->p99_us = q(0.99);
-        st->max_us = *std::max_element(v.begin(), v.end()) / 1e3;
-        double sum = 0;
-        for (uint32_t x : v)
-            sum += x;
-        st->mean_us = sum / v.size() / 1e3;
+    st->gpu_p50_us = srv->gpu.quantile_us(0.50);
+    st->gpu_p99_us = srv->gpu.quantile_us(0.99);
+    st->wait_p50_us = srv->wait.quantile_us(0.50);
+    st->wait_p99_us = srv->wait.quantile_us(0.99);
+    if (srv->lat.count()) {
+        st->p50_us = srv->lat.quantile_us(0.50);
+        st->p99_us = srv->lat.quantile_us(0.99);
+        st->max_us = srv->lat.max_us();
+        st->mean_us = srv->lat.mean_us();
     }
     if (srv->t_last > srv->t_first) {
         const double span = (double)(srv->t_last - srv->t_first);
@@ -913,9 +947,9 @@ int cmd_server_stats_get(cmd_server *srv, cmd_server_stats *st, int reset)
     }
     st->mean_inflight = srv->batches ? (double)srv->inflight_sum / srv->batches : 0;
     if (reset) {
-        srv->lat_ns.clear();
-        srv->gpu_ns.clear();
-        srv->wait_ns.clear();
+        srv->lat.clear();
+        srv->gpu.clear();
+        srv->wait.clear();
         srv->submitted -= srv->completed;
         srv->completed = 0;
         srv->refused = srv->batches = srv->fused_batches = srv->batched_cts = 0;
