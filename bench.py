@@ -66,6 +66,8 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--keygen-only", action="store_true",
                     help="run only the key-generation leg and print its JSON (for profiling)")
     ap.add_argument("--keygen-count", type=int, default=64, help="seeds in the key-generation batch")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own GPU_Optimised decoder (oracle/_ref)")
     ap.add_argument("--no-reference-check", action="store_true",
                     help="skip comparing every mixed-batch and serving row with the reference CPU decoder")
     ap.add_argument("--no-configs", action="store_true",
@@ -234,6 +236,49 @@ def serving_leg(cmd, eng, nkeys: int, rates: list[float], seconds: float, pool: 
             out["points"].append(pt)
     under = [p for p in out["points"] if p["p99_ms"] < 1.0]
     out["max_decaps_per_s_p99_under_1ms"] = max((p["decaps_per_s"] for p in under), default=None)
+    return out
+
+
+def reference_gpu_leg(cmd, eng, key, stream) -> dict:
+    """The reference's own GPU_Optimised decoder (its sources built for sm_100a
+    by oracle/Makefile, run by oracle/run_gpu_optimised.py) on 50,000
+    mceliece6960119 ciphertexts, its per-stage times beside this engine's
+    per-stage kernels and fused kernel on a batch of the same size and key."""
+    import torch
+    from oracle import run_gpu_optimised as rgo
+    if not rgo.available():
+        return {"unavailable": "oracle/_ref GPU_Optimised build missing (make -C oracle gpu_optimised)"}
+    ref = rgo.run(env={"CUDA_MODULE_LOADING": "EAGER"})  # no module load inside its first stage's timing
+    out = {"reference": {k: ref.get(k) for k in ("synd_ms", "bm_ms", "chien_ms", "kernel_ms", "kernel_decaps_per_s",
+                                                 "h2d_ms", "d2h_ms", "errorstream_matches", "rc")},
+           "ciphertexts": rgo.COUNT,
+           "timing": "reference: its own wall-clock stage times (kernel + synchronise, CUDA_MODULE_LOADING=EAGER); "
+                     "ours: CUDA events per kernel on the same batch size"}
+    _, cts, errs = rgo.make_inputs(rgo.COUNT)
+    n, info = rgo.COUNT, key.info
+    d_ct = torch.from_numpy(cts).cuda()
+    d_s = torch.zeros((n, 2 * info.t), dtype=torch.int16, device="cuda")
+    d_l = torch.zeros((n, info.t + 1), dtype=torch.int16, device="cuda")
+    d_e = torch.zeros((n, info.err_words), dtype=torch.int32, device="cuda")
+    d_w = torch.zeros(n, dtype=torch.int16, device="cuda")
+    sp = stream.cuda_stream
+    ours = {"synd_ms": _time_stream(lambda: cmd.synd(eng, key, d_ct.data_ptr(), n, d_s.data_ptr(), sp), stream, 3, 1),
+            "bm_ms": _time_stream(lambda: cmd.bm(eng, SET, d_s.data_ptr(), n, d_l.data_ptr(), sp), stream, 3, 1),
+            "root_ms": _time_stream(lambda: cmd.root(eng, key, d_l.data_ptr(), n, d_e.data_ptr(), d_w.data_ptr(), sp),
+                                    stream, 3, 1)}
+    plain_ok = bool(np.array_equal(d_e.cpu().numpy().astype("<u4").view(np.uint8).reshape(n, -1)[:, :info.err_bytes],
+                                   errs))
+    ours["fused_ms"] = _time_stream(lambda: cmd.decrypt_device(eng, key, d_ct.data_ptr(), n, d_e.data_ptr(),
+                                                               d_w.data_ptr(), sp, "fused"), stream, 3, 1)
+    fused_ok = bool(np.array_equal(d_e.cpu().numpy().astype("<u4").view(np.uint8).reshape(n, -1)[:, :info.err_bytes],
+                                   errs))
+    ours["results_match_planted"] = plain_ok and fused_ok
+    out["ours"] = ours
+    r = out["reference"]
+    if r.get("synd_ms"):
+        out["speedup"] = {"synd": r["synd_ms"] / ours["synd_ms"], "bm": r["bm_ms"] / ours["bm_ms"],
+                          "root": r["chien_ms"] / ours["root_ms"], "fused_vs_reference_kernels": r["kernel_ms"] /
+                          ours["fused_ms"]}
     return out
 
 
@@ -731,6 +776,8 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(sk, cts)
+    if world == 1 and not args.no_reference_gpu:
+        line["reference_gpu"] = reference_gpu_leg(cmd, eng, key, stream)
     if world == 1 and not args.no_configs:
         line["configs"] = {"all_sets_2^20": config_all_sets(cmd, eng, stream),
                            "mixed_64keys_2^18": config_mixed(cmd, eng, stream,

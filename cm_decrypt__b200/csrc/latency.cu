@@ -217,12 +217,8 @@ __global__ void __launch_bounds__(TS_WARPS * 32) k_tile_tsynd(const LatItem *__r
     }
 }
 
-// Threads of k_tile_bm: coefficient warps, thread i of which owns locator
-// coefficient i (t+1 <= 129), and as many helper warps, helper c forming the
-// products b*C_i of coefficient warp c's coefficients.  Helper c is warp
-// BM_CWARPS + c, so that it issues from another scheduler than warp c.
-constexpr int BM_CWARPS = 5;
-constexpr int BM_WARPS = 2 * BM_CWARPS;
+// Threads of k_tile_bm: thread i owns locator coefficient i (t+1 <= 129).
+constexpr int BM_WARPS = 5;
 constexpr int BM_THREADS = BM_WARPS * 32;
 
 template <int S> struct TileSmem {
@@ -230,19 +226,8 @@ template <int S> struct TileSmem {
     static constexpr int SS = Z::M | 1;  // odd plane stride: per-coefficient rows meet no bank conflicts
     uint32_t sx[Z::NS * SS];             // group sums -> syndromes -> converted locators
     uint32_t ring[(Z::T + 2) * SS];      // B, rotated one slot per step (the x*B shift)
-    uint32_t cs[BM_CWARPS * 32 * SS];    // C after each step, for the helpers
-    uint32_t bc[BM_CWARPS * 32 * SS];    // b*C from the helpers, for the update
-    alignas(16) uint32_t part[2][BM_CWARPS][16];  // per-warp discrepancy shares, by step parity
+    alignas(16) uint32_t part[2][BM_WARPS][16];  // per-warp discrepancy shares, by step parity
 };
-
-__device__ __forceinline__ void bar_arrive(int id, int threads)
-{
-    asm volatile("bar.arrive %0, %1;\n" ::"r"(id), "r"(threads) : "memory");
-}
-__device__ __forceinline__ void bar_sync(int id, int threads)
-{
-    asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(threads) : "memory");
-}
 
 // Steps 1-2 of k_tile_bm, by the whole CTA: gather the tile's group sums
 // (sx[s][k] bit q = plane k of sum s of ciphertext q; zero for q >= count),
@@ -278,7 +263,7 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
     using Z = TsDims<S>;
     using Sm = TileSmem<S>;
     constexpr int M = Z::M, T = Z::T, NS = Z::NS, SS = Sm::SS, R = T + 2;
-    static_assert(T + 1 <= BM_CWARPS * 32, "one coefficient thread per locator coefficient");
+    static_assert(T + 1 <= BM_THREADS, "one thread per locator coefficient");
     Sm &sm = *reinterpret_cast<Sm *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -288,23 +273,14 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
     tile_syndromes<S>(count, tile_scratch, sm, scalpow);
 
     // ---- 3. scaled Berlekamp-Massey, thread i owns C_i -------------------
-    // Per step N, coefficient warp c (thread i = 32c + lane):
-    //   (1) if some coefficient of the warp is <= min(N, t, max L): its
-    //       shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp;
-    //   barrier;
-    //   (2) the shares summed (d, per ciphertext); every warp derives the same
-    //       decisions; for i up to a bound on the new L: C_i <- b*C_i + d*B_i
-    //       (b*C_i from the helper), B_i <- (N >= 2L and d != 0) ? old C_i :
-    //       B_i in the ring slot of coefficient i; above it, up to the
-    //       largest possible degree of B, B_i only takes the swap (C_i = 0);
-    //   (3) the new C_i to shared memory, then an arrival at named barrier
-    //       1 + c.
-    // Helper c: waits at named barrier 1 + c for the new C, forms b*C_i for
-    // the same coefficients while warp c forms the discrepancy shares, and
-    // follows the decisions after the barrier.
-    const bool helper = warp >= BM_CWARPS;
-    const int cw = helper ? warp - BM_CWARPS : warp;  // the coefficient warp served
-    const int i = 32 * cw + lane;
+    // Per step: (1) warps holding coefficients i <= min(N, t, max L) form
+    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp;
+    // barrier; (2) every thread sums the shares (d, per ciphertext), every
+    // warp derives the same decisions, and the owners of i <= new max L form
+    // C_i <- b*C_i + d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in
+    // the ring slot of coefficient i.  Ring entries above that, up to the
+    // largest possible degree of B, only take the swap (C_i = 0 there).
+    const int i = tid;
     uint32_t C[M], bb[M];
 #pragma unroll
     for (int k = 0; k < M; k++) {
@@ -313,34 +289,10 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
     }
     int Lq = 0, Bd = 1;    // lane q: L and a bound on deg B of ciphertext q
     int Lmax = 0, Bmax = 1;
-    int Lub = 1;           // bound on every ciphertext's L after this step
-    if (!helper) {
-#pragma unroll
-        for (int k = 0; k < M; k++)
-            sm.cs[i * SS + k] = C[k];
-        bar_arrive(1 + cw, 64);
-    }
 #pragma unroll 1
     for (int N = 0; N < 2 * T; N++) {
         const int lim = min(N, min(T, Lmax));
-        const int ub = min(Lub, T);
-        if (helper) {
-            bar_sync(1 + cw, 64);  // C of coefficient warp cw after step N-1
-            if (32 * cw <= ub) {
-                uint32_t cv[M], q[2 * M - 1];
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    cv[k] = sm.cs[i * SS + k];
-#pragma unroll
-                for (int k = 0; k < 2 * M - 1; k++)
-                    q[k] = 0;
-                bs_mul_acc<M>(q, bb, cv);
-                bs_reduce<M>(q);
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    sm.bc[i * SS + k] = q[k];
-            }
-        } else if (32 * cw <= lim) {
+        if (32 * warp <= lim) {
             uint32_t p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
@@ -358,7 +310,7 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
             for (int k = 0; k < M; k++) {
                 const uint32_t v = __reduce_xor_sync(FULL, p[k]);
                 if (lane == 0)
-                    sm.part[N & 1][cw][k] = v;
+                    sm.part[N & 1][warp][k] = v;
             }
         }
         __syncthreads();
@@ -368,15 +320,15 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
 #pragma unroll
         for (int k = 0; k < M; k++)
             d[k] = 0;
-        uint4 xs[BM_CWARPS][(M + 3) / 4];
+        uint4 xs[BM_WARPS][(M + 3) / 4];
 #pragma unroll
-        for (int w = 0; w < BM_CWARPS; w++)
+        for (int w = 0; w < BM_WARPS; w++)
 #pragma unroll
             for (int v = 0; v < (M + 3) / 4; v++)
                 xs[w][v] = 32 * w <= lim ? reinterpret_cast<const uint4 *>(sm.part[N & 1][w])[v]
                                          : make_uint4(0, 0, 0, 0);
 #pragma unroll
-        for (int w = 0; w < BM_CWARPS; w++)
+        for (int w = 0; w < BM_WARPS; w++)
 #pragma unroll
             for (int v = 0; v < (M + 3) / 4; v++) {
                 if (4 * v + 0 < M) d[4 * v + 0] ^= xs[w][v].x;
@@ -391,58 +343,51 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
         const uint32_t mle = __ballot_sync(FULL, my_mle);
         const int Lnew = my_mle ? N + 1 - Lq : Lq;
         const int Bdnew = min(min(my_mle ? Lq : Bd, T) + 1, T);
-        if (!helper) {
-            int slot = i - N % R;
-            slot = slot < 0 ? slot + R : slot;
-            uint32_t *bp = sm.ring + slot * SS;
-            if (i <= ub) {
-                uint32_t bv[M], q1[2 * M - 1];
+        const int Lb = min(__reduce_max_sync(FULL, (unsigned)Lnew), (unsigned)T);
+        int slot = i - N % R;
+        slot = slot < 0 ? slot + R : slot;
+        uint32_t *bp = sm.ring + slot * SS;
+        if (i <= Lb) {
+            uint32_t bv[M], q1[2 * M - 1];
 #pragma unroll
-                for (int k = 0; k < M; k++)
-                    bv[k] = bp[k];
+            for (int k = 0; k < 2 * M - 1; k++)
+                q1[k] = 0;
 #pragma unroll
-                for (int k = 0; k < 2 * M - 1; k++)
-                    q1[k] = 0;
-                bs_mul_acc<M>(q1, d, bv);
-                bs_reduce<M>(q1);
+            for (int k = 0; k < M; k++)
+                bv[k] = bp[k];
+            bs_mul_acc<M>(q1, bb, C);
+            bs_mul_acc<M>(q1, d, bv);
+            bs_reduce<M>(q1);
 #pragma unroll
-                for (int k = 0; k < M; k++) {
-                    bp[k] = (bv[k] & ~mle) | (C[k] & mle);
-                    C[k] = q1[k] ^ sm.bc[i * SS + k];
-                    sm.cs[i * SS + k] = C[k];
-                }
-            } else if (i <= min(Bmax, T)) {
-#pragma unroll
-                for (int k = 0; k < M; k++)
-                    bp[k] &= ~mle;
+            for (int k = 0; k < M; k++) {
+                bp[k] = (bv[k] & ~mle) | (C[k] & mle);
+                C[k] = q1[k];
             }
-            // the slot that becomes coefficient 0 of x*B at step N+1
-            const int freeslot = (R - (N + 1) % R) % R;
-            if (tid < M)
-                sm.ring[freeslot * SS + tid] = 0;
-            bar_arrive(1 + cw, 64);
+        } else if (i <= min(Bmax, T)) {
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bp[k] &= ~mle;
         }
+        // the slot that becomes coefficient 0 of x*B at step N+1
+        const int freeslot = (R - (N + 1) % R) % R;
+        if (tid < M)
+            sm.ring[freeslot * SS + tid] = 0;
 #pragma unroll
         for (int k = 0; k < M; k++)
             bb[k] = (bb[k] & ~mle) | (d[k] & mle);
         Lq = Lnew;
         Bd = Bdnew;
-        // Maxima over the tile for the next step; slots past `count` never
-        // take the swap (their syndromes are zero), so they do not count.
-        Lmax = (int)__reduce_max_sync(FULL, (unsigned)Lnew);
-        const int nb = Lnew > N + 2 - Lnew ? Lnew : N + 2 - Lnew;
-        Lub = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)nb : 0u);
+        Lmax = Lb;
+        // (slots past `count` never take the swap: their syndromes are zero)
         Bmax = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)Bdnew : 0u);
     }
-    if (helper)
-        bar_sync(1 + cw, 64);  // the coefficient warp's last arrival
     __syncthreads();
     // ---- 4. radix conversion of the reversed locators, out ---------------
     // Entry x of the conversion array is C[T-x] (bm.c:62-65 reverses the
     // locator before root() evaluates it), zero for T < x < 2^D.
     using F = FftDims<S>;
     static_assert(F::NX <= NS && F::NX * 16 <= TILE_LOC_WORDS, "conversion array size");
-    if (!helper && i <= T)
+    if (i <= T)
 #pragma unroll
         for (int k = 0; k < M; k++)
             sm.sx[(T - i) * SS + k] = C[k];

@@ -8,8 +8,11 @@ so every figure below is bit operations / 32 ("lane-ops").
 Work of the algorithm the fused kernel executes, per decryption:
 
   W_synd = sb * 2t * m / 32                      masked XOR of table rows
-  W_bm   = [sum_{N<2t} (min(N,t)+1) + 2t(t+1) + 8*2t] * (m^2 + R_m) / 32
-           (discrepancies, C updates, d/b counted as 8 multiplies)
+  W_bm   = [sum_{N<2t} (min(N, t, L_N) + 1) + 2 sum_{N<2t} (min(L_{N+1}, t) + 1)]
+           * (m^2 + R_m) / 32
+           (the scaled, L-bounded Berlekamp-Massey: discrepancy terms up to
+           the current L, then b*C_i + d*B_i for the coefficients up to the
+           new L; L_N = floor((N+1)/2), the trajectory of a weight-t error)
   W_root = additive FFT at all 2^m field elements, D = ceil(log2(t+1)):
            [ (D-1) 2^D (m^2+R_m)                   radix-conversion scalings
            + 2^(D-2) m D(D-1)                      Taylor-expansion XORs
@@ -47,8 +50,9 @@ def work_per_decap(set_id: int) -> dict:
     mul = m * m + r
     sb = 8 * ct
     w_synd = sb * 2 * t * m / 32
-    disc = sum(min(N, t) + 1 for N in range(2 * t))
-    w_bm = (disc + 2 * t * (t + 1) + 8 * 2 * t) * mul / 32
+    disc = sum(min(N, t, (N + 1) // 2) + 1 for N in range(2 * t))
+    upd = sum(min((N + 2) // 2, t) + 1 for N in range(2 * t))
+    w_bm = (disc + 2 * upd) * mul / 32
     D = fft_depth(t)
     w_root = ((D - 1) * (1 << D) * mul + (1 << (D - 2)) * m * D * (D - 1)
               + D * (1 << (m - 1)) * (mul + 2 * m) + (1 << m) * m + (2 * m - 1) * (1 << (m - 1)) * 3) / 32
