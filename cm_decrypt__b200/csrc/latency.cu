@@ -226,7 +226,7 @@ template <int S> struct TileSmem {
     static constexpr int SS = Z::M | 1;  // odd plane stride: per-coefficient rows meet no bank conflicts
     uint32_t sx[Z::NS * SS];             // group sums -> syndromes -> converted locators
     uint32_t ring[(Z::T + 2) * SS];      // B, rotated one slot per step (the x*B shift)
-    alignas(16) uint32_t part[2][BM_WARPS][16];  // per-warp discrepancy shares, by step parity
+    alignas(16) uint32_t dsum[3][16];  // the discrepancy, summed by the warps' atomic XORs (step mod 3)
 };
 
 // Steps 1-2 of k_tile_bm, by the whole CTA: gather the tile's group sums
@@ -274,12 +274,16 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
 
     // ---- 3. scaled Berlekamp-Massey, thread i owns C_i -------------------
     // Per step: (1) warps holding coefficients i <= min(N, t, max L) form
-    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp;
-    // barrier; (2) every thread sums the shares (d, per ciphertext), every
+    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp and
+    // added into the step's sum in shared memory by atomic XOR; barrier;
+    // (2) every thread reads the sum (d, per ciphertext), every
     // warp derives the same decisions, and the owners of i <= new max L form
     // C_i <- b*C_i + d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in
     // the ring slot of coefficient i.  Ring entries above that, up to the
     // largest possible degree of B, only take the swap (C_i = 0 there).
+    if (tid < 32)
+        sm.dsum[tid >> 4][tid & 15] = 0;  // the sums of steps 0 and 1
+    __syncthreads();
     const int i = tid;
     uint32_t C[M], bb[M];
 #pragma unroll
@@ -306,36 +310,34 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
                 bs_mul_acc<M>(p, C, sv);
                 bs_reduce<M>(p);
             }
+            // lane k < M adds plane k of the warp's share into the step's sum
+            uint32_t mine = 0;
 #pragma unroll
             for (int k = 0; k < M; k++) {
                 const uint32_t v = __reduce_xor_sync(FULL, p[k]);
-                if (lane == 0)
-                    sm.part[N & 1][warp][k] = v;
+                mine = lane == k ? v : mine;
             }
+            if (lane < M)
+                atomicXor(&sm.dsum[N % 3][lane], mine);
         }
         __syncthreads();
-        // every warp's shares at once (independent loads; warps past `lim`
-        // contribute nothing this step)
+        // The sum of step N+2 (the buffer of step N-1) starts from zero: its
+        // readers, at step N-1, all passed this step's barrier, and its
+        // writers, at step N+2, come after the next one.
+        if (tid < 16)
+            sm.dsum[(N + 2) % 3][tid] = 0;
         uint32_t d[M], mne = 0;
-#pragma unroll
-        for (int k = 0; k < M; k++)
-            d[k] = 0;
-        uint4 xs[BM_WARPS][(M + 3) / 4];
-#pragma unroll
-        for (int w = 0; w < BM_WARPS; w++)
-#pragma unroll
-            for (int v = 0; v < (M + 3) / 4; v++)
-                xs[w][v] = 32 * w <= lim ? reinterpret_cast<const uint4 *>(sm.part[N & 1][w])[v]
-                                         : make_uint4(0, 0, 0, 0);
-#pragma unroll
-        for (int w = 0; w < BM_WARPS; w++)
+        {
+            const uint4 *ds = reinterpret_cast<const uint4 *>(sm.dsum[N % 3]);
 #pragma unroll
             for (int v = 0; v < (M + 3) / 4; v++) {
-                if (4 * v + 0 < M) d[4 * v + 0] ^= xs[w][v].x;
-                if (4 * v + 1 < M) d[4 * v + 1] ^= xs[w][v].y;
-                if (4 * v + 2 < M) d[4 * v + 2] ^= xs[w][v].z;
-                if (4 * v + 3 < M) d[4 * v + 3] ^= xs[w][v].w;
+                const uint4 x = ds[v];
+                if (4 * v + 0 < M) d[4 * v + 0] = x.x;
+                if (4 * v + 1 < M) d[4 * v + 1] = x.y;
+                if (4 * v + 2 < M) d[4 * v + 2] = x.z;
+                if (4 * v + 3 < M) d[4 * v + 3] = x.w;
             }
+        }
 #pragma unroll
         for (int k = 0; k < M; k++)
             mne |= d[k];
