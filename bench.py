@@ -58,7 +58,9 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--kernel-only", action="store_true",
-                    help="only the fused-kernel steps (profiling runs: no peak, plain, e2e or CPU legs)")
+                    help="only the decrypt-kernel steps of --path (profiling runs: no peak, e2e or CPU legs)")
+    ap.add_argument("--path", choices=["fused", "plain", "tile"], default="fused",
+                    help="decrypt path the --kernel-only steps launch")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--serve-keys", type=int, default=1024)
     ap.add_argument("--serve-seconds", type=float, default=1.0)
@@ -658,9 +660,10 @@ def main() -> None:
         return ms, launches, clk.summary()
 
     if args.kernel_only:
-        ms, launches, _ = timed("fused", args.steps, args.warmup)
+        ms, launches, _ = timed(args.path, args.steps, args.warmup)
         if rank == 0:
-            print(json.dumps({"kernel_only": True, "decaps_per_s": job_rate(world, count * args.steps, ms * 1e-3),
+            print(json.dumps({"kernel_only": True, "path": args.path,
+                              "decaps_per_s": job_rate(world, count * args.steps, ms * 1e-3),
                               "ms_per_step": ms / args.steps, "gpu_launches": launches}), flush=True)
         return
     int_peak = eng.int_peak()
