@@ -226,8 +226,23 @@ template <int S> struct TileSmem {
     static constexpr int SS = Z::M | 1;  // odd plane stride: per-coefficient rows meet no bank conflicts
     uint32_t sx[Z::NS * SS];             // group sums -> syndromes -> converted locators
     uint32_t ring[(Z::T + 2) * SS];      // B, rotated one slot per step (the x*B shift)
-    alignas(16) uint32_t dsum[3][16];  // the discrepancy, summed by the warps' atomic XORs (step mod 3)
+    // Each warp's share of the discrepancy, plane k in word k (step parity):
+    // plain stores, summed by every reader after the barrier.  (Shared
+    // atomics from several warps onto the same 13 words serialise: about
+    // 500 cycles a step on B200.)
+    alignas(16) uint32_t wsum[2][BM_WARPS][16];
 };
+
+// The barrier of the warps that hold locator coefficients: the block
+// barrier when all of them do, else named barrier 1 for the first NT threads.
+template <int NT> __device__ __forceinline__ void bm_barrier()
+{
+    static_assert(NT % 32 == 0 && NT <= BM_THREADS, "whole warps");
+    if constexpr (NT == BM_THREADS)
+        __syncthreads();
+    else
+        asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
+}
 
 // Steps 1-2 of k_tile_bm, by the whole CTA: gather the tile's group sums
 // (sx[s][k] bit q = plane k of sum s of ciphertext q; zero for q >= count),
@@ -273,115 +288,149 @@ __device__ __forceinline__ void tile_bm(int count, const uint32_t *tile_scratch,
     tile_syndromes<S>(count, tile_scratch, sm, scalpow);
 
     // ---- 3. scaled Berlekamp-Massey, thread i owns C_i -------------------
-    // Per step: (1) warps holding coefficients i <= min(N, t, max L) form
-    // their shares C_i * S_{N-i} of the discrepancy, XOR-reduced per warp and
-    // added into the step's sum in shared memory by atomic XOR; barrier;
-    // (2) every thread reads the sum (d, per ciphertext), every
-    // warp derives the same decisions, and the owners of i <= new max L form
-    // C_i <- b*C_i + d*B_i and B_i <- (N >= 2L and d != 0) ? old C_i : B_i in
-    // the ring slot of coefficient i.  Ring entries above that, up to the
-    // largest possible degree of B, only take the swap (C_i = 0 there).
-    if (tid < 32)
-        sm.dsum[tid >> 4][tid & 15] = 0;  // the sums of steps 0 and 1
-    __syncthreads();
+    // Warps 0 .. NWA-1 hold coefficients 0..t and run the loop on their own
+    // named barrier (the fifth warp, needed only for t = 128, otherwise waits
+    // at the block barrier after the loop).  Per step:
+    //  (1) warps holding coefficients i <= max L form their shares
+    //      C_i * S_{N-i}, XOR-reduce them across the warp (plane k to lane
+    //      k) and store them; b * C_i, which needs no discrepancy, is formed
+    //      in the same straight-line block, so it covers the reductions'
+    //      latency;
+    //  (2) barrier; every thread sums the warps' shares: d, bitsliced;
+    //  (3) the owners of i <= hi form C_i <- b*C_i + d*B_i and B_i <- (N >=
+    //      2L and d != 0) ? old C_i : B_i in the ring slot of coefficient i.
+    //      hi = max(Lup, largest possible degree of B), with Lup = min(t,
+    //      max(max L, N + 1 - min L)) a bound on every ciphertext's new L
+    //      that is known before d is.  Coefficients above a ciphertext's new
+    //      L come out zero (deg C <= L; b*C_i + d*B_i = 0 there), so a larger
+    //      bound changes nothing, and above Lup the update is the swap alone.
+    // The next step's decisions (mle = (d != 0) & (N >= 2L) from a mask of
+    // the second condition, the new L, the tile's bounds) are lane bits and
+    // warp reductions that overlap the update's multiplies.
+    constexpr int NWA = (T + 32) / 32;  // warps holding coefficients 0..t
+    static_assert(NWA <= BM_WARPS && 32 * NWA > T, "coefficient warps");
     const int i = tid;
-    uint32_t C[M], bb[M];
+    uint32_t C[M];
 #pragma unroll
-    for (int k = 0; k < M; k++) {
+    for (int k = 0; k < M; k++)
         C[k] = (i == 0 && k == 0) ? FULL : 0u;
-        bb[k] = k == 0 ? FULL : 0u;  // b = 1
-    }
-    int Lq = 0, Bd = 1;    // lane q: L and a bound on deg B of ciphertext q
-    int Lmax = 0, Bmax = 1;
+    __syncthreads();  // the syndromes and the ring are in place
+    if (warp < NWA) {
+        uint32_t bb[M];
+#pragma unroll
+        for (int k = 0; k < M; k++)
+            bb[k] = k == 0 ? FULL : 0u;  // b = 1
+        int Lq = 0, Bd = 1;              // lane q: L and a bound on deg B of ciphertext q
+        int Lmax = 0, Lmin = 0, Bmax = 1;
+        uint32_t geq = FULL;             // bit q: N >= 2 L_q
 #pragma unroll 1
-    for (int N = 0; N < 2 * T; N++) {
-        const int lim = min(N, min(T, Lmax));
-        if (32 * warp <= lim) {
-            uint32_t p[2 * M - 1];
+        for (int N = 0; N < 2 * T; N++) {
+            // L <= N at step N, so lim = min(N, t, max L) is the tile's
+            // largest L, and C_i = 0 for every i above it.
+            const int lim = min(N, min(T, Lmax));
+            const int Lup = min(T, max(Lmax, N + 1 - Lmin));
+            uint32_t(*ws)[16] = sm.wsum[N & 1];
+            uint32_t q1[2 * M - 1];  // b * C_i, unreduced (zero where C_i = 0)
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
-                p[k] = 0;
-            if (i <= lim) {
-                uint32_t sv[M];
-                const uint32_t *src = sm.sx + (N - i) * SS;
+                q1[k] = 0;
+            if (32 * warp <= lim) {
+                // Lanes above lim multiply C_i = 0 (their row index is
+                // clamped to stay inside the syndromes).
+                uint32_t p[2 * M - 1], sv[M], v[M];
+#pragma unroll
+                for (int k = 0; k < 2 * M - 1; k++)
+                    p[k] = 0;
+                const uint32_t *src = sm.sx + max(N - i, 0) * SS;
 #pragma unroll
                 for (int k = 0; k < M; k++)
                     sv[k] = src[k];
                 bs_mul_acc<M>(p, C, sv);
                 bs_reduce<M>(p);
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    v[k] = __reduce_xor_sync(FULL, p[k]);
+                bs_mul_acc<M>(q1, bb, C);
+                uint32_t mine = 0;
+#pragma unroll
+                for (int k = 0; k < M; k++)
+                    mine = lane == k ? v[k] : mine;
+                if (lane < M)
+                    ws[warp][lane] = mine;
             }
-            // lane k < M adds plane k of the warp's share into the step's sum
-            uint32_t mine = 0;
-#pragma unroll
-            for (int k = 0; k < M; k++) {
-                const uint32_t v = __reduce_xor_sync(FULL, p[k]);
-                mine = lane == k ? v : mine;
-            }
-            if (lane < M)
-                atomicXor(&sm.dsum[N % 3][lane], mine);
-        }
-        __syncthreads();
-        // The sum of step N+2 (the buffer of step N-1) starts from zero: its
-        // readers, at step N-1, all passed this step's barrier, and its
-        // writers, at step N+2, come after the next one.
-        if (tid < 16)
-            sm.dsum[(N + 2) % 3][tid] = 0;
-        uint32_t d[M], mne = 0;
-        {
-            const uint4 *ds = reinterpret_cast<const uint4 *>(sm.dsum[N % 3]);
-#pragma unroll
-            for (int v = 0; v < (M + 3) / 4; v++) {
-                const uint4 x = ds[v];
-                if (4 * v + 0 < M) d[4 * v + 0] = x.x;
-                if (4 * v + 1 < M) d[4 * v + 1] = x.y;
-                if (4 * v + 2 < M) d[4 * v + 2] = x.z;
-                if (4 * v + 3 < M) d[4 * v + 3] = x.w;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < M; k++)
-            mne |= d[k];
-        const bool my_mle = ((mne >> lane) & 1u) && (N >= 2 * Lq);
-        const uint32_t mle = __ballot_sync(FULL, my_mle);
-        const int Lnew = my_mle ? N + 1 - Lq : Lq;
-        const int Bdnew = min(min(my_mle ? Lq : Bd, T) + 1, T);
-        const int Lb = min(__reduce_max_sync(FULL, (unsigned)Lnew), (unsigned)T);
-        int slot = i - N % R;
-        slot = slot < 0 ? slot + R : slot;
-        uint32_t *bp = sm.ring + slot * SS;
-        if (i <= Lb) {
-            uint32_t bv[M], q1[2 * M - 1];
-#pragma unroll
-            for (int k = 0; k < 2 * M - 1; k++)
-                q1[k] = 0;
+            bm_barrier<NWA * 32>();
+            // Ring entries this step touches: coefficients i <= hi (B_i, and
+            // the swap), loaded before d so the loads overlap its sum.
+            const int hi = max(Lup, min(Bmax, T));
+            const bool own = i <= hi;
+            int slot = i - N % R;
+            slot = slot < 0 ? slot + R : slot;
+            uint32_t *bp = sm.ring + slot * SS;
+            uint32_t bv[M];
 #pragma unroll
             for (int k = 0; k < M; k++)
-                bv[k] = bp[k];
-            bs_mul_acc<M>(q1, bb, C);
-            bs_mul_acc<M>(q1, d, bv);
-            bs_reduce<M>(q1);
-#pragma unroll
-            for (int k = 0; k < M; k++) {
-                bp[k] = (bv[k] & ~mle) | (C[k] & mle);
-                C[k] = q1[k];
-            }
-        } else if (i <= min(Bmax, T)) {
+                bv[k] = own ? bp[k] : 0u;
+            // The buffer of step N is written again at step N + 2, after
+            // every reader here has passed the next step's barrier.
+            uint32_t d[M];
 #pragma unroll
             for (int k = 0; k < M; k++)
-                bp[k] &= ~mle;
-        }
-        // the slot that becomes coefficient 0 of x*B at step N+1
-        const int freeslot = (R - (N + 1) % R) % R;
-        if (tid < M)
-            sm.ring[freeslot * SS + tid] = 0;
+                d[k] = 0;
 #pragma unroll
-        for (int k = 0; k < M; k++)
-            bb[k] = (bb[k] & ~mle) | (d[k] & mle);
-        Lq = Lnew;
-        Bd = Bdnew;
-        Lmax = Lb;
-        // (slots past `count` never take the swap: their syndromes are zero)
-        Bmax = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)Bdnew : 0u);
+            for (int w = 0; w < NWA; w++) {
+                if (32 * w <= lim) {
+                    const uint4 *src = reinterpret_cast<const uint4 *>(ws[w]);
+#pragma unroll
+                    for (int v = 0; v < (M + 3) / 4; v++) {
+                        const uint4 x = src[v];
+                        if (4 * v + 0 < M) d[4 * v + 0] ^= x.x;
+                        if (4 * v + 1 < M) d[4 * v + 1] ^= x.y;
+                        if (4 * v + 2 < M) d[4 * v + 2] ^= x.z;
+                        if (4 * v + 3 < M) d[4 * v + 3] ^= x.w;
+                    }
+                }
+            }
+            uint32_t mne = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                mne |= d[k];
+            const uint32_t mle = mne & geq;
+            const bool my_mle = (mle >> lane) & 1u;
+            const int Lnew = my_mle ? N + 1 - Lq : Lq;
+            const int Bdnew = min(min(my_mle ? Lq : Bd, T) + 1, T);
+            // the tile's bounds for the next step (lanes past `count` keep
+            // L = 0 and never take the swap: their syndromes are zero)
+            const int Lmax_n = (int)__reduce_max_sync(FULL, (unsigned)Lnew);
+            const int Lmin_n = (int)__reduce_min_sync(FULL, lane < count ? (unsigned)Lnew : 0xFFFFu);
+            const int Bmax_n = (int)__reduce_max_sync(FULL, lane < count ? (unsigned)Bdnew : 0u);
+            const uint32_t geq_n = __ballot_sync(FULL, N + 1 >= 2 * Lnew);
+            // C_i <- b*C_i + d*B_i for i <= hi; lanes above hi hold C_i = 0
+            // and load B_i = 0, so they keep C_i = 0 and store nothing
+            // (their slots belong to other coefficients).
+            if (32 * warp <= hi) {
+                bs_mul_acc<M>(q1, d, bv);
+                bs_reduce<M>(q1);
+#pragma unroll
+                for (int k = 0; k < M; k++) {
+                    if (own)
+                        bp[k] = (bv[k] & ~mle) | (C[k] & mle);
+                    C[k] = q1[k];
+                }
+            }
+            // the slot that becomes coefficient 0 of x*B at step N+1
+            const int freeslot = (R - (N + 1) % R) % R;
+            if (tid < M)
+                sm.ring[freeslot * SS + tid] = 0;
+#pragma unroll
+            for (int k = 0; k < M; k++)
+                bb[k] = (bb[k] & ~mle) | (d[k] & mle);
+            Lq = Lnew;
+            Bd = Bdnew;
+            Lmax = min(Lmax_n, T);
+            Lmin = Lmin_n;
+            Bmax = Bmax_n;
+            geq = geq_n;
+        }
     }
     __syncthreads();
     // ---- 4. radix conversion of the reversed locators, out ---------------
