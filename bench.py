@@ -61,6 +61,8 @@ def parse() -> argparse.Namespace:
                     help="only the decrypt-kernel steps of --path (profiling runs: no peak, e2e or CPU legs)")
     ap.add_argument("--path", choices=["fused", "plain", "tile"], default="fused",
                     help="decrypt path the --kernel-only steps launch")
+    ap.add_argument("--wpb", type=int, default=0,
+                    help="--kernel-only: fused-kernel warps per CTA (0: the tuner's cached choice or the default)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving-loop leg")
     ap.add_argument("--serve-keys", type=int, default=1024)
     ap.add_argument("--serve-seconds", type=float, default=1.0)
@@ -614,6 +616,8 @@ def main() -> None:
 
     # Launch configuration chosen by the autotuner (cached per GPU and set),
     # then one captured CUDA graph per buffer set, replayed every step.
+    if args.kernel_only and args.wpb:
+        cmd.set_fused_config(eng, SET, args.wpb)
     tuned = cmd.fused_config(eng, SET) if args.kernel_only else cmd.tune(eng, key)
     graphs = [cmd.Graph(eng, key, d_cts[b].data_ptr(), count, d_err[b].data_ptr(), d_w[b].data_ptr(), path="fused")
               for b in range(nbuf)]
