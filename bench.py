@@ -286,6 +286,32 @@ def reference_gpu_leg(cmd, eng, key, stream) -> dict:
     return out
 
 
+def plain_roofline(cmd, eng, key, d_ct, count: int, stream, int_peak: float) -> dict:
+    """Each plain per-stage kernel timed alone (CUDA events on `stream`,
+    3 calls after 1 warm-up) over the bench batch, against the work of the
+    reference's own algorithm for that stage (roofline.plain_stage_work)."""
+    import torch
+    from cm_decrypt__b200.roofline import plain_stage_work
+    info = key.info
+    d_s = torch.zeros((count, 2 * info.t), dtype=torch.int16, device="cuda")
+    d_l = torch.zeros((count, info.t + 1), dtype=torch.int16, device="cuda")
+    d_e = torch.zeros((count, info.err_words), dtype=torch.int32, device="cuda")
+    d_w = torch.zeros(count, dtype=torch.int16, device="cuda")
+    sp = stream.cuda_stream
+    ms = {"synd": _time_stream(lambda: cmd.synd(eng, key, d_ct.data_ptr(), count, d_s.data_ptr(), sp), stream, 3, 1),
+          "bm": _time_stream(lambda: cmd.bm(eng, SET, d_s.data_ptr(), count, d_l.data_ptr(), sp), stream, 3, 1),
+          "root": _time_stream(lambda: cmd.root(eng, key, d_l.data_ptr(), count, d_e.data_ptr(), d_w.data_ptr(), sp),
+                               stream, 3, 1)}
+    work = plain_stage_work(SET)
+    out = {"bound": "int_alu", "unit": "Tlane-ops/s (lop3)", "peak": int_peak / 1e12,
+           "work": "the reference's algorithm per stage: table-row sums, bm()'s multiplies, Horner at every "
+                   "support point (cm_decrypt__b200/roofline.py)", "stages": {}}
+    for k in ("synd", "bm", "root"):
+        a = count / (ms[k] * 1e-3) * work[k]
+        out["stages"][k] = {"ms": ms[k], "lane_ops_per_decap": work[k], "achieved": a / 1e12, "frac": a / int_peak}
+    return out
+
+
 def rank_seed(rank: int) -> int:
     """Seed of a replica's workload: every rank decrypts its own batch."""
     return 1000 + rank
@@ -672,9 +698,10 @@ def main() -> None:
         return
     int_peak = eng.int_peak()
     ms, launches, clocks = timed("fused", args.steps, args.warmup)
-    ms_plain = None
+    ms_plain, roof_plain = None, None
     if not args.no_plain:
         ms_plain, _, _ = timed("plain", max(1, min(args.steps, 3)), 1)
+        roof_plain = plain_roofline(cmd, eng, key, d_cts[0], count, stream, int_peak)
 
     # End to end through the public host-buffer call, pinned host memory.
     h_cts = torch.from_numpy(cts).pin_memory().numpy()
@@ -777,7 +804,8 @@ def main() -> None:
                                    "x_peak": per_rank * w["yardstick_total"] / int_peak},
                      "traffic": traffic, "traffic_detail": traffic_detail,
                      "hbm": {"achieved_gbs": hbm / 1e9, "peak_gbs": hbm_peak, "frac": hbm / 1e9 / hbm_peak,
-                             "bytes_per_decap": hbm_bytes_per_decap(SET)}},
+                             "bytes_per_decap": hbm_bytes_per_decap(SET)},
+                     "plain": roof_plain},
         "clocks": clocks,
         "fused_config": {"tuned": tuned, "launch": "CUDA graph replay, one graph per buffer set"},
     }

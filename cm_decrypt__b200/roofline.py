@@ -28,6 +28,16 @@ point, root_13.c:216-240) is kept beside it:
 
   W_chien = n * t * (m^2 + R_m + m) / 32
 
+The plain per-stage kernels are measured against the work of the
+reference's own algorithm for each stage:
+
+  synd          W_synd as above (sum of table rows)
+  bm            the reference bm()'s multiplies: sum_{N<2t} (min(N,t) + 1)
+                discrepancy terms, t+1 updates per step, and the d/b of each
+                step as 8 multiply-equivalents (an inversion chain), each
+                multiply m^2 + R_m + m bit operations
+  root          W_chien (Horner at every support point)
+
 Bytes per decryption that must cross HBM: the ciphertext in and the n-bit
 error vector out.
 """
@@ -59,6 +69,15 @@ def work_per_decap(set_id: int) -> dict:
     w_chien = n * t * (mul + m) / 32
     return {"synd": w_synd, "bm": w_bm, "root_fft": w_root, "total": w_synd + w_bm + w_root,
             "yardstick_chien": w_chien, "yardstick_total": w_synd + w_bm + w_chien}
+
+
+def plain_stage_work(set_id: int) -> dict:
+    """Lane-ops per decryption of the reference algorithm of each plain stage."""
+    m, n, t, ct = SETS[set_id]
+    r = 22 if m == 12 else 48
+    w = work_per_decap(set_id)
+    muls = sum(min(N, t) + 1 for N in range(2 * t)) + 2 * t * (t + 1) + 16 * t
+    return {"synd": w["synd"], "bm": muls * (m * m + r + m) / 32, "root": w["yardstick_chien"]}
 
 
 def hbm_bytes_per_decap(set_id: int) -> int:
