@@ -43,6 +43,16 @@ template <int S> struct FftDims {
     static_assert(D <= M - 5, "butterflies must pair whole words");
 };
 
+// Where word w of a plane of the per-warp butterfly array is stored: odd
+// 32-word rows keep their words with the bank bits inverted.  The butterfly
+// levels that pair words less than 32 apart put lanes l and l + 16 in rows 2r
+// and 2r + 1 at the same offsets; with the inversion those offsets fall in
+// disjoint halves of the banks (offsets whose bit log2(distance) is 0 map to
+// ones where it is 1), so no level meets a bank conflict.  Whole-row accesses
+// stay a permutation of the banks.  Every read and write of the array goes
+// through this map.
+__device__ __forceinline__ int fa_word(int w) { return w ^ ((0 - ((w >> 5) & 1)) & 31); }
+
 // Radix conversion of the bitsliced array cv[x * CVS + k] (x < 2^D, k < M),
 // by NT cooperating threads (tid in [0, NT)); `sync` orders the steps.
 template <int S, int CVS, int NT, class Sync>
@@ -217,11 +227,12 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
                 p[k] = 0;
             bs_mul_acc<M>(p, G, B);
             bs_reduce<M>(p);
+            const int pa = fa_word(wa), pb = fa_word(wa + Sw);
 #pragma unroll
             for (int k = 0; k < M; k++) {
                 const uint32_t na = (0u - ((cv[sa * CVS + k] >> q) & 1u)) ^ p[k];
-                fa[k * NWD + wa] = na;
-                fa[k * NWD + wa + Sw] = na ^ B[k];
+                fa[k * NWD + pa] = na;
+                fa[k * NWD + pb] = na ^ B[k];
             }
         }
         __syncwarp();
@@ -235,11 +246,12 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
             const int P2 = lane + 32 * j;
             const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
             const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+            const int pa = fa_word(wa), pb = fa_word(wa + Sw);
             uint32_t A[M], B[M], G[M], p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                A[k] = fa[k * NWD + wa];
-                B[k] = fa[k * NWD + wa + Sw];
+                A[k] = fa[k * NWD + pa];
+                B[k] = fa[k * NWD + pb];
                 G[k] = __ldg(g + k);
             }
 #pragma unroll
@@ -250,8 +262,8 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
 #pragma unroll
             for (int k = 0; k < M; k++) {
                 const uint32_t na = A[k] ^ p[k];
-                fa[k * NWD + wa] = na;
-                fa[k * NWD + wa + Sw] = na ^ B[k];
+                fa[k * NWD + pa] = na;
+                fa[k * NWD + pb] = na ^ B[k];
             }
         }
         __syncwarp();
@@ -266,11 +278,12 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
         for (int j = 0; j < R / 2; j++) {
             const int wa = lane + 32 * j;
             const uint32_t *g = tw + (size_t)wa * 16;  // depth 0: offset 0
+            const int pa = fa_word(wa), pb = fa_word(wa + Sw);
             uint32_t A[M], B[M], G[M], p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                A[k] = fa[k * NWD + wa];
-                B[k] = fa[k * NWD + wa + Sw];
+                A[k] = fa[k * NWD + pa];
+                B[k] = fa[k * NWD + pb];
                 G[k] = __ldg(g + k);
             }
 #pragma unroll

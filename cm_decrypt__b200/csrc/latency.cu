@@ -120,10 +120,11 @@ __device__ __forceinline__ void tsynd_one(const LatItem &it, const uint8_t *__re
             p[k] = 0;
         bs_mul_acc<M>(p, G, A);
         bs_reduce<M>(p);
+        const int pa = fa_word(wa), pb = fa_word(wb);
 #pragma unroll
         for (int k = 0; k < M; k++) {
-            fa[k * NWD + wa] = A[k];
-            fa[k * NWD + wb] = B[k] ^ p[k];
+            fa[k * NWD + pa] = A[k];
+            fa[k * NWD + pb] = B[k] ^ p[k];
         }
     }
     __syncwarp();
@@ -137,11 +138,12 @@ __device__ __forceinline__ void tsynd_one(const LatItem &it, const uint8_t *__re
             const int P2 = lane + 32 * j;
             const int wa = ((P2 >> sbit) << (sbit + 1)) | (P2 & (Sw - 1));
             const uint32_t *g = twd + (P2 & (Sw - 1)) * 16;
+            const int pa = fa_word(wa), pb = fa_word(wa + Sw);
             uint32_t A[M], B[M], G[M], p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                B[k] = fa[k * NWD + wa + Sw];
-                A[k] = fa[k * NWD + wa] ^ B[k];
+                B[k] = fa[k * NWD + pb];
+                A[k] = fa[k * NWD + pa] ^ B[k];
                 G[k] = __ldg(g + k);
             }
 #pragma unroll
@@ -151,8 +153,8 @@ __device__ __forceinline__ void tsynd_one(const LatItem &it, const uint8_t *__re
             bs_reduce<M>(p);
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                fa[k * NWD + wa] = A[k];
-                fa[k * NWD + wa + Sw] = B[k] ^ p[k];
+                fa[k * NWD + pa] = A[k];
+                fa[k * NWD + pb] = B[k] ^ p[k];
             }
         }
         __syncwarp();
@@ -169,11 +171,12 @@ __device__ __forceinline__ void tsynd_one(const LatItem &it, const uint8_t *__re
 #pragma unroll 1
         for (int j = 0; j < R / 2; j++) {
             const int wa = 2 * (lane + 32 * j);
+            const int ia = fa_word(wa), ib = fa_word(wa + 1);
             uint32_t A[M], B[M], p[2 * M - 1];
 #pragma unroll
             for (int k = 0; k < M; k++) {
-                B[k] = fa[k * NWD + wa + 1];
-                A[k] = fa[k * NWD + wa] ^ B[k];
+                B[k] = fa[k * NWD + ib];
+                A[k] = fa[k * NWD + ia] ^ B[k];
             }
 #pragma unroll
             for (int k = 0; k < 2 * M - 1; k++)
