@@ -18,8 +18,10 @@
 //  * Small batches run the latency kernels of latency.cu (any mix of keys and
 //    sets in three launches, a short pass per ciphertext); batches of
 //    fused_threshold or more run the fused kernel (highest throughput).
-//  * A completer thread polls the batches in flight without the queue lock,
-//    takes whichever finishes first, copies each result to its request's
+//  * A completer thread watches the batches in flight without the queue lock
+//    (each batch's stream copies its sequence number to a pinned word after
+//    the results, so the watch is plain loads, not CUDA calls), takes
+//    whichever finishes first, copies each result to its request's
 //    buffer (large batches split across a few copy threads) and records
 //    arrival-to-completion latency for the p50/p99 statistics.
 //  * Host work per request is O(1): the queue is a vector whose buffers
@@ -205,6 +207,7 @@ struct Slot {
     uint32_t *d_counter = nullptr;
     std::vector<Request> reqs;  // taken from the queue (a buffer swap when a batch takes it all)
     uint64_t gen = 0;          // generation of the batch in this slot (its keys carry it)
+    uint64_t seq = 0;          // sequence number of the batch in this slot (from 1)
     bool fused = false;
     // completer scratch, reused batch to batch
     std::vector<uint32_t> lats, waits;
@@ -275,9 +278,19 @@ struct cmd_server {
     std::condition_variable cv_dispatch, cv_complete, cv_poll;
     RequestQueue pending;
     std::deque<KeyEntry> keys;   // deque: entries keep their address as keys are added
+    // The keys' sets again, for the submitters: they read a key's set for
+    // every request, while the dispatcher writes its generation stamps into
+    // the key entries; reading the set from those entries kept their cache
+    // lines moving between the two cores (about 70 us of every batch's key
+    // pass at several thousand batches a second).
+    std::deque<int32_t> key_sets;
     std::vector<Slot> slots;
     std::deque<int> free_slots;
     std::atomic<uint32_t> inflight{0};  // bit s: slot s has a batch on the GPU (set under mu)
+    // done_seq[s]: pinned host word that slot s's stream overwrites with the
+    // batch's sequence number after its result copies (a stream-ordered
+    // 8-byte copy), so the completer sees a finished batch with plain loads
+    volatile uint64_t *done_seq = nullptr;
     std::deque<cmd_completion> completions;
     std::thread dispatcher, completer;
     std::unique_ptr<CopyPool> copiers;
@@ -312,7 +325,7 @@ size_t tile_cap(size_t B) { return B / 32 + NSETS + 1; }
 // ciphertext, then (fused) ct_off, err_off, order, tiles, key table, then
 // (tile path) the work items.
 struct InLayout {
-    size_t cts, key_idx, ct_off, err_off, order, tiles, keys, items, total;
+    size_t cts, key_idx, ct_off, err_off, order, tiles, keys, items, seq, total;
     InLayout(size_t B, size_t max_keys)
     {
         auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -324,7 +337,8 @@ struct InLayout {
         tiles = al(order + B * 4);
         keys = al(tiles + B * sizeof(FusedTile));
         items = al(keys + max_keys * sizeof(FusedKeyRef));
-        total = al(items + row_cap(B) * sizeof(LatItem));
+        seq = al(items + row_cap(B) * sizeof(LatItem));  // the batch's sequence number (8 bytes)
+        total = al(seq + 8);
     }
 };
 
@@ -383,7 +397,16 @@ int cmd_server::launch(Slot &sl)
     std::shared_lock<std::shared_mutex> key_hold(keys_mu);
     std::vector<uint32_t> kid;
     uint64_t gen = ++batch_gen;
-    for (const Request &r : sl.reqs) {
+    // The requests were just written by the submitting threads, so each first
+    // touch here is a miss served from another core's cache; prefetching a
+    // few requests ahead overlaps those misses instead of taking them one by
+    // one.
+    constexpr size_t AHEAD = 12;
+    const size_t nreq = sl.reqs.size();
+    for (size_t i = 0; i < nreq; i++) {
+        if (i + AHEAD < nreq)
+            __builtin_prefetch(&sl.reqs[i + AHEAD]);
+        const Request &r = sl.reqs[i];
         KeyEntry &ke = keys[r.key_id];
         if (ke.seen_gen != gen) {
             ke.seen_gen = gen;
@@ -416,6 +439,8 @@ int cmd_server::launch(Slot &sl)
     sl.gen = gen;  // the batch's keys stay in use while it is in flight
     const size_t B = sl.reqs.size();
     InLayout lay(B, B);
+    sl.seq++;
+    memcpy(sl.h_in + lay.seq, &sl.seq, 8);
     for (size_t i = 0; i < B; i++)
         memcpy(sl.h_in + lay.cts + i * CT_STRIDE, sl.reqs[i].ct, CT_STRIDE);
     LaunchCounter lc{&eng->launches};
@@ -458,7 +483,7 @@ int cmd_server::launch(Slot &sl)
         sl.rows_used = (size_t)ntiles * 32;
         if ((e = cudaMemcpyAsync(sl.d_in + lay.cts, sl.h_in + lay.cts, B * CT_STRIDE, cudaMemcpyHostToDevice, s)) !=
                 cudaSuccess ||
-            (e = cudaMemcpyAsync(sl.d_in + lay.items, sl.h_in + lay.items, sl.rows_used * sizeof(LatItem),
+            (e = cudaMemcpyAsync(sl.d_in + lay.items, sl.h_in + lay.items, lay.seq + 8 - lay.items,
                                  cudaMemcpyHostToDevice, s)) != cudaSuccess)
             return cuda_fail(e, "server H2D");
         FftPlans plans;
@@ -530,7 +555,9 @@ int cmd_server::launch(Slot &sl)
     if ((e = cudaMemcpyAsync(sl.h_err, sl.d_err, sl.rows_used * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) !=
             cudaSuccess ||
         (e = cudaMemcpyAsync(sl.h_w, sl.d_w, sl.rows_used * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
-        (e = cudaEventRecord(sl.done, s)) != cudaSuccess)
+        (e = cudaEventRecord(sl.done, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync((void *)(done_seq + (&sl - slots.data())), sl.d_in + lay.seq, 8, cudaMemcpyDeviceToHost,
+                             s)) != cudaSuccess)
         return cuda_fail(e, "server D2H");
     return CMD_OK;
 }
@@ -607,6 +634,7 @@ void cmd_server::dispatch_loop()
 void cmd_server::complete_loop()
 {
     cudaSetDevice(eng->device);
+    uint64_t idle_since = 0;
     while (true) {
         uint32_t mask = inflight.load();
         if (!mask) {
@@ -621,19 +649,35 @@ void cmd_server::complete_loop()
         // a large one.  With one batch in flight, block on its event.  The
         // in-flight set is read without the queue lock, so polling does not
         // slow submitters down.
+        // A batch is finished when its stream has copied the batch's
+        // sequence number into done_seq (after its results): the check is a
+        // plain load, with no CUDA call that would contend in the runtime
+        // with the dispatcher's launches.  A failed stream never delivers
+        // it, so after 2 ms without a finished batch the events are queried
+        // for errors.
         int si = -1;
         cudaError_t e = cudaSuccess;
-        if (__builtin_popcount(mask) == 1) {
-            si = __builtin_ctz(mask);
-            e = cudaEventSynchronize(slots[si].done);
-        } else {
-            for (uint32_t m = mask; m; m &= m - 1) {
-                const int x = __builtin_ctz(m);
-                const cudaError_t q = cudaEventQuery(slots[x].done);
-                if (q != cudaErrorNotReady) {
-                    si = x;
-                    e = q;
-                    break;
+        for (uint32_t m = mask; m; m &= m - 1) {
+            const int x = __builtin_ctz(m);
+            if (done_seq[x] == slots[x].seq) {
+                si = x;
+                break;
+            }
+        }
+        if (si < 0) {
+            const uint64_t tn = now_ns();
+            if (!idle_since)
+                idle_since = tn;
+            if (tn - idle_since > 2000000) {
+                idle_since = tn;
+                for (uint32_t m = mask; m; m &= m - 1) {
+                    const int x = __builtin_ctz(m);
+                    const cudaError_t q = cudaEventQuery(slots[x].done);
+                    if (q != cudaErrorNotReady && q != cudaSuccess) {
+                        si = x;
+                        e = q;
+                        break;
+                    }
                 }
             }
             if (si < 0) {
@@ -641,6 +685,8 @@ void cmd_server::complete_loop()
                 continue;
             }
         }
+        idle_since = 0;
+        std::atomic_thread_fence(std::memory_order_acquire);  // the results landed before the sequence word
         Slot &sl = slots[si];
         const uint64_t t = now_ns();
         float gpu_ms = 0;
@@ -711,7 +757,7 @@ int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8
         if (srv->stop)
             return CMD_E_ARG;
         for (size_t i = 0; i < n; i++)
-            if (key_ids[i] >= srv->keys.size())
+            if (key_ids[i] >= srv->key_sets.size())
                 return CMD_E_ARG;
         const size_t before = srv->pending.size();
         const uint64_t now = t_arrive ? 0 : now_ns();
@@ -720,7 +766,7 @@ int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8
             r.key_id = key_ids[k];
             r.tag = tags ? tags[k] : k;
             r.err_out = h_err_base ? h_err_base + k * err_stride : nullptr;
-            r.set = srv->keys[r.key_id].set;
+            r.set = srv->key_sets[r.key_id];
             const int ctb = set_info(r.set).ct;
             memcpy(r.ct, h_cts + k * ct_stride, ctb);
             memset(r.ct + ctb, 0, CT_STRIDE - ctb);
@@ -767,7 +813,9 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
         return CMD_E_BUDGET;
     }
     srv->slots.resize(cfg->slots);
-    cudaError_t e = cudaSuccess;
+    cudaError_t e = cudaMallocHost((void **)&srv->done_seq, 16 * sizeof(uint64_t));
+    if (e == cudaSuccess)
+        memset((void *)srv->done_seq, 0, 16 * sizeof(uint64_t));
     for (auto &sl : srv->slots) {
         if (e == cudaSuccess)
             e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
@@ -844,6 +892,8 @@ void cmd_server_destroy(cmd_server *srv)
     for (auto &k : srv->keys)
         if (k.key)
             cmd_key_free(k.key);
+    if (srv->done_seq)
+        cudaFreeHost((void *)srv->done_seq);
     if (srv->device_bytes)
         budget_give(srv->eng, srv->device_bytes);
     delete srv;
@@ -859,6 +909,7 @@ int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t
     ke.set = set;
     ke.sk.assign(h_sk, h_sk + sk_len);
     srv->keys.push_back(std::move(ke));
+    srv->key_sets.push_back(set);
     *key_id = (uint32_t)(srv->keys.size() - 1);
     return CMD_OK;
 }

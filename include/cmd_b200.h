@@ -270,7 +270,10 @@ int cmd_decrypt_files_binary(cmd_engine *eng, cmd_set set, const char *sk_path,
  * once, the requests of the keys that did not fit wait for the next batch.
  * Batches of at least fused_threshold requests run the fused kernel, smaller
  * ones the latency kernels (one short pass per ciphertext; fused_threshold 0:
- * always the latency kernels). */
+ * always the latency kernels).  Each slot has its own stream: give the process
+ * at least as many hardware work queues (CUDA_DEVICE_MAX_CONNECTIONS, read at
+ * context creation, default 8) as slots plus the streams of other work, or
+ * batches queue behind each other on the device. */
 typedef struct cmd_server cmd_server;
 typedef struct {
     uint32_t max_batch;          /* requests per batch, 1..65536              */
