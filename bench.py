@@ -651,7 +651,9 @@ def main() -> None:
     # then one captured CUDA graph per buffer set, replayed every step.
     if args.kernel_only and args.wpb:
         cmd.set_fused_config(eng, SET, args.wpb)
-    tuned = cmd.fused_config(eng, SET) if args.kernel_only else cmd.tune(eng, key)
+    # tuned for this batch size (the winner depends on how the batch fills
+    # whole rounds of the resident warps)
+    tuned = cmd.fused_config(eng, SET) if args.kernel_only else cmd.tune(eng, key, sample_count=count)
     graphs = [cmd.Graph(eng, key, d_cts[b].data_ptr(), count, d_err[b].data_ptr(), d_w[b].data_ptr(), path="fused")
               for b in range(nbuf)]
 

@@ -203,18 +203,31 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
         return;  // no work for this warp in this round (the CTA-wide part is done)
 
     // ---- 3. transpose: sS[j*M + k] bit q = bit k of syndrome j of ct q ----
-    // Syndrome bit x = j*M + k is bit x mod 32 of accumulator word x / 32: one
-    // ballot per bit, lane l keeps the ballot of bit l of the word.
+    // Syndrome bit x = j*M + k is bit x mod 32 of accumulator word x / 32.
+    // Each accumulator word is a 32x32 bit matrix (row q = lane q's word),
+    // and sS wants its transpose: five butterfly steps, each swapping the
+    // off-diagonal blocks of one size (16, 8, 4, 2, 1 columns) between lanes
+    // l and l ^ j, leave bit b of every ciphertext in lane b.  (One shuffle
+    // and four logic operations a step, against 32 ballots and selects.)
+    {
+        constexpr uint32_t M0[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+        uint32_t keep[5];  // per step: the columns this lane keeps
 #pragma unroll
-    for (int w = 0; w < NWU; w++) {
-        uint32_t mine = 0;
-#pragma unroll 1
-        for (int b = 0; b < 32; b++) {
-            const uint32_t v = __ballot_sync(FULLMASK, (acc[w] >> b) & 1u);
-            mine = lane == b ? v : mine;
+        for (int st = 0; st < 5; st++)
+            keep[st] = (lane & (16 >> st)) ? ~M0[st] : M0[st];
+#pragma unroll
+        for (int w = 0; w < NWU; w++) {
+            uint32_t v = acc[w];
+#pragma unroll
+            for (int st = 0; st < 5; st++) {
+                const int j = 16 >> st;
+                const uint32_t x = __shfl_xor_sync(FULLMASK, v, j);
+                const uint32_t t = (lane & j) ? (x >> j) : (x << j);
+                v = (v & keep[st]) | (t & ~keep[st]);
+            }
+            if (32 * w + lane < 2 * T * M)
+                sS[32 * w + lane] = v;
         }
-        if (32 * w + lane < 2 * T * M)
-            sS[32 * w + lane] = mine;
     }
     __syncwarp();
 

@@ -112,9 +112,15 @@ static void save_cache(const std::map<std::string, FusedConfig> &m)
     fclose(f);
 }
 
-static std::string cache_key(const cmd_engine *eng, int set)
+// A tuning for a given batch size is kept apart from the default one: which
+// configuration wins depends on how a batch of that size fills whole rounds
+// of the resident warps, not only on the kernel's steady-state rate.
+static std::string cache_key(const cmd_engine *eng, int set, size_t sample_count)
 {
-    return std::string(eng->gpu_name) + "|" + std::to_string(set_info(set).id);
+    std::string k = std::string(eng->gpu_name) + "|" + std::to_string(set_info(set).id);
+    if (sample_count)
+        k += "|n=" + std::to_string(sample_count);
+    return k;
 }
 
 }  // namespace cmd
@@ -172,7 +178,7 @@ int cmd_tune(cmd_engine *eng, const cmd_key *key, size_t sample_count, int force
     const SetInfo si = set_info(set);
     cudaSetDevice(eng->device);
     auto cache = load_cache();
-    const std::string ck = cache_key(eng, set);
+    const std::string ck = cache_key(eng, set, sample_count);
     if (!force) {
         auto it = cache.find(ck);
         if (it != cache.end()) {

@@ -362,7 +362,9 @@ int cmd_kem_keypair_batch(cmd_engine *eng, cmd_set set, const uint8_t *h_seeds, 
 /* ---- fused-kernel tuning and graph replay (no reference counterpart) --- */
 /* Picks the fused kernel's launch configuration for key's set on this GPU
  * (warps per CTA 4|8, equal-share or full rounds) by timing the candidates on
- * sample_count ciphertexts (0 = about three waves), then the batch size below
+ * sample_count ciphertexts (0 = about three waves; pass the batch size the
+ * caller runs: the winner depends on how that size fills whole rounds of the
+ * resident warps, and each size is cached apart), then the batch size below
  * which CMD_PATH_AUTO takes the tile kernels instead (five warps per
  * 32-ciphertext tile for Berlekamp-Massey rather than the fused kernel's
  * one), from timings of both at 256 .. 65,536 ciphertexts.  Results are
