@@ -832,8 +832,8 @@ def main() -> None:
         line["keygen"] = keygen_leg(cmd, eng, count=args.keygen_count)
     if world == 1 and not args.no_serve:
         fused_rate = value
-        rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, 4e6, 5e6, 6e6, 6.5e6, 7e6, round(0.5 * fused_rate, -5),
-                        round(0.6 * fused_rate, -5)})
+        rates = sorted({1e4, 1e5, 5e5, 1e6, 2e6, 3e6, 4e6, 5e6, 6e6, 7e6, 7.5e6, 8e6,
+                        round(0.5 * fused_rate, -5), round(0.6 * fused_rate, -5)})
         line["serving"] = serving_leg(cmd, eng, args.serve_keys, rates, args.serve_seconds,
                                       reference_check=not args.no_reference_check)
         line["serving"]["fused_batch_decaps_per_s"] = fused_rate
