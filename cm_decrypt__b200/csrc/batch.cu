@@ -79,7 +79,7 @@ uint32_t fused_round(cmd_engine *eng, int set, size_t count)
 
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                       uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced,
-                      uint32_t round_cts)
+                      uint32_t round_cts, uint8_t *err_packed)
 {
     const int set = key->dev.set;
     const SetInfo si = set_info(set);
@@ -114,6 +114,7 @@ int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts,
     a.err_stride = (uint32_t)si.nw;
     a.pos = d_pos;
     a.pos_stride = (uint32_t)(si.t + 1);
+    a.err_packed = err_packed;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), s);
     if (e != cudaSuccess)
         return cuda_fail(e, "cudaMemsetAsync(counter)");

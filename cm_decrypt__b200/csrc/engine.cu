@@ -489,6 +489,29 @@ int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const
     return run_device(eng, key, path, d_cts, count, d_err, d_weight, stream ? (cudaStream_t)stream : eng->stream);
 }
 
+// A device address through which kernels can write the host range [h, h +
+// bytes), or null: pinned memory the GPU maps (cudaHostAlloc / cudaMallocHost
+// memory under unified addressing, or registered memory with a device
+// mapping), 2-byte aligned, whose first and last bytes map to one contiguous
+// device range.  Anything else (pageable memory, a range running past its
+// pinned allocation) gives null, and the caller copies through staging.
+static uint8_t *device_view(uint8_t *h, size_t bytes)
+{
+    if (!h || !bytes || (((uintptr_t)h) & 1))
+        return nullptr;
+    cudaPointerAttributes a0{}, a1{};
+    if (cudaPointerGetAttributes(&a0, h) != cudaSuccess || a0.type != cudaMemoryTypeHost || !a0.devicePointer) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (cudaPointerGetAttributes(&a1, h + bytes - 1) != cudaSuccess || a1.type != cudaMemoryTypeHost ||
+        static_cast<uint8_t *>(a1.devicePointer) != static_cast<uint8_t *>(a0.devicePointer) + (bytes - 1)) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return static_cast<uint8_t *>(a0.devicePointer);
+}
+
 int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *h_cts, size_t count,
                       uint8_t *h_err, uint16_t *h_weight)
 {
@@ -515,6 +538,10 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
     // (each with its own work counter, full rounds): one piece's copies run
     // while the others compute, and the pieces' kernels share the SMs.
     const bool pieces = path != CMD_PATH_PLAIN && path != CMD_PATH_TILE && chunk >= (size_t)BATCH_STREAMS * 8192;
+    // With host error rows the GPU can write, the pieces' kernels store the
+    // packed rows there directly: the rows cross PCIe while the kernels run,
+    // instead of in a copy after the last piece's kernel.
+    uint8_t *err_view = pieces ? device_view(h_err, count * (size_t)(si.n / 8)) : nullptr;
     if (pieces) {
         if ((rc = ensure_counter(eng)))
             return rc;
@@ -545,12 +572,14 @@ int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const 
                                     ps);
                 if (e != cudaSuccess)
                     break;
-                rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, d_err + p0 * si.nw, d_w + p0, ps,
-                                       eng->tile_counter + 1 + i, nullptr, 0, round);
+                uint8_t *pack = err_view ? err_view + (c0 + p0) * (size_t)(si.n / 8) : nullptr;
+                rc = run_fused_counter(eng, key, d_cts + p0 * si.ct, pn, pack ? nullptr : d_err + p0 * si.nw,
+                                       d_w + p0, ps, eng->tile_counter + 1 + i, nullptr, 0, round, pack);
                 if (rc)
                     break;
-                e = cudaMemcpy2DAsync(h_err + (c0 + p0) * (si.n / 8), si.n / 8, d_err + p0 * si.nw, (size_t)si.nw * 4,
-                                      si.n / 8, pn, cudaMemcpyDeviceToHost, ps);
+                if (!pack)
+                    e = cudaMemcpy2DAsync(h_err + (c0 + p0) * (si.n / 8), si.n / 8, d_err + p0 * si.nw,
+                                          (size_t)si.nw * 4, si.n / 8, pn, cudaMemcpyDeviceToHost, ps);
                 if (e == cudaSuccess && h_weight)
                     e = cudaMemcpyAsync(h_weight + c0 + p0, d_w + p0, pn * 2, cudaMemcpyDeviceToHost, ps);
             }

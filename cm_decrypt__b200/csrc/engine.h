@@ -61,9 +61,11 @@ int run_fused_single(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, 
 // Explicit work counter and round schedule (balanced: -1 = the tuned choice,
 // 0 = full rounds, 1 = equal shares; round_cts > 0 overrides all three with
 // rounds of that many ciphertexts, a multiple of 32 from fused_round).
+// err_packed: or null, a device-writable view of rows of n/8 bytes back to
+// back (a host-mapped buffer the kernel fills directly).
 int run_fused_counter(cmd_engine *eng, const cmd_key *key, const uint8_t *d_cts, size_t count, uint32_t *d_err,
                       uint16_t *d_weight, cudaStream_t s, uint32_t *counter, uint16_t *d_pos, int balanced,
-                      uint32_t round_cts = 0);
+                      uint32_t round_cts = 0, uint8_t *err_packed = nullptr);
 // Ciphertexts per round of one launch over `count` ciphertexts of `set` under
 // the tuned schedule.
 uint32_t fused_round(cmd_engine *eng, int set, size_t count);

@@ -190,9 +190,52 @@ __device__ __forceinline__ void swap_layer(uint32_t *z, const uint32_t *__restri
     }
 }
 
+// Error row of n/8 bytes at byte address p (2-byte aligned), from the words
+// v[j] = row word lane + 32j: 32-bit stores to 4-byte aligned addresses (a
+// warp's store covers whole 128-byte lines), the row's odd 16-bit ends as
+// 16-bit stores.  For a row that starts 2 bytes into a word, every stored
+// word joins the upper half of row word k and the lower half of word k + 1
+// (the next lane's, or lane 0's next word).  Used for host-mapped outputs,
+// whose stores cross PCIe as they are made.
+template <int S>
+__device__ __forceinline__ void store_row_packed(uint8_t *p, const uint32_t *v, int lane)
+{
+    using F = FftDims<S>;
+    constexpr int R = F::R, RB = F::N / 8;  // row bytes (even for every set)
+    constexpr uint32_t FULL = 0xFFFFFFFFu;
+    static_assert(RB % 2 == 0, "rows of whole 16-bit units");
+    if ((((uintptr_t)p) & 3) == 0) {
+        uint32_t *o = reinterpret_cast<uint32_t *>(p);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int w = lane + 32 * j;
+            if (w < RB / 4)
+                o[w] = v[j];
+            else if ((RB & 2) && w == RB / 4)
+                *reinterpret_cast<uint16_t *>(p + 4 * w) = (uint16_t)v[j];
+        }
+    } else {
+        if (lane == 0)
+            *reinterpret_cast<uint16_t *>(p) = (uint16_t)v[0];
+        uint32_t *o = reinterpret_cast<uint32_t *>(p + 2);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            const int k = lane + 32 * j;
+            const uint32_t up = __shfl_down_sync(FULL, v[j], 1);
+            const uint32_t wrap = __shfl_sync(FULL, j + 1 < R ? v[j + 1 < R ? j + 1 : j] : 0u, 0);
+            const uint32_t nxt = lane == 31 ? wrap : up;
+            if (k < (RB - 2) / 4)
+                o[k] = (v[j] >> 16) | (nxt << 16);
+            else if ((RB & 2) == 0 && k == (RB - 2) / 4)
+                *reinterpret_cast<uint16_t *>(p + 2 + 4 * k) = (uint16_t)(v[j] >> 16);
+        }
+    }
+}
+
 // One warp: error row (and weight) of locator q from the converted array cv
 // (bitsliced, cv[s * CVS + k]).  fa: this warp's FA_WORDS words of shared
-// memory.  erow: NW words, or null.  prow: null, or t+1 u16 that receive the
+// memory.  erow: NW words, or null.  epack: null, or the row's n/8 bytes
+// packed (store_row_packed).  prow: null, or t+1 u16 that receive the
 // weight, the flagged positions in ascending order and 0xFFFF in the unused
 // slots (the weight never exceeds t: the reversed locator's leading
 // coefficient is C[0], which the update never zeroes).  Returns the weight
@@ -200,7 +243,7 @@ __device__ __forceinline__ void swap_layer(uint32_t *z, const uint32_t *__restri
 template <int S, int CVS>
 __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t *fa, const uint32_t *__restrict__ tw,
                                             const uint32_t *__restrict__ bctl, uint32_t *erow, uint16_t *prow,
-                                            int lane)
+                                            int lane, uint8_t *epack = nullptr)
 {
     using F = FftDims<S>;
     constexpr int M = F::M, D = F::D, NWD = F::NWD, R = F::R, NW = F::NW;
@@ -318,6 +361,8 @@ __device__ __forceinline__ int fft_root_one(const uint32_t *cv, int q, uint32_t 
             erow[w] = v[j];
         cnt += __popc(v[j]);
     }
+    if (epack)
+        store_row_packed<S>(epack, v, lane);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
         cnt += __shfl_xor_sync(FULL, cnt, off);

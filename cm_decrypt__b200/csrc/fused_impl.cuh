@@ -358,7 +358,8 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
         const uint64_t c = ct_index(rc, warp, q);
         uint32_t *erow = a.err ? a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride) : nullptr;
         uint16_t *prow = a.pos ? a.pos + c * (uint64_t)a.pos_stride : nullptr;
-        const int cnt = fft_root_one<S, M>(cv, q, fa, pl.tw, rc.key.bctl, erow, prow, lane);
+        uint8_t *epack = a.err_packed ? a.err_packed + c * (uint64_t)(Set<S>::N / 8) : nullptr;
+        const int cnt = fft_root_one<S, M>(cv, q, fa, pl.tw, rc.key.bctl, erow, prow, lane, epack);
         if (lane == 0 && a.weight)
             a.weight[c] = (uint16_t)cnt;
     }

@@ -111,6 +111,8 @@ struct FusedArgs {
     uint16_t *pos;                 // or null: per ciphertext t+1 u16, the weight
                                    // then the error positions ascending, 0xFFFF after
     uint32_t pos_stride;           // u16 per positions row
+    uint8_t *err_packed;           // or null: error rows of n/8 bytes back to back
+                                   // (a host-mapped buffer), row c at c * n/8
     FftPlanDev fft[NSETS];         // root-search plans, indexed by set
 };
 cudaError_t launch_fused(const FusedArgs &a, int grid, int warps_per_block, cudaStream_t s,

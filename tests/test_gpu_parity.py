@@ -273,6 +273,30 @@ def test_host_batch_in_pieces(oracle_mod, engine, keys, s):
     assert np.array_equal(cmd.decrypt_positions(engine, keys[s], cts), cmd.positions_from_errors(s, err))
 
 
+@pytest.mark.parametrize("s", [348864, 6960119, 8192128])
+def test_host_batch_into_pinned_rows(engine, keys, s):
+    """With pinned error rows, which the GPU can write, the pieces' kernels
+    store the packed rows straight into the caller's buffer.  The rows equal
+    the staged copy's, both from a 4-byte aligned start and from one 2 bytes
+    into a word (6960119's 870-byte rows alternate between the two), and no
+    byte outside the rows changes."""
+    pk = cmd.PubKey(s, golden_sk(s))
+    count = 4 * 8192 * 3 + 17
+    cts, planted, valid = pk.ciphertexts(seed=11, count=count, malformed_permille=100)
+    ref, w = cmd.decrypt(engine, keys[s], cts, path="fused")  # pageable rows: staged copies
+    assert np.array_equal(ref[valid == 1], planted[valid == 1])
+    rb = keys[s].info.err_bytes
+    base = torch.full((count * rb + 64,), 0xEE, dtype=torch.uint8).pin_memory().numpy()
+    for off in (16, 18):
+        base[:] = 0xEE
+        wts = np.zeros(count, np.uint16)
+        cmd._check(cmd.lib().cmd_decrypt_batch(engine.handle, keys[s].handle, cmd.PATHS["fused"], cts.ctypes.data,
+                                               count, base.ctypes.data + off, wts.ctypes.data), "cmd_decrypt_batch")
+        assert np.array_equal(base[off:off + count * rb].reshape(count, rb), ref)
+        assert (base[:off] == 0xEE).all() and (base[off + count * rb:] == 0xEE).all()
+        assert np.array_equal(wts, w)
+
+
 @pytest.mark.parametrize("s", SETS)
 def test_positions_output(oracle_mod, engine, keys, s):
     """cmd_decrypt_positions rows equal the positions of the packed error
