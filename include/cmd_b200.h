@@ -113,7 +113,11 @@ typedef enum { CMD_PATH_AUTO = 0, CMD_PATH_PLAIN = 1, CMD_PATH_FUSED = 2, CMD_PA
  * h_cts: count * ct_bytes, raw concatenation (the ct_<set>.bin layout).
  * h_err: count * err_bytes; bit i of vector c is set iff position i is flagged
  * (the reference's error_vector layout).  h_weight (may be NULL): flagged
- * positions per ciphertext.  Synchronous; host buffers may be pageable. */
+ * positions per ciphertext.  Synchronous; host buffers may be pageable.
+ * When h_err is pinned memory the GPU maps (cudaHostAlloc / cudaMallocHost,
+ * or registered with a device mapping; 2-byte aligned, all count * err_bytes
+ * in one allocation), batches of 65,536 ciphertexts or more have the kernels
+ * store the rows into it directly while they run, with no copy after them. */
 int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path,
                       const uint8_t *h_cts, size_t count, uint8_t *h_err,
                       uint16_t *h_weight);
