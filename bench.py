@@ -356,7 +356,7 @@ def _time_stream(fn, stream, reps: int, warmup: int) -> float:
     return e0.elapsed_time(e1) / reps
 
 
-def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3) -> dict:
+def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3, int_peak: float = 0.0) -> dict:
     """All five parameter sets in turn, `count` ciphertexts of one
     seeded key (the reference kem/ key of the set), autotuned fused kernel
     replayed as a CUDA graph; every output checked against its planted error
@@ -382,6 +382,10 @@ def config_all_sets(cmd, eng, stream, count: int = 1 << 20, reps: int = 3) -> di
                   and (d_w.cpu().numpy().view(np.uint16) == info.t).all())
         row = {"ciphertexts": count, "fused_ms": ms, "fused_decaps_per_s": count / (ms * 1e-3),
                "tuned": tuned, "results_match_planted": ok}
+        if int_peak:
+            # the executed algorithm's lane-ops at this rate against the measured lop3 rate
+            from cm_decrypt__b200.roofline import work_per_decap
+            row["roofline_frac"] = count / (ms * 1e-3) * work_per_decap(s)["total"] / int_peak
         if s == SET:
             msp = _time_stream(lambda: cmd.decrypt_device(eng, key, d_ct.data_ptr(), count, d_err.data_ptr(),
                                                           d_w.data_ptr(), sp, "plain"), stream, 1, 1)
@@ -823,7 +827,7 @@ def main() -> None:
     if world == 1 and not args.no_reference_gpu:
         line["reference_gpu"] = reference_gpu_leg(cmd, eng, key, stream)
     if world == 1 and not args.no_configs:
-        line["configs"] = {"all_sets_2^20": config_all_sets(cmd, eng, stream),
+        line["configs"] = {"all_sets_2^20": config_all_sets(cmd, eng, stream, int_peak=int_peak),
                            "mixed_64keys_2^18": config_mixed(cmd, eng, stream,
                                                              reference_check=not args.no_reference_check)}
     for g_ in graphs:

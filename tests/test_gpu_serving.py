@@ -19,6 +19,26 @@ from conftest import SETS, golden_sk, rng
 pytestmark = pytest.mark.gpu
 
 
+def test_tune_per_sample_size(engine):
+    """A tuning for a given batch size is cached apart from the default one,
+    so tuning at the batch a caller runs does not replace the default choice
+    (the winners differ: at 65,536 ciphertexts how the batch fills whole
+    rounds decides)."""
+    s = 6960119
+    key = cmd.Key(engine, s, golden_sk(s))
+    try:
+        sized = cmd.tune(engine, key, sample_count=65536, force=True)
+        default = cmd.tune(engine, key, force=True)
+        again = cmd.tune(engine, key, sample_count=65536)  # from the cache, keyed by the size
+        assert (again["wpb"], again["balanced"]) == (sized["wpb"], sized["balanced"])
+        assert again["ns_per_ct"] == pytest.approx(sized["ns_per_ct"], rel=1e-3)
+        back = cmd.tune(engine, key)
+        assert (back["wpb"], back["balanced"]) == (default["wpb"], default["balanced"])
+        assert back["ns_per_ct"] == pytest.approx(default["ns_per_ct"], rel=1e-3)
+    finally:
+        key.free()
+
+
 def test_tune_and_graph_replay(engine):
     s = 6960119
     key = cmd.Key(engine, s, golden_sk(s))
