@@ -80,6 +80,11 @@ struct RequestQueue {
     bool empty() const { return head == v.size(); }
     const Request &front() const { return v[head]; }
     void push_back(const Request &r) { v.push_back(r); }
+    Request &emplace_back()  // a new request at the back, filled in place by the caller
+    {
+        v.emplace_back();
+        return v.back();
+    }
     // Moves the oldest `take` requests into out (whose old contents are dropped).
     void take_front(size_t take, std::vector<Request> &out)
     {
@@ -762,7 +767,7 @@ int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8
         const size_t before = srv->pending.size();
         const uint64_t now = t_arrive ? 0 : now_ns();
         for (; k < n && srv->pending.size() < srv->cfg.queue_capacity; k++) {
-            Request r;
+            Request &r = srv->pending.emplace_back();
             r.key_id = key_ids[k];
             r.tag = tags ? tags[k] : k;
             r.err_out = h_err_base ? h_err_base + k * err_stride : nullptr;
@@ -773,7 +778,6 @@ int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8
             r.t_arrive = t_arrive ? t_arrive[k] : now;
             if (srv->submitted++ == 0)
                 srv->t_first = r.t_arrive;
-            srv->pending.push_back(r);
         }
         srv->refused += n - k;
         // The dispatcher waits for a first request or for a full batch: only
@@ -1029,9 +1033,7 @@ int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *
     std::exponential_distribution<double> gap(rate_per_s);
     constexpr size_t GROUP = 4096;
     std::vector<uint32_t> g_key(GROUP);
-    std::vector<uint64_t> g_tag(GROUP), g_t(GROUP);
-    std::vector<uint8_t> g_ct(GROUP * CT_STRIDE);
-    std::vector<uint8_t *> g_err(GROUP);
+    std::vector<uint64_t> g_tag(GROUP), g_t(GROUP), g_row(GROUP);
     const uint64_t t0 = now_ns();
     const uint64_t t_end = t0 + (uint64_t)(seconds * 1e9);
     double next = (double)t0 + gap(rng) * 1e9;
@@ -1047,24 +1049,23 @@ int cmd_server_loadgen(cmd_server *srv, const uint32_t *key_ids, const uint8_t *
             g_key[g] = key_ids[k];
             g_tag[g] = i;
             g_t[g] = (uint64_t)next;
-            memcpy(g_ct.data() + g * CT_STRIDE, cts + k * ct_stride, std::min<size_t>(ct_stride, CT_STRIDE));
-            g_err[g] = err_pool ? err_pool + k * err_stride : nullptr;
+            g_row[g] = k;
             g++;
             i++;
             next += gap(rng) * 1e9;
         }
-        // one lock per group; outputs are scattered, so queue one by one
-        // inside it through the group call per request run of the pool
+        // one group call per run of consecutive pool rows (ciphertexts and
+        // result rows both straight from the pool: no staging copy)
         size_t acc = 0;
         for (size_t a = 0; a < g;) {
-            // consecutive requests whose result rows are consecutive pool rows
             size_t b = a + 1;
-            while (b < g && err_pool && g_err[b] == g_err[b - 1] + err_stride)
+            while (b < g && g_row[b] == g_row[b - 1] + 1)
                 b++;
             size_t got = 0;
-            const int rc = submit_group(srv, b - a, g_key.data() + a, g_ct.data() + a * CT_STRIDE, CT_STRIDE,
-                                        g_err[a], err_pool ? err_stride : 0, g_tag.data() + a, g_t.data() + a,
-                                        &got);
+            const size_t k = g_row[a];
+            const int rc = submit_group(srv, b - a, g_key.data() + a, cts + k * ct_stride, ct_stride,
+                                        err_pool ? err_pool + k * err_stride : nullptr, err_pool ? err_stride : 0,
+                                        g_tag.data() + a, g_t.data() + a, &got);
             if (rc != CMD_OK)
                 return rc;
             acc += got;
