@@ -817,6 +817,13 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
         return CMD_E_BUDGET;
     }
     srv->slots.resize(cfg->slots);
+    // The request buffers circulate between the queue and the slots; giving
+    // each a batch's capacity up front keeps their growth (a copy of every
+    // queued request, under the queue lock) out of the first seconds at a
+    // higher load.
+    srv->pending.v.reserve(cfg->max_batch);
+    for (auto &sl : srv->slots)
+        sl.reqs.reserve(cfg->max_batch);
     cudaError_t e = cudaMallocHost((void **)&srv->done_seq, 16 * sizeof(uint64_t));
     if (e == cudaSuccess)
         memset((void *)srv->done_seq, 0, 16 * sizeof(uint64_t));
