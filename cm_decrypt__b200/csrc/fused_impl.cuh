@@ -49,7 +49,7 @@
 namespace cmd {
 
 constexpr uint32_t FULLMASK = 0xFFFFFFFFu;
-constexpr int TAB_ROWS = 16;  // syndrome-table rows per staged chunk
+constexpr int GROUP_ROWS = 4;  // syndrome-table rows combined per step (16 XOR combinations)
 
 __host__ __device__ constexpr int cmax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int al16(int x) { return (x + 15) / 16 * 16; }
@@ -67,7 +67,12 @@ template <int S> struct Fz {
     static constexpr int A_B = al16(cmax(cmax(RAW_B + 16, RING_B + CM_B), FA_B));
     static constexpr int S_B = al16(2 * T * M * 4);  // bitsliced syndromes / locator
     static constexpr int WARP_B = A_B + S_B;
-    static constexpr int TAB_B = TAB_ROWS * TWD * 4;  // one chunk buffer
+    static constexpr int NWU = (2 * T * M + 31) / 32;  // syndrome accumulator words in use
+    static constexpr int CS = NWU | 1;  // combination row stride: odd, so the 16 rows lanes pick meet distinct banks
+    // the CTA's syndrome region: two staged groups of table rows, then the
+    // group's 16 XOR combinations
+    static constexpr int SYN_B = al16((2 * GROUP_ROWS * TWD + 16 * CS) * 4);
+    static_assert(P::SB % GROUP_ROWS == 0, "whole groups of ciphertext bits");
     static_assert(NX * M * 4 <= S_B, "conversion array must fit the syndrome region");
 };
 
@@ -116,7 +121,7 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     const int ntile = rem < 0 ? 0 : (rem > 32 ? 32 : rem);
 
     uint32_t *tabbuf = reinterpret_cast<uint32_t *>(smem);
-    uint8_t *wbase = smem + 2 * Z::TAB_B + warp * Z::WARP_B;
+    uint8_t *wbase = smem + Z::SYN_B + warp * Z::WARP_B;
     uint8_t *raw = wbase;                                            // phase 1-2
     uint32_t *ring = reinterpret_cast<uint32_t *>(wbase);            // phase 4
     uint32_t *fa = reinterpret_cast<uint32_t *>(wbase);              // phase 5
@@ -152,52 +157,62 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     // The key's dense table: row b holds the 2t values L_b^j / g(L_b)^2 as m
     // bits each, back to back (bit j*m + k = bit k of value j), so lane q's
     // accumulator word w holds bits 32w .. 32w+31 of ciphertext q's 2t*m
-    // syndrome bits.
-    constexpr int NWU = (2 * T * M + 31) / 32;  // accumulator words in use
+    // syndrome bits.  The rows go in groups of four: the CTA forms the 16
+    // XOR combinations of a group once (combination x = the rows whose bit is
+    // set in x), and each lane adds the one its ciphertext's four bits select
+    // -- one load and one XOR per word instead of four masked XORs.  Rows of
+    // the next group are staged by cp.async meanwhile.
+    constexpr int NWU = Z::NWU, CS = Z::CS, G = GROUP_ROWS;
+    constexpr int NG = P::SB / G;
     uint32_t acc[NWU];
 #pragma unroll
     for (int w = 0; w < NWU; w++)
         acc[w] = 0;
-    constexpr int NCHUNK = P::SB / TAB_ROWS;
-    constexpr int CHUNK_V = TAB_ROWS * TWD / 4;  // 16-byte pieces per chunk
-    {
-        const uint32_t *src = tab;
-        for (int v = tid; v < CHUNK_V; v += WPB * 32)
-            cp_async16(tabbuf + 4 * v, src + 4 * v);
+    uint32_t *comb = tabbuf + 2 * G * TWD;  // [16][CS]
+    auto stage = [&](int g) {  // rows of group g into buffer g & 1: TWD 16-byte pieces
+        if (tid < TWD)
+            cp_async16(tabbuf + (g & 1) * G * TWD + 4 * tid, tab + (size_t)g * G * TWD + 4 * tid);
         cp_async_commit();
-    }
+    };
+    stage(0);
     const uint8_t *myct = raw + lane * P::CT;
     uint32_t ctw = 0;
-    for (int c = 0; c < NCHUNK; c++) {
-        if (c + 1 < NCHUNK) {
-            const uint32_t *src = tab + (size_t)(c + 1) * TAB_ROWS * TWD;
-            uint32_t *dst = tabbuf + ((c + 1) & 1) * TAB_ROWS * TWD;
-            for (int v = tid; v < CHUNK_V; v += WPB * 32)
-                cp_async16(dst + 4 * v, src + 4 * v);
-            cp_async_commit();
-            cp_async_wait<1>();
-        } else {
-            cp_async_wait<0>();
-        }
-        __syncthreads();
-        const uint32_t *buf = tabbuf + (c & 1) * TAB_ROWS * TWD;
 #pragma unroll 1
-        for (int r = 0; r < TAB_ROWS; r++) {
-            const int b = c * TAB_ROWS + r;
-            if ((b & 31) == 0)
-                ctw = ld_u32_any(myct + (b >> 3));
-            const uint32_t mask = (uint32_t)((int32_t)(ctw << (31 - (b & 31))) >> 31);
-            const uint4 *row = reinterpret_cast<const uint4 *>(buf + r * TWD);
-#pragma unroll
-            for (int v = 0; v < TWD / 4; v++) {
-                const uint4 x = row[v];
-                if (4 * v + 0 < NWU) acc[4 * v + 0] ^= x.x & mask;
-                if (4 * v + 1 < NWU) acc[4 * v + 1] ^= x.y & mask;
-                if (4 * v + 2 < NWU) acc[4 * v + 2] ^= x.z & mask;
-                if (4 * v + 3 < NWU) acc[4 * v + 3] ^= x.w & mask;
-            }
+    for (int g = 0; g < NG; g++) {
+        cp_async_wait<0>();
+        __syncthreads();  // group g's rows are in; every lane is done with group g-1's combinations
+        if (g + 1 < NG)
+            stage(g + 1);
+        if (tid < NWU) {
+            const uint32_t *rows = tabbuf + (g & 1) * G * TWD + tid;
+            const uint32_t r0 = rows[0], r1 = rows[TWD], r2 = rows[2 * TWD], r3 = rows[3 * TWD];
+            const uint32_t c3 = r0 ^ r1, c5 = r2 ^ r0, c6 = r2 ^ r1, c7 = r2 ^ c3;
+            uint32_t *o = comb + tid;
+            o[0 * CS] = 0u;
+            o[1 * CS] = r0;
+            o[2 * CS] = r1;
+            o[3 * CS] = c3;
+            o[4 * CS] = r2;
+            o[5 * CS] = c5;
+            o[6 * CS] = c6;
+            o[7 * CS] = c7;
+            o[8 * CS] = r3;
+            o[9 * CS] = r3 ^ r0;
+            o[10 * CS] = r3 ^ r1;
+            o[11 * CS] = r3 ^ c3;
+            o[12 * CS] = r3 ^ r2;
+            o[13 * CS] = r3 ^ c5;
+            o[14 * CS] = r3 ^ c6;
+            o[15 * CS] = r3 ^ c7;
         }
-        __syncthreads();
+        __syncthreads();  // the combinations are in
+        const int b = g * G;  // a multiple of 4: the group's bits share one ciphertext word
+        if ((b & 31) == 0)
+            ctw = ld_u32_any(myct + (b >> 3));
+        const uint32_t *pick = comb + ((ctw >> (b & 31)) & 15u) * CS;
+#pragma unroll
+        for (int w = 0; w < NWU; w++)
+            acc[w] ^= pick[w];
     }
     if (ntile == 0)
         return;  // no work for this warp in this round (the CTA-wide part is done)
@@ -403,7 +418,7 @@ __global__ void __launch_bounds__(WPB * 32, 1) k_fused(FusedArgs a)
     }
 }
 
-template <int S> constexpr size_t fz_smem(int wpb) { return 2 * (size_t)Fz<S>::TAB_B + (size_t)wpb * Fz<S>::WARP_B; }
+template <int S> constexpr size_t fz_smem(int wpb) { return (size_t)Fz<S>::SYN_B + (size_t)wpb * Fz<S>::WARP_B; }
 
 size_t smem_limit_bytes();
 

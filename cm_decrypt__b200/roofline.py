@@ -7,7 +7,11 @@ so every figure below is bit operations / 32 ("lane-ops").
 
 Work of the algorithm the fused kernel executes, per decryption:
 
-  W_synd = sb * 2t * m / 32                      masked XOR of table rows
+  W_synd = (sb / 4) * (NWU + 11 * NWU / 256)
+           the dense table in groups of four rows: the CTA forms the group's
+           16 XOR combinations (11 word XORs per accumulator word, shared by
+           the 256 ciphertexts of a full round), and each ciphertext adds the
+           one its four bits select (NWU = ceil(2tm / 32) words)
   W_bm   = [sum_{N<2t} (min(N, t, L_N) + 1) + 2 sum_{N<2t} (min(L_{N+1}, t) + 1)]
            * (m^2 + R_m) / 32
            (the scaled, L-bounded Berlekamp-Massey: discrepancy terms up to
@@ -23,20 +27,18 @@ Work of the algorithm the fused kernel executes, per decryption:
 ``achieved = decaps/s * (W_synd + W_bm + W_root)`` lane-ops/s against the
 measured lop3 rate.
 
-The fixed yardstick of the reference's algorithm (Horner at every support
-point, root_13.c:216-240) is kept beside it:
+The fixed yardstick of the reference's algorithm is kept beside it, as the
+work table of the decrypt path's scope defines it:
 
-  W_chien = n * t * (m^2 + R_m + m) / 32
+  W_synd_table = sb * 2t * m / 32            masked XOR of every set bit's row
+  W_bm_ref     = [sum_{N<2t} (min(N,t) + 1) + 2t(t+1) + 8 * 2t] * (m^2 + R_m) / 32
+                 (bm()'s discrepancy and update multiplies, each step's d/b as
+                 eight multiply-equivalents)
+  W_chien      = n * t * (m^2 + R_m + m) / 32   Horner at every support point
+                 (root_13.c:216-240)
 
-The plain per-stage kernels are measured against the work of the
-reference's own algorithm for each stage:
-
-  synd          W_synd as above (sum of table rows)
-  bm            the reference bm()'s multiplies: sum_{N<2t} (min(N,t) + 1)
-                discrepancy terms, t+1 updates per step, and the d/b of each
-                step as 8 multiply-equivalents (an inversion chain), each
-                multiply m^2 + R_m + m bit operations
-  root          W_chien (Horner at every support point)
+The plain per-stage kernels, which run the reference's algorithm, are
+measured against those three, stage by stage.
 
 Bytes per decryption that must cross HBM: the ciphertext in and the n-bit
 error vector out.
@@ -45,6 +47,7 @@ from __future__ import annotations
 
 SETS = {348864: (12, 3488, 64, 96), 460896: (13, 4608, 96, 156), 6688128: (13, 6688, 128, 208),
         6960119: (13, 6960, 119, 194), 8192128: (13, 8192, 128, 208)}
+ROUND_CTS = 256  # ciphertexts sharing one CTA's combinations (8 warps of 32)
 
 
 def fft_depth(t: int) -> int:
@@ -59,25 +62,26 @@ def work_per_decap(set_id: int) -> dict:
     r = 22 if m == 12 else 48
     mul = m * m + r
     sb = 8 * ct
-    w_synd = sb * 2 * t * m / 32
+    nwu = (2 * t * m + 31) // 32
+    w_synd = sb / 4 * (nwu + 11 * nwu / ROUND_CTS)
     disc = sum(min(N, t, (N + 1) // 2) + 1 for N in range(2 * t))
     upd = sum(min((N + 2) // 2, t) + 1 for N in range(2 * t))
     w_bm = (disc + 2 * upd) * mul / 32
     D = fft_depth(t)
     w_root = ((D - 1) * (1 << D) * mul + (1 << (D - 2)) * m * D * (D - 1)
               + D * (1 << (m - 1)) * (mul + 2 * m) + (1 << m) * m + (2 * m - 1) * (1 << (m - 1)) * 3) / 32
-    w_chien = n * t * (mul + m) / 32
+    ys = sb * 2 * t * m / 32
+    yb = (sum(min(N, t) + 1 for N in range(2 * t)) + 2 * t * (t + 1) + 16 * t) * mul / 32
+    yc = n * t * (mul + m) / 32
     return {"synd": w_synd, "bm": w_bm, "root_fft": w_root, "total": w_synd + w_bm + w_root,
-            "yardstick_chien": w_chien, "yardstick_total": w_synd + w_bm + w_chien}
+            "yardstick_synd_table": ys, "yardstick_bm_ref": yb, "yardstick_chien": yc,
+            "yardstick_total": ys + yb + yc}
 
 
 def plain_stage_work(set_id: int) -> dict:
     """Lane-ops per decryption of the reference algorithm of each plain stage."""
-    m, n, t, ct = SETS[set_id]
-    r = 22 if m == 12 else 48
     w = work_per_decap(set_id)
-    muls = sum(min(N, t) + 1 for N in range(2 * t)) + 2 * t * (t + 1) + 16 * t
-    return {"synd": w["synd"], "bm": muls * (m * m + r + m) / 32, "root": w["yardstick_chien"]}
+    return {"synd": w["yardstick_synd_table"], "bm": w["yardstick_bm_ref"], "root": w["yardstick_chien"]}
 
 
 def hbm_bytes_per_decap(set_id: int) -> int:
