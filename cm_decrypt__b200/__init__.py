@@ -148,6 +148,7 @@ def lib() -> ctypes.CDLL:
         "cmd_server_add_key": (_i32, [_vp, _i32, _vp, _sz, ctypes.POINTER(ctypes.c_uint32)]),
         "cmd_server_submit": (_i32, [_vp, ctypes.c_uint32, _vp, _vp, _u64]),
         "cmd_server_submit_many": (_i32, [_vp, _sz, _vp, _vp, _sz, _vp, _sz, _vp, ctypes.POINTER(_sz)]),
+        "cmd_server_register_rows": (_i32, [_vp, _vp, _sz]),
         "cmd_server_poll": (_i32, [_vp, ctypes.POINTER(Completion), _sz, ctypes.POINTER(_sz), ctypes.c_uint32]),
         "cmd_server_drain": (_i32, [_vp, ctypes.c_uint32]),
         "cmd_server_stats_get": (_i32, [_vp, ctypes.POINTER(ServerStats), _i32]),
@@ -359,11 +360,13 @@ class Server:
         _check(lib().cmd_server_create(engine.handle, ctypes.byref(cfg), ctypes.byref(h)), "cmd_server_create")
         self.handle = h
         self.key_sets: list[int] = []
+        self._rows: list[np.ndarray] = []  # registered row memory, kept alive until close()
 
     def close(self) -> None:
         if self.handle:
             lib().cmd_server_destroy(self.handle)
             self.handle = None
+        self._rows = []
 
     def __enter__(self):
         return self
@@ -378,6 +381,15 @@ class Server:
                "cmd_server_add_key")
         self.key_sets.append(set_id)
         return kid.value
+
+    def register_rows(self, rows: np.ndarray) -> None:
+        """Result rows inside `rows` (a C-contiguous array, kept alive by the
+        server until close()) are stored there by the GPU itself on the
+        latency kernels' path (cmd_server_register_rows)."""
+        if not rows.flags.c_contiguous:
+            raise ValueError("register_rows needs a C-contiguous array")
+        _check(lib().cmd_server_register_rows(self.handle, _ptr(rows), rows.nbytes), "cmd_server_register_rows")
+        self._rows.append(rows)
 
     def submit(self, key_id: int, ct: np.ndarray, err_out: np.ndarray | None, tag: int) -> int:
         """Returns CMD_OK or CMD_E_BUSY; err_out must stay alive until completion."""

@@ -475,27 +475,13 @@ int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t
     return run_fused_single(eng, key, d_cts, count, d_err, d_weight, s);
 }
 
-}  // namespace cmd
-
-extern "C" {
-
-int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
-                       uint32_t *d_err, uint16_t *d_weight, void *stream)
-{
-    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_err)) || path < 0 || path > 3)
-        return CMD_E_ARG;
-    cudaSetDevice(eng->device);
-    std::lock_guard<std::mutex> lk(eng->mu);
-    return run_device(eng, key, path, d_cts, count, d_err, d_weight, stream ? (cudaStream_t)stream : eng->stream);
-}
-
 // A device address through which kernels can write the host range [h, h +
 // bytes), or null: pinned memory the GPU maps (cudaHostAlloc / cudaMallocHost
 // memory under unified addressing, or registered memory with a device
 // mapping), 2-byte aligned, whose first and last bytes map to one contiguous
 // device range.  Anything else (pageable memory, a range running past its
 // pinned allocation) gives null, and the caller copies through staging.
-static uint8_t *device_view(uint8_t *h, size_t bytes)
+uint8_t *device_view(uint8_t *h, size_t bytes)
 {
     if (!h || !bytes || (((uintptr_t)h) & 1))
         return nullptr;
@@ -511,6 +497,21 @@ static uint8_t *device_view(uint8_t *h, size_t bytes)
     }
     return static_cast<uint8_t *>(a0.devicePointer);
 }
+
+}  // namespace cmd
+
+extern "C" {
+
+int cmd_decrypt_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,
+                       uint32_t *d_err, uint16_t *d_weight, void *stream)
+{
+    if (!eng || !key || key->eng != eng || (count && (!d_cts || !d_err)) || path < 0 || path > 3)
+        return CMD_E_ARG;
+    cudaSetDevice(eng->device);
+    std::lock_guard<std::mutex> lk(eng->mu);
+    return run_device(eng, key, path, d_cts, count, d_err, d_weight, stream ? (cudaStream_t)stream : eng->stream);
+}
+
 
 int cmd_decrypt_batch(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *h_cts, size_t count,
                       uint8_t *h_err, uint16_t *h_weight)

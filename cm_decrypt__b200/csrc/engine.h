@@ -52,6 +52,9 @@ int cuda_fail(cudaError_t e, const char *what);
 int kg_pubkey_columns(cmd_engine *eng, int set, const uint16_t *d_L, const uint16_t *d_g, uint32_t *d_cols, int cwp);
 bool valid_set(int set);
 bool budget_take(cmd_engine *eng, size_t bytes);
+// Device address of GPU-mapped host memory [h, h + bytes) (2-byte aligned,
+// one contiguous mapping), or null.
+uint8_t *device_view(uint8_t *h, size_t bytes);
 void budget_give(cmd_engine *eng, size_t bytes);
 
 int run_device(cmd_engine *eng, const cmd_key *key, cmd_path path, const uint8_t *d_cts, size_t count,

@@ -11,10 +11,12 @@
 //     is one aligned slab);
 //  2. syndrome (util.c:102-114): lane q accumulates the 2t syndromes of
 //     ciphertext q, m bits each back to back; the key's dense syndrome table
-//     streams through shared memory in 16-row chunks (cp.async double
-//     buffer, shared by all warps) and each row is masked by the ciphertext
-//     bit, never branched on;
-//  3. ballot-transpose the syndromes to bitsliced form (bit q = ciphertext q);
+//     streams through shared memory four rows at a time (cp.async double
+//     buffer, shared by all warps), the CTA forms the 16 XOR combinations of
+//     each four rows, and each lane adds the combination its ciphertext's
+//     four bits select (a read indexed by public ciphertext bits only);
+//  3. transpose the syndromes to bitsliced form (bit q = ciphertext q) by a
+//     shuffle butterfly;
 //  4. Berlekamp-Massey (bm.c:12-68) bitsliced across the 32 ciphertexts: lane
 //     l owns locator coefficients l, l+32, ... (kept in shared memory, so the
 //     per-step loop over them stays rolled and small), the discrepancy is a

@@ -126,6 +126,7 @@ struct LatItem {
     uint32_t err_off;     // word offset of the error row in the batch
     int32_t set;
     int32_t pad;
+    uint8_t *row;         // or the packed n/8-byte error row, stored here (GPU-mapped host memory)
 };
 // Tile path: ntiles tiles of 32 item slots (LatItem.pad = tile count, padding
 // slots set -1).  d_scratch holds ntiles * TILE_SCRATCH_WORDS words: each

@@ -55,7 +55,7 @@ namespace {
 constexpr uint32_t FULL = 0xFFFFFFFFu;
 }
 
-static_assert(sizeof(LatItem) == 32, "LatItem layout");
+static_assert(sizeof(LatItem) == 40, "LatItem layout");
 
 template <int S> struct TsDims {
     using F = FftDims<S>;
@@ -480,7 +480,13 @@ __device__ __forceinline__ void root_tile(const LatItem &it, const uint32_t *cv,
 {
     static_assert(FftDims<S>::FA_WORDS <= ROOT_FA_WORDS, "root array");
     const int lane = threadIdx.x & 31;
-    const int cnt = fft_root_one<S, 16>(cv, q, fa, pl.tw, it.bctl, err + it.err_off, nullptr, lane);
+    // The row goes to the batch's error rows, or packed straight into the
+    // request's own (host) buffer; the fence makes those stores visible to the
+    // host before anything the stream writes after this kernel.
+    const int cnt = fft_root_one<S, 16>(cv, q, fa, pl.tw, it.bctl, it.row ? nullptr : err + it.err_off, nullptr,
+                                        lane, it.row);
+    if (it.row)
+        __threadfence_system();
     if (lane == 0 && weight)
         *weight = (uint16_t)cnt;
 }
@@ -530,7 +536,7 @@ __global__ void k_tile_items(LatItem *__restrict__ items, uint32_t count, const 
         return;
     const uint32_t t = slot >> 5, q = slot & 31, left = count - 32 * t;
     const uint32_t cnt = left < 32 ? left : 32;
-    items[slot] = LatItem{wfft, bctl, slot * ct_bytes, slot * nw, q < cnt ? set : -1, (int32_t)cnt};
+    items[slot] = LatItem{wfft, bctl, slot * ct_bytes, slot * nw, q < cnt ? set : -1, (int32_t)cnt, nullptr};
 }
 
 // The syndromes of every ciphertext of a tile as rows of 2t u16 (the

@@ -23,7 +23,9 @@
 //    the results, so the watch is plain loads, not CUDA calls), takes
 //    whichever finishes first, copies each result to its request's
 //    buffer (large batches split across a few copy threads) and records
-//    arrival-to-completion latency for the p50/p99 statistics.
+//    arrival-to-completion latency for the p50/p99 statistics.  A buffer in
+//    memory registered with cmd_server_register_rows needs no copy: the tile
+//    path's root kernel stores the row there itself.
 //  * Host work per request is O(1): the queue is a vector whose buffers
 //    circulate between the queue and the slots (no allocation per request),
 //    keys are marked once per batch by generation stamp, and the tile path
@@ -66,6 +68,7 @@ struct Request {
     int32_t set;  // the key's set, fixed when the request is queued
     uint64_t tag;
     uint8_t *err_out;
+    uint8_t *err_dev;  // device address of err_out when it lies in a registered row range, else null
     uint64_t t_arrive;
     uint8_t ct[CT_STRIDE];
 };
@@ -210,6 +213,7 @@ struct Slot {
     std::vector<uint32_t> slot_of;      // request i -> result row (item slot)
     size_t rows_used = 0;               // result rows to copy back
     uint32_t *d_counter = nullptr;
+    bool rows_direct = false;           // every row went straight to its request's buffer: no row copy
     std::vector<Request> reqs;  // taken from the queue (a buffer swap when a batch takes it all)
     uint64_t gen = 0;          // generation of the batch in this slot (its keys carry it)
     uint64_t seq = 0;          // sequence number of the batch in this slot (from 1)
@@ -297,6 +301,15 @@ struct cmd_server {
     // 8-byte copy), so the completer sees a finished batch with plain loads
     volatile uint64_t *done_seq = nullptr;
     std::deque<cmd_completion> completions;
+    // Caller memory registered for result rows (cmd_server_register_rows):
+    // requests whose row lies inside one get it stored by the tile path's
+    // root kernel itself.  Appended under mu, read by submitters under mu.
+    struct RowRange {
+        uint8_t *host, *dev;
+        size_t bytes;
+        bool registered_here;  // pinned by cmd_server_register_rows: unregistered at destroy
+    };
+    std::vector<RowRange> row_ranges;
     std::thread dispatcher, completer;
     std::unique_ptr<CopyPool> copiers;
     bool stop = false;
@@ -313,6 +326,17 @@ struct cmd_server {
     uint64_t tick = 0;
     uint64_t completions_gen = 0;  // bumped each time a batch completes
 
+    // Device address of a result row [p, p + bytes) inside a registered range
+    // (2-byte aligned, as the kernels' packed row stores need), or null.
+    uint8_t *row_device(uint8_t *p, size_t bytes) const
+    {
+        if (((uintptr_t)p) & 1)
+            return nullptr;
+        for (const RowRange &rr : row_ranges)
+            if (p >= rr.host && (size_t)(p - rr.host) + bytes <= rr.bytes)
+                return rr.dev + (p - rr.host);
+        return nullptr;
+    }
     void dispatch_loop();
     void complete_loop();
     int ensure_key(uint32_t id);
@@ -470,6 +494,7 @@ int cmd_server::launch(Slot &sl)
             tile0[st] = ntiles;
             ntiles += (cnt[st] + 31) / 32;
         }
+        size_t direct = 0;
         for (size_t i = 0; i < B; i++) {
             const Request &r = sl.reqs[i];
             const uint32_t pos = next[r.set]++;
@@ -477,15 +502,17 @@ int cmd_server::launch(Slot &sl)
             const uint32_t left = cnt[r.set] - pos / 32 * 32;
             const KeyDev &kd = keys[r.key_id].key->dev;
             items[slot] = LatItem{kd.wfft, kd.bctl, (uint32_t)(i * CT_STRIDE), slot * ERR_STRIDE, r.set,
-                                  (int32_t)(left < 32 ? left : 32)};
+                                  (int32_t)(left < 32 ? left : 32), r.err_dev};
+            direct += r.err_dev != nullptr;
             sl.slot_of[i] = slot;
         }
         for (int st = 0; st < NSETS; st++)
             for (uint32_t pos = cnt[st]; pos % 32; pos++) {  // the set's last tile, past its count
                 const uint32_t slot = 32 * (tile0[st] + pos / 32) + pos % 32;
-                items[slot] = LatItem{nullptr, nullptr, 0, slot * ERR_STRIDE, -1, (int32_t)(cnt[st] % 32)};
+                items[slot] = LatItem{nullptr, nullptr, 0, slot * ERR_STRIDE, -1, (int32_t)(cnt[st] % 32), nullptr};
             }
         sl.rows_used = (size_t)ntiles * 32;
+        sl.rows_direct = direct == B;
         if ((e = cudaMemcpyAsync(sl.d_in + lay.cts, sl.h_in + lay.cts, B * CT_STRIDE, cudaMemcpyHostToDevice, s)) !=
                 cudaSuccess ||
             (e = cudaMemcpyAsync(sl.d_in + lay.items, sl.h_in + lay.items, lay.seq + 8 - lay.items,
@@ -555,10 +582,13 @@ int cmd_server::launch(Slot &sl)
         if ((e = launch_fused(a, grid, wpb, s, lc)) != cudaSuccess)
             return cuda_fail(e, "server fused launch");
     }
-    if (sl.fused)
+    if (sl.fused) {
         sl.rows_used = B;
-    if ((e = cudaMemcpyAsync(sl.h_err, sl.d_err, sl.rows_used * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) !=
-            cudaSuccess ||
+        sl.rows_direct = false;  // the fused kernel's rows take the staged copy
+    }
+    if ((!sl.rows_direct &&
+         (e = cudaMemcpyAsync(sl.h_err, sl.d_err, sl.rows_used * ERR_STRIDE * 4, cudaMemcpyDeviceToHost, s)) !=
+             cudaSuccess) ||
         (e = cudaMemcpyAsync(sl.h_w, sl.d_w, sl.rows_used * 2, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (e = cudaEventRecord(sl.done, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync((void *)(done_seq + (&sl - slots.data())), sl.d_in + lay.seq, 8, cudaMemcpyDeviceToHost,
@@ -710,7 +740,8 @@ void cmd_server::complete_loop()
             const size_t end = std::min(B, (c + 1) * CHUNK);
             for (size_t i = c * CHUNK; i < end; i++) {
                 const Request &r = sl.reqs[i];
-                if (e == cudaSuccess && r.err_out)
+                // (a tile-path row in registered memory is already there)
+                if (e == cudaSuccess && r.err_out && (sl.fused || !r.err_dev))
                     memcpy(r.err_out, sl.h_err + (size_t)sl.slot_of[i] * ERR_STRIDE, set_info(r.set).n / 8);
                 const uint64_t lat = t - r.t_arrive;
                 sl.lats[i] = (uint32_t)std::min<uint64_t>(lat, 0xFFFFFFFFu);
@@ -772,6 +803,7 @@ int submit_group(cmd_server *srv, size_t n, const uint32_t *key_ids, const uint8
             r.tag = tags ? tags[k] : k;
             r.err_out = h_err_base ? h_err_base + k * err_stride : nullptr;
             r.set = srv->key_sets[r.key_id];
+            r.err_dev = r.err_out ? srv->row_device(r.err_out, set_info(r.set).n / 8) : nullptr;
             const int ctb = set_info(r.set).ct;
             memcpy(r.ct, h_cts + k * ct_stride, ctb);
             memset(r.ct + ctb, 0, CT_STRIDE - ctb);
@@ -903,6 +935,9 @@ void cmd_server_destroy(cmd_server *srv)
     for (auto &k : srv->keys)
         if (k.key)
             cmd_key_free(k.key);
+    for (const auto &rr : srv->row_ranges)
+        if (rr.registered_here)
+            cudaHostUnregister(rr.host);
     if (srv->done_seq)
         cudaFreeHost((void *)srv->done_seq);
     if (srv->device_bytes)
@@ -922,6 +957,31 @@ int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t
     srv->keys.push_back(std::move(ke));
     srv->key_sets.push_back(set);
     *key_id = (uint32_t)(srv->keys.size() - 1);
+    return CMD_OK;
+}
+
+int cmd_server_register_rows(cmd_server *srv, uint8_t *h_rows, size_t bytes)
+{
+    if (!srv || !h_rows || !bytes)
+        return CMD_E_ARG;
+    cudaSetDevice(srv->eng->device);
+    uint8_t *dev = device_view(h_rows, bytes);
+    bool here = false;
+    if (!dev) {
+        // pageable memory: pin and map it for the server's lifetime
+        cudaError_t e = cudaHostRegister(h_rows, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "cmd_server_register_rows: cudaHostRegister");
+        here = true;
+        dev = device_view(h_rows, bytes);
+        if (!dev) {
+            cudaHostUnregister(h_rows);
+            set_last_error("cmd_server_register_rows: the range has no contiguous device mapping");
+            return CMD_E_ARG;
+        }
+    }
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->row_ranges.push_back(cmd_server::RowRange{h_rows, dev, bytes, here});
     return CMD_OK;
 }
 

@@ -7,11 +7,12 @@ so every figure below is bit operations / 32 ("lane-ops").
 
 Work of the algorithm the fused kernel executes, per decryption:
 
-  W_synd = (sb / 4) * (NWU + 11 * NWU / 256)
+  W_synd = (sb / 4) * (NWU + 11 * NWU / R)
            the dense table in groups of four rows: the CTA forms the group's
            16 XOR combinations (11 word XORs per accumulator word, shared by
-           the 256 ciphertexts of a full round), and each ciphertext adds the
-           one its four bits select (NWU = ceil(2tm / 32) words)
+           the R ciphertexts of a full round: 32 per warp of the CTA), and
+           each ciphertext adds the one its four bits select
+           (NWU = ceil(2tm / 32) words)
   W_bm   = [sum_{N<2t} (min(N, t, L_N) + 1) + 2 sum_{N<2t} (min(L_{N+1}, t) + 1)]
            * (m^2 + R_m) / 32
            (the scaled, L-bounded Berlekamp-Massey: discrepancy terms up to
@@ -47,7 +48,7 @@ from __future__ import annotations
 
 SETS = {348864: (12, 3488, 64, 96), 460896: (13, 4608, 96, 156), 6688128: (13, 6688, 128, 208),
         6960119: (13, 6960, 119, 194), 8192128: (13, 8192, 128, 208)}
-ROUND_CTS = 256  # ciphertexts sharing one CTA's combinations (8 warps of 32)
+ROUND_CTS = 256  # ciphertexts sharing one CTA's combinations: 8 warps of 32
 
 
 def fft_depth(t: int) -> int:
@@ -57,13 +58,13 @@ def fft_depth(t: int) -> int:
     return d
 
 
-def work_per_decap(set_id: int) -> dict:
+def work_per_decap(set_id: int, round_cts: int = ROUND_CTS) -> dict:
     m, n, t, ct = SETS[set_id]
     r = 22 if m == 12 else 48
     mul = m * m + r
     sb = 8 * ct
     nwu = (2 * t * m + 31) // 32
-    w_synd = sb / 4 * (nwu + 11 * nwu / ROUND_CTS)
+    w_synd = sb / 4 * (nwu + 11 * nwu / round_cts)
     disc = sum(min(N, t, (N + 1) // 2) + 1 for N in range(2 * t))
     upd = sum(min((N + 2) // 2, t) + 1 for N in range(2 * t))
     w_bm = (disc + 2 * upd) * mul / 32

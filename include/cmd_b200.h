@@ -312,6 +312,17 @@ int cmd_server_create(cmd_engine *eng, const cmd_server_config *cfg, cmd_server 
 void cmd_server_destroy(cmd_server *srv);
 int cmd_server_add_key(cmd_server *srv, cmd_set set, const uint8_t *h_sk, size_t sk_len,
                        uint32_t *key_id);
+/* Registers [h_rows, h_rows + bytes) for result rows.  A request queued
+ * afterwards whose result buffer (err_bytes from an even address) lies in a
+ * registered range has its row stored there by the GPU itself on the latency
+ * kernels' path: the row crosses PCIe while the batch runs, and nothing is
+ * copied on the host when it completes.  Memory the GPU already maps (pinned
+ * by cudaHostAlloc / cudaMallocHost, or registered as mapped) is used as it
+ * is; other memory is pinned and mapped here (cudaHostRegister) and
+ * unregistered by cmd_server_destroy.  The range must stay allocated until
+ * cmd_server_destroy returns.  Other requests, and fused-kernel batches,
+ * take the staged copy. */
+int cmd_server_register_rows(cmd_server *srv, uint8_t *h_rows, size_t bytes);
 /* Queues one ciphertext (ct_bytes of key_id's set); on completion err_bytes
  * of packed error bits are written to h_err_out (may be NULL).  Non-blocking;
  * CMD_E_BUSY when queue_capacity requests are waiting. */

@@ -227,3 +227,38 @@ def test_server_poisson_loadgen(engine, workload):
             s, _ = ring[key_of[i]]
             nb = cmd.set_info(s).err_bytes
             assert np.array_equal(err_pool[i, :nb], expect[i]), i
+
+
+@pytest.mark.parametrize("fused_threshold", [0, 1, 300])
+def test_server_registered_rows(engine, workload, fused_threshold):
+    """Results into registered memory: the tile path's root kernel stores each
+    row there itself (at 4-byte and 2-byte aligned starts), fused batches and
+    odd addresses take the staged copy, and no byte around a row changes."""
+    ring, key_of, cts, expect = workload
+    n = cts.shape[0]
+    stride = 1030  # 2 mod 4: row starts alternate between 4-byte and 2-byte alignment
+    flat = np.full(n * stride + 64, 0xA5, np.uint8)
+    plain = np.full((n, 1024), 0x5A, np.uint8)  # not registered
+    with cmd.Server(engine, max_batch=512, slots=3, max_wait_us=300, fused_threshold=fused_threshold) as srv:
+        ids = [srv.add_key(s, sk) for s, sk in ring]
+        srv.register_rows(flat)
+        offs = []
+        for i in range(n):
+            nb = cmd.set_info(ring[key_of[i]][0]).err_bytes
+            off = 2 + i * stride + (1 if i % 97 == 5 else 0)  # a few odd starts
+            offs.append(off)
+            out = plain[i, :nb] if i % 11 == 3 else flat[off:off + nb]
+            assert srv.submit(ids[key_of[i]], cts[i], out, i) == cmd.CMD_OK
+        srv.drain()
+        comps = srv.poll(max_n=n + 10)
+        assert len(comps) == n and all(c[1] == cmd.CMD_OK for c in comps)
+    touched = np.zeros(flat.size, bool)
+    for i in range(n):
+        nb = cmd.set_info(ring[key_of[i]][0]).err_bytes
+        if i % 11 == 3:
+            assert np.array_equal(plain[i, :nb], expect[i]), i
+            assert (plain[i, nb:] == 0x5A).all(), i
+        else:
+            assert np.array_equal(flat[offs[i]:offs[i] + nb], expect[i]), i
+            touched[offs[i]:offs[i] + nb] = True
+    assert (flat[~touched] == 0xA5).all()
