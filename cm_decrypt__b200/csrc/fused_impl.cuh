@@ -3,12 +3,12 @@
 // batches of many keys and parameter sets.
 //
 // Work unit ("round"): up to WPB*32 ciphertexts of one key.  A CTA takes
-// rounds from a device counter until none are left; warp w of the CTA owns
-// the 32-ciphertext tile w of the round, so after the shared syndrome-table
-// pipeline every warp runs independently:
+// rounds from a device counter until none are left; each warp owns a tile of
+// up to 32 of the round's ciphertexts (warp_share), so after the shared
+// syndrome-table pipeline every warp runs independently:
 //
-//  1. stage its 32 ciphertexts in shared memory (128-bit loads when the round
-//     is one aligned slab);
+//  1. stage its ciphertexts in shared memory (128-bit loads for a full
+//     aligned tile of one slab, 16-bit loads for a partial one);
 //  2. syndrome (util.c:102-114): lane q accumulates the 2t syndromes of
 //     ciphertext q, m bits each back to back; the key's dense syndrome table
 //     streams through shared memory four rows at a time (cp.async double
@@ -104,10 +104,31 @@ struct RoundCtx {
     FusedKeyRef key;
 };
 
-// Index (in the batch) of ciphertext q of warp `warp` in this round.
-__device__ __forceinline__ uint64_t ct_index(const RoundCtx &rc, int warp, int q)
+// Which ciphertexts of a round warp `warp` takes: *first (offset in the
+// round) and the count.  Rounds of more than 16*WPB ciphertexts are spread
+// evenly over the WPB warps (each takes 32 or fewer); smaller ones are packed
+// into whole 32-ciphertext tiles.  Per warp, Berlekamp-Massey costs the same
+// for any fill while the root search costs per ciphertext, and the two warps
+// that share a scheduler set a round's time: once packing would put two full
+// tiles on one scheduler, an even spread shortens the round (a round of 222
+// on 8 warps: 27 or 28 each instead of 32 on seven warps and none on one).
+template <int WPB> __device__ __forceinline__ int warp_share(uint32_t count, int warp, uint32_t *first)
 {
-    const uint64_t slot = rc.tile.first + (uint64_t)warp * 32 + q;
+    if (count > 16u * WPB) {
+        const uint32_t base = count / WPB, extra = count % WPB;
+        *first = warp * base + min((uint32_t)warp, extra);
+        return (int)(base + ((uint32_t)warp < extra ? 1u : 0u));
+    }
+    const int rem = (int)count - warp * 32;
+    *first = (uint32_t)warp * 32;
+    return rem < 0 ? 0 : (rem > 32 ? 32 : rem);
+}
+
+// Index (in the batch) of ciphertext q of the warp whose share starts at
+// offset `first` of this round.
+__device__ __forceinline__ uint64_t ct_index(const RoundCtx &rc, uint32_t first, int q)
+{
+    const uint64_t slot = rc.tile.first + first + q;
     return rc.a->order ? rc.a->order[slot] : slot;
 }
 
@@ -119,8 +140,8 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     constexpr int M = Z::M, T = Z::T, TWD = Z::TWD, NW = P::NW;
     const FusedArgs &a = *rc.a;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int rem = (int)rc.tile.count - warp * 32;
-    const int ntile = rem < 0 ? 0 : (rem > 32 ? 32 : rem);
+    uint32_t wfirst;
+    const int ntile = warp_share<WPB>(rc.tile.count, warp, &wfirst);
 
     uint32_t *tabbuf = reinterpret_cast<uint32_t *>(smem);
     uint8_t *wbase = smem + Z::SYN_B + warp * Z::WARP_B;
@@ -132,25 +153,28 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     const uint32_t *tab = rc.key.tab;
 
     // ---- 1. stage ciphertexts --------------------------------------------
-    if (!a.order && ntile == 32) {
-        const uint8_t *src = a.cts + ct_index(rc, warp, 0) * P::CT;
-        if ((((uintptr_t)src) & 15) == 0) {
+    if (!a.order && !a.ct_off) {
+        // one slab: 128-bit loads for a whole aligned tile, else 16-bit loads
+        // (every set's ciphertext length is even)
+        const uint8_t *src = a.cts + ct_index(rc, wfirst, 0) * P::CT;
+        if (ntile == 32 && (((uintptr_t)src) & 15) == 0) {
             for (int v = lane; v < Z::RAW_B / 16; v += 32)
                 reinterpret_cast<uint4 *>(raw)[v] = __ldg(reinterpret_cast<const uint4 *>(src) + v);
         } else {
-            for (int v = lane; v < Z::RAW_B; v += 32)
-                raw[v] = src[v];
+            const uint16_t *s16 = reinterpret_cast<const uint16_t *>(src);
+            for (int v = lane; v < ntile * P::CT / 2; v += 32)
+                reinterpret_cast<uint16_t *>(raw)[v] = __ldg(s16 + v);
         }
     } else {
         for (int q = 0; q < ntile; q++) {
-            const uint64_t c = ct_index(rc, warp, q);
+            const uint64_t c = ct_index(rc, wfirst, q);
             const uint8_t *src = a.cts + (a.ct_off ? a.ct_off[c] : c * (uint64_t)P::CT);
             for (int v = lane; v < P::CT; v += 32)
                 raw[q * P::CT + v] = src[v];
         }
-        for (int v = ntile * P::CT + lane; v < Z::RAW_B; v += 32)
-            raw[v] = 0;
     }
+    for (int v = ntile * P::CT + lane; v < Z::RAW_B; v += 32)
+        raw[v] = 0;
     if (lane < 4)
         reinterpret_cast<uint32_t *>(raw + Z::RAW_B)[lane] = 0;  // tail read by ld_u32_any
     __syncwarp();
@@ -372,7 +396,7 @@ __device__ __forceinline__ void fused_round(const RoundCtx &rc, uint8_t *smem)
     const FftPlanDev pl = a.fft[S];
     fft_convert<S, M, 32>(cv, pl.scalpow, lane, [] { __syncwarp(); });
     for (int q = 0; q < ntile; q++) {
-        const uint64_t c = ct_index(rc, warp, q);
+        const uint64_t c = ct_index(rc, wfirst, q);
         uint32_t *erow = a.err ? a.err + (a.err_off ? a.err_off[c] : c * (uint64_t)a.err_stride) : nullptr;
         uint16_t *prow = a.pos ? a.pos + c * (uint64_t)a.pos_stride : nullptr;
         uint8_t *epack = a.err_packed ? a.err_packed + c * (uint64_t)(Set<S>::N / 8) : nullptr;
