@@ -110,8 +110,8 @@ struct RoundCtx {
 // into whole 32-ciphertext tiles.  Per warp, Berlekamp-Massey costs the same
 // for any fill while the root search costs per ciphertext, and the two warps
 // that share a scheduler set a round's time: once packing would put two full
-// tiles on one scheduler, an even spread shortens the round (a round of 222
-// on 8 warps: 27 or 28 each instead of 32 on seven warps and none on one).
+// tiles on one scheduler, an even spread shortens the round (a round of 224
+// on 8 warps: 28 each instead of 32 on seven warps and none on one).
 template <int WPB> __device__ __forceinline__ int warp_share(uint32_t count, int warp, uint32_t *first)
 {
     if (count > 16u * WPB) {

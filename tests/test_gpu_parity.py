@@ -107,6 +107,29 @@ def test_kem_fixture_errorstream(engine, keys, s, path):
     assert cmd.errorstream(s, err) == golden_errorstream(s)
 
 
+@pytest.mark.parametrize("wpb,balanced", [(8, True), (8, False), (4, True), (4, False)])
+def test_fused_round_shares(engine, keys, wpb, balanced):
+    """Fused rounds of every fill: whole tiles, rounds spread evenly over the
+    CTA's warps (more than 16 ciphertexts a warp) and short tails, for both
+    CTA sizes and round schedules.  The fused rows must equal the plain path's
+    (itself checked against the oracle) bit for bit, malformed ones included,
+    and the valid ones their planted errors."""
+    s = 6960119
+    pk = cmd.PubKey(s, golden_sk(s))
+    before = cmd.fused_config(engine, s)
+    try:
+        cmd.set_fused_config(engine, s, wpb, balanced)
+        for count in (148 * 160, 148 * 224 + 100, 5 * 32 * wpb + 77, 200, 131, 33):
+            cts, planted, valid = pk.ciphertexts(seed=500 + count, count=count, malformed_permille=100)
+            err_f, w_f = cmd.decrypt(engine, keys[s], cts, path="fused")
+            err_p, w_p = cmd.decrypt(engine, keys[s], cts, path="plain")
+            assert np.array_equal(err_f, err_p), (wpb, balanced, count)
+            assert np.array_equal(w_f, w_p), (wpb, balanced, count)
+            assert np.array_equal(err_f[valid == 1], planted[valid == 1]), (wpb, balanced, count)
+    finally:
+        cmd.set_fused_config(engine, s, before["wpb"], before["balanced"])
+
+
 @pytest.mark.parametrize("path", ["plain", "fused", "tile"])
 @pytest.mark.parametrize("s", SETS)
 def test_decrypt_vs_oracle(oracle_mod, engine, keys, s, path):
